@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the pairwise SIFT brute-force matcher (dense int8 contraction workload).
+
+Workload (N=1): one image pair of 32768 query x 32768 train 128-byte SIFT-like descriptors
+(50% true overlap, noise sigma 10), matched bidirectionally with second-best distance, ratio
+test 0.8 and cross-check flags. A step = squared norms of both sets + the fused tcgen05 matcher
+(init, match, flags kernels) over inputs already resident in HBM. Inputs (8 MiB) are smaller than
+L2, so L2 is flushed (a 256 MiB write) between timed steps, outside the timed region.
+
+Multi-GPU: image pairs are independent, so each rank matches its own pair (weak scaling, no
+collective on the data path); the step time is the max over ranks.
+
+--impl reference: the reference has no CPU matcher; its CPU path is the exhaustive exact loop of
+its kernel tests (test/bruteForceMatchKernelTest.cpp:140-164), restated in oracle/ and timed on
+the host cores (all threads) on a bounded row sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUERY = 32768
+N_TRAIN = 32768
+OVERLAP = 0.5
+SIGMA = 10.0
+WORKLOAD = "bf_pair_32768x32768"
+METRIC = "desc-pairs/s"
+
+
+def _config():
+    return {
+        "workload": WORKLOAD,
+        "n_query": N_QUERY,
+        "n_train": N_TRAIN,
+        "overlap": OVERLAP,
+        "noise_sigma": SIGMA,
+        "ratio": 0.8,
+        "cross_check": True,
+        "l2": "256 MiB flush write between timed steps (inputs 8 MiB < L2)",
+        "parallelism": "independent pairs per rank (replicas)",
+    }
+
+
+def _dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons in the background during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(q, t, rows, threads):
+    """Times the oracle port (exhaustive exact loop + cross-check) on `rows` query rows."""
+    from oracle import oracle as orc
+    orc.load()
+    sub = q[:rows]
+    orc.bf_match(sub[:8], t, threads=threads)  # warm
+    t0 = time.perf_counter()
+    fwd, bwd, sec = orc.bf_match(sub, t, threads=threads)
+    dt = time.perf_counter() - t0
+    return rows * len(t) / dt, dt
+
+
+def run_reference(args):
+    import numpy as np  # noqa: F401
+    from rapidsfm_b200 import synth
+    ws, rank, _ = _dist_env()
+    if rank != 0:
+        return
+    q, t, _ = synth.make_pair(N_QUERY, N_TRAIN, OVERLAP, SIGMA, seed=1)
+    threads = os.cpu_count() or 1
+    rows = 256
+    # size the sample to ~10 s of CPU work per step at most
+    rate, dt = cpu_baseline(q, t, 32, threads)
+    rows = int(max(32, min(4096, rate * 5.0 / len(t))))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(q, t, min(rows, 64), threads)
+    for _ in range(args.steps):
+        v, _ = cpu_baseline(q, t, rows, threads)
+        vals.append(v)
+    value = statistics.median(vals)
+    ms_per_step = N_QUERY * N_TRAIN / value * 1e3
+    sample = f"{rows} query rows x {N_TRAIN} train of the {N_QUERY}x{N_TRAIN} pair, exact bidirectional"
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "desc-pairs/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": _config(),
+        "cpu_baseline": {"value": value, "unit": "desc-pairs/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "desc-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import rapidsfm_b200 as R
+    from rapidsfm_b200 import synth
+
+    ws, rank, local = _dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = R._lib.load()
+    stream = torch.cuda.current_stream(dev)
+
+    q, t, _ = synth.make_pair(N_QUERY, N_TRAIN, OVERLAP, SIGMA, seed=1 + rank)
+    dq = torch.from_numpy(q).to(dev)
+    dt_ = torch.from_numpy(t).to(dev)
+    task = R.BFTask(dq, dt_)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    nops = 2.0 * N_QUERY * N_TRAIN * 128
+
+    def step():
+        n = 0
+        R.precomp_sift_sqr_norm(task.descA, out=task.sqrA)
+        n += R.last_launch_count()
+        R.precomp_sift_sqr_norm(task.descB, out=task.sqrB)
+        n += R.last_launch_count()
+        R.bf_match_ext([task])
+        n += R.last_launch_count()
+        return n
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    assert R.device_error() == 0
+
+    # ---- device-timed steps (inputs resident in HBM)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    import ctypes
+    lib.rsfm_profile_enable(1)
+    step_ms, launches = [], 0
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_(i & 255)
+        evs[i][0].record(stream)
+        launches += step()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    kms = ctypes.c_float(0)
+    klaunch = ctypes.c_uint32(0)
+    R._lib.check(lib.rsfm_profile_collect(ctypes.byref(kms), ctypes.byref(klaunch)), "rsfm_profile_collect")
+    lib.rsfm_profile_enable(0)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if ws > 1:
+        tt = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        torch.distributed.barrier()
+    clocks = sampler.stop() if sampler else None
+    ms_per_step = total_ms / args.steps
+    value = ws * N_QUERY * N_TRAIN / (ms_per_step * 1e-3)
+    kernel_ms = kms.value / max(1, klaunch.value)
+
+    # ---- end to end through the public API: H2D of both descriptor sets from pinned memory,
+    # match, D2H of every result array; all inside the timed region.
+    hq = torch.from_numpy(q).pin_memory()
+    ht = torch.from_numpy(t).pin_memory()
+    outs = {k: torch.empty(v.numel(), dtype=v.dtype).pin_memory() for k, v in
+            (("fwd", task.bestA), ("bwd", task.bestB), ("sec", task.secondA), ("flg", task.flagsA))}
+    h2d = hq.numel() + ht.numel()
+    d2h = sum(v.numel() * v.element_size() for v in outs.values())
+    e2e_ms = []
+    for i in range(args.steps + 1):
+        flush.fill_(i & 255)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dq.copy_(hq, non_blocking=True)
+        dt_.copy_(ht, non_blocking=True)
+        step()
+        outs["fwd"].copy_(task.bestA, non_blocking=True)
+        outs["bwd"].copy_(task.bestB, non_blocking=True)
+        outs["sec"].copy_(task.secondA, non_blocking=True)
+        outs["flg"].copy_(task.flagsA, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_step = statistics.mean(e2e_ms)
+    if ws > 1:
+        tt = torch.tensor([e2e_step], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_step = float(tt.item())
+    e2e_value = ws * N_QUERY * N_TRAIN / (e2e_step * 1e-3)
+
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    # ---- roofline: dense int8 tensor pipe (live MMA-only probe on this GPU)
+    tops = ctypes.c_float(0)
+    pms = ctypes.c_float(0)
+    R._lib.check(lib.rsfm_int8_mma_peak(20000, ctypes.byref(tops), ctypes.byref(pms)), "rsfm_int8_mma_peak")
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    bf16 = None
+    if os.path.exists(peaks_path):
+        try:
+            bf16 = json.load(open(peaks_path)).get("bf16_tflops")
+        except Exception:
+            bf16 = None
+    achieved = nops / (kernel_ms * 1e-3) / 1e12
+    peak = float(tops.value)
+    roofline = {
+        "bound": "tensor",
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "TOP/s",
+        "frac": achieved / peak,
+        "traffic": None,
+        "kernel": "bf_match_kernel",
+        "kernel_ms": kernel_ms,
+        "peak_source": "measured live: int8 tcgen05 MMA-only probe (rsfm_int8_mma_peak), dense",
+        "peak_bf16_x2_of_measured": (2 * bf16) if bf16 else None,
+        "ops_per_launch": nops,
+    }
+
+    # ---- CPU baseline: oracle port on a bounded row sample (~10 s)
+    threads = os.cpu_count() or 1
+    rate, _ = cpu_baseline(q, t, 32, threads)
+    rows = int(max(32, min(4096, rate * 8.0 / N_TRAIN)))
+    cpu_val, cpu_dt = cpu_baseline(q, t, rows, threads)
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "desc-pairs/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": _config(),
+        "e2e": {"value": e2e_value, "unit": "desc-pairs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "cpu_baseline": {"value": cpu_val, "unit": "desc-pairs/s", "cores": threads, "kind": "port",
+                         "sample": f"{rows} query rows x {N_TRAIN} train of the pair ({cpu_dt:.1f} s)"},
+        "clocks": clocks,
+        "int8_tops_effective": nops / (ms_per_step * 1e-3) / 1e12,
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,26 @@
+#!/usr/bin/env bash
+# Builds RapidSFM's own matcher kernels (from the reference sources, unmodified, where they lie)
+# into oracle/_ref/librsfm_ref.so, for sm_100a, with the reference's release flags
+# (CMakeLists.txt:60-62: --use_fast_math -DNDEBUG --expt-relaxed-constexpr). The missing
+# cuda-utils headers are replaced by this project's minimal stand-ins in oracle/ref_shim/.
+# Test infrastructure only. Output goes to oracle/_ref/ (git-ignored; travels with the tree).
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${RSFM_REFERENCE_DIR:-/root/reference}"
+OUT="$HERE/_ref"
+if [ ! -f "$REF/bruteForceMatchIMMA.cu" ]; then
+  echo "reference sources not found at $REF; skipping" >&2
+  exit 0
+fi
+mkdir -p "$OUT"
+NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+"$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 --use_fast_math -DNDEBUG \
+  --expt-relaxed-constexpr -Xcompiler -fPIC -shared \
+  -I"$HERE/ref_shim" -I"$REF" \
+  -o "$OUT/librsfm_ref.so.tmp" \
+  "$REF/bruteForceMatchIMMA.cu" "$REF/bruteForceMatch.cpp" \
+  "$REF/casHash/accumulateDesc.cu" "$REF/casHash/computeHash.cu" \
+  "$REF/casHash/buildBuckets.cu" "$REF/casHash/findBestMatch.cu" \
+  "$HERE/ref_wrapper.cu"
+mv "$OUT/librsfm_ref.so.tmp" "$OUT/librsfm_ref.so"
+echo "$OUT/librsfm_ref.so"

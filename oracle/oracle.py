@@ -1,0 +1,225 @@
+"""ctypes front end of the CPU oracle (oracle/liboracle.so). TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, as the
+checker of the CUDA path. The product (rapidsfm_b200/) never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+_P = ctypes.c_void_p
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = ctypes.CDLL(LIB_PATH)
+    u32, i32, u64 = ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint64
+    sig = {
+        "orc_sqr_norm": (None, [_P, u32, _P]),
+        "orc_bf_match": (None, [_P, u32, _P, u32, _P, _P, _P, ctypes.c_int]),
+        "orc_match_flags": (None, [_P, _P, u32, _P, u32, u32, u32, _P]),
+        "orc_cross_check": (ctypes.c_size_t, [_P, u32, _P, u32, _P]),
+        "orc_remove_match_conflicts": (ctypes.c_size_t, [_P, u32, u32, _P]),
+        "orc_cashash_make_weights": (None, [_P, _P]),
+        "orc_cashash_accumulate": (None, [_P, u32, _P, ctypes.c_int]),
+        "orc_cashash_compute_bias": (None, [_P, _P, _P, u64, i32, _P]),
+        "orc_cashash_compute_bias_float": (None, [_P, _P, _P, u64, _P]),
+        "orc_cashash_hash": (None, [_P, _P, i32, _P, u32, _P, _P]),
+        "orc_cashash_histogram": (None, [_P, u32, _P]),
+        "orc_cashash_bucket_bounds": (u32, [_P, _P, _P]),
+        "orc_cashash_build_buckets": (None, [_P, u32, _P, _P]),
+        "orc_cashash_find_best_match": (None, [_P, u32, _P, _P, _P, u32, _P, _P, _P, _P]),
+        "orc_cashash_match_ranked": (None, [_P, _P, _P, u32, _P, _P, _P, u32, i32, i32, u32, u32, _P, _P, _P, _P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _c(a):
+    return a.ctypes.data_as(_P)
+
+
+def sqr_norm(desc):
+    desc = np.ascontiguousarray(desc, dtype=np.uint8)
+    out = np.empty(len(desc), dtype=np.uint32)
+    load().orc_sqr_norm(_c(desc), len(desc), _c(out))
+    return out
+
+
+def bf_match(a, b, threads=0):
+    """Exact bidirectional matcher. Returns (fwd [nA,2] uint32, bwd [nB,2] uint32, second [nA] uint32)."""
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.uint8)
+    fwd = np.empty((len(a), 2), dtype=np.uint32)
+    bwd = np.empty((len(b), 2), dtype=np.uint32)
+    sec = np.empty(len(a), dtype=np.uint32)
+    load().orc_bf_match(_c(a), len(a), _c(b), len(b), _c(fwd), _c(bwd), _c(sec), threads)
+    return fwd, bwd, sec
+
+
+def match_flags(fwd, second, bwd, ratio_num=64, ratio_den=100):
+    out = np.empty(len(fwd), dtype=np.uint32)
+    fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
+    bwd = np.ascontiguousarray(bwd, dtype=np.uint32)
+    second = np.ascontiguousarray(second, dtype=np.uint32)
+    load().orc_match_flags(_c(fwd), _c(second), len(fwd), _c(bwd), len(bwd), ratio_num, ratio_den, _c(out))
+    return out
+
+
+_VM = np.dtype([("idxQuery", "<u4"), ("idxTrain", "<u4"), ("distance", "<f4")])
+
+
+def cross_check(fwd, bwd):
+    fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
+    bwd = np.ascontiguousarray(bwd, dtype=np.uint32)
+    out = np.empty(max(1, min(len(fwd), len(bwd))), dtype=_VM)
+    n = load().orc_cross_check(_c(fwd), len(fwd), _c(bwd), len(bwd), _c(out))
+    return out[:n].copy()
+
+
+def remove_match_conflicts(fwd, nb_train):
+    fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
+    out = np.empty(max(1, min(len(fwd), nb_train)), dtype=_VM)
+    n = load().orc_remove_match_conflicts(_c(fwd), len(fwd), nb_train, _c(out))
+    return out[:n].copy()
+
+
+# ---------------------------------------------------------------- cascade hash
+def cashash_weights():
+    w = np.empty((64, 128), dtype=np.int8)
+    b = np.empty(64, dtype=np.int32)
+    load().orc_cashash_make_weights(_c(w), _c(b))
+    return w, b
+
+
+def cashash_accumulate(desc, acc=None):
+    desc = np.ascontiguousarray(desc, dtype=np.uint8)
+    init = acc is None
+    acc = np.zeros(128, dtype=np.uint64) if acc is None else acc
+    load().orc_cashash_accumulate(_c(desc), len(desc), _c(acc), int(init))
+    return acc
+
+
+def cashash_bias(weights, bias_base, acc, n, exact=True):
+    weights = np.ascontiguousarray(weights, dtype=np.int8)
+    bias_base = np.ascontiguousarray(bias_base, dtype=np.int32)
+    out = np.empty(len(bias_base), dtype=np.int32)
+    if exact:
+        load().orc_cashash_compute_bias(_c(weights), _c(bias_base), _c(acc), n, len(bias_base), _c(out))
+    else:
+        load().orc_cashash_compute_bias_float(_c(weights), _c(bias_base), _c(acc), n, _c(out))
+    return out
+
+
+def cashash_hash(weights, bias, desc):
+    """weights int8 [C,128] (C = 64 or 192), bias int32 [C] -> keys uint8 [n,8], remap uint32 [n,4] or None."""
+    weights = np.ascontiguousarray(weights, dtype=np.int8)
+    bias = np.ascontiguousarray(bias, dtype=np.int32)
+    desc = np.ascontiguousarray(desc, dtype=np.uint8)
+    c = len(weights)
+    keys = np.empty((len(desc), 8), dtype=np.uint8)
+    remap = np.empty((len(desc), 4), dtype=np.uint32) if c > 64 else None
+    load().orc_cashash_hash(_c(weights), _c(bias), c, _c(desc), len(desc), _c(keys),
+                            _c(remap) if remap is not None else None)
+    return keys, remap
+
+
+def cashash_buckets(keys):
+    """-> (hist [8,256], lower [8,256], upper [8,256], max bucket size, buckets [8,n])."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint8)
+    n = len(keys)
+    hist = np.empty((8, 256), dtype=np.uint32)
+    lower = np.empty((8, 256), dtype=np.uint32)
+    upper = np.empty((8, 256), dtype=np.uint32)
+    L = load()
+    L.orc_cashash_histogram(_c(keys), n, _c(hist))
+    mx = L.orc_cashash_bucket_bounds(_c(hist), _c(lower), _c(upper))
+    alloc = lower.copy()
+    buckets = np.empty((8, max(n, 1)), dtype=np.uint32)
+    L.orc_cashash_build_buckets(_c(keys), n, _c(alloc), _c(buckets))
+    return hist, lower, upper, int(mx), buckets[:, :n]
+
+
+def cashash_find_best_match(q_desc, q_upper, q_buckets, t_desc, t_upper, t_buckets):
+    q_desc = np.ascontiguousarray(q_desc, dtype=np.uint8)
+    t_desc = np.ascontiguousarray(t_desc, dtype=np.uint8)
+    q_upper = np.ascontiguousarray(q_upper, dtype=np.uint32)
+    t_upper = np.ascontiguousarray(t_upper, dtype=np.uint32)
+    q_buckets = np.ascontiguousarray(q_buckets, dtype=np.uint32)
+    t_buckets = np.ascontiguousarray(t_buckets, dtype=np.uint32)
+    qb = np.empty((len(q_desc), 2), dtype=np.uint32)
+    tb = np.empty((len(t_desc), 2), dtype=np.uint32)
+    load().orc_cashash_find_best_match(_c(q_desc), len(q_desc), _c(q_upper), _c(q_buckets), _c(t_desc),
+                                       len(t_desc), _c(t_upper), _c(t_buckets), _c(qb), _c(tb))
+    return qb, tb
+
+
+def cashash_match_ranked(q_desc, q_keys, q_codes, t_desc, t_keys, t_codes, tables=6, top_k=10, ratio_num=64,
+                         ratio_den=100):
+    arrs = [np.ascontiguousarray(x) for x in (q_desc, q_keys, q_codes, t_desc, t_keys, t_codes)]
+    q_desc, q_keys, q_codes, t_desc, t_keys, t_codes = arrs
+    nq = len(q_desc)
+    best = np.empty((nq, 2), dtype=np.uint32)
+    second = np.empty(nq, dtype=np.uint32)
+    flags = np.empty(nq, dtype=np.uint32)
+    ncand = np.empty(nq, dtype=np.uint32)
+    load().orc_cashash_match_ranked(_c(q_desc), _c(q_keys), _c(q_codes), nq, _c(t_desc), _c(t_keys), _c(t_codes),
+                                    len(t_desc), tables, top_k, ratio_num, ratio_den, _c(best), _c(second),
+                                    _c(flags), _c(ncand))
+    return best, second, flags, ncand
+
+
+# ---------------------------------------------------------------- reference kernels (GPU)
+REF_LIB_PATH = os.path.join(HERE, "_ref", "librsfm_ref.so")
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB_PATH)
+
+
+def load_ref():
+    """RapidSFM's own matcher kernels, built from its sources by oracle/build_ref.sh."""
+    global _ref
+    if _ref is not None:
+        return _ref
+    lib = ctypes.CDLL(REF_LIB_PATH)
+    u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+    sig = {
+        "ref_precomp_sqr_norm": (i32, [_P, _P, u32, _P]),
+        "ref_bf_match_imma": (i32, [_P, ctypes.c_size_t, _P]),
+        "ref_cross_check": (ctypes.c_size_t, [_P, u32, _P, u32, _P]),
+        "ref_remove_match_conflicts": (ctypes.c_size_t, [_P, u32, u32, _P]),
+        "ref_cashash_accumulate": (i32, [_P, _P, u32, i32, _P]),
+        "ref_cashash_compute_bias": (i32, [_P, _P, _P, _P, u64, _P]),
+        "ref_cashash_hash": (i32, [_P, _P, i32, _P, u32, _P, _P, _P, _P]),
+        "ref_cashash_histogram": (i32, [_P, _P, u32, _P]),
+        "ref_cashash_bucket_bound": (i32, [_P, _P, _P, _P, _P]),
+        "ref_cashash_build_buckets": (i32, [_P, u32, _P, _P, _P]),
+        "ref_cashash_find_best_match": (i32, [_P, _P, _P, u32, _P, u32, _P, u32, _P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _ref = lib
+    return lib

@@ -1,0 +1,40 @@
+// Minimal stand-in for cuda-utils' cuda_utils.h (written for this project): error checks,
+// integer helpers and a kernel-launch helper, enough for RapidSFM's matcher sources.
+#pragma once
+#include <algorithm>
+#include <array>
+#include <cassert>
+#include <limits>
+#include <vector>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <cuda_runtime.h>
+
+#define cudaCheck(expr)                                                                          \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(_e)); \
+    } while (0)
+#define ASSERT(cond)                                                       \
+    do {                                                                   \
+        if (!(cond)) throw std::runtime_error("assertion failed: " #cond); \
+    } while (0)
+
+template <typename A, typename B>
+__host__ __device__ constexpr auto divUp(A a, B b) -> std::common_type_t<A, B> {
+    return (a + b - 1) / b;
+}
+template <typename T, typename L, typename U>
+__host__ __device__ constexpr bool inRange(T x, L lo, U hi) {
+    return x >= lo && x < hi;
+}
+#ifdef __CUDACC__
+template <typename Kernel, typename... Args>
+void launchKernel(Kernel kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, const Args&... args) {
+    kernel<<<grid, block, smem, stream>>>(args...);
+    cudaCheck(cudaGetLastError());
+}
+#endif

@@ -1,0 +1,18 @@
+"""rapidsfm_b200: B200 (sm_100a) implementation of RapidSFM's pairwise SIFT matching hot path.
+
+The compute lives in the CUDA library rapidsfm_b200/lib/librsfm_b200.so behind the C ABI of
+include/rsfm_b200.h; this package is the Python host side (ctypes + torch device buffers).
+"""
+from . import _lib  # noqa: F401
+from .matcher import (  # noqa: F401
+    BFTask,
+    BruteForceMatcher,
+    bf_match,
+    bf_match_ext,
+    cross_check_matches,
+    device_error,
+    last_launch_count,
+    precomp_sift_sqr_norm,
+    remove_match_conflicts,
+    unpack_best,
+)

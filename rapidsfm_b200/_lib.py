@@ -1,0 +1,94 @@
+"""ctypes binding of the C ABI declared in include/rsfm_b200.h.
+
+The shared library is built in-tree (rapidsfm_b200/lib/librsfm_b200.so). Loading fails loudly
+when it is missing: there is no fallback implementation.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librsfm_b200.so")
+
+RSFM_OK = 0
+STATUS_NAMES = {
+    0: "RSFM_OK",
+    1: "RSFM_ERR_INVALID_ARG",
+    2: "RSFM_ERR_CAPACITY",
+    3: "RSFM_ERR_CUDA",
+    4: "RSFM_ERR_DEVICE_TIMEOUT",
+    5: "RSFM_ERR_UNSUPPORTED",
+}
+
+
+class RsfmError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}")
+
+
+class BestMatch(ctypes.Structure):
+    """BestMatchImpl<uint32_t> (bruteForceMatch.h:89-94)."""
+    _fields_ = [("index", ctypes.c_uint32), ("distance", ctypes.c_uint32)]
+
+
+class SiftBFTask(ctypes.Structure):
+    """SiftBruteForceMatchTask (bruteForceMatch.h:96-112)."""
+    _fields_ = [
+        ("nbDescA", ctypes.c_uint32),
+        ("nbDescB", ctypes.c_uint32),
+        ("descA", ctypes.c_void_p),
+        ("descB", ctypes.c_void_p),
+        ("bestMatchA", ctypes.c_void_p),
+        ("bestMatchB", ctypes.c_void_p),
+        ("sqrNormDescA", ctypes.c_void_p),
+        ("sqrNormDescB", ctypes.c_void_p),
+    ]
+
+
+class ValidMatch(ctypes.Structure):
+    """ValidMatch (bruteForceMatch.h:120-125)."""
+    _fields_ = [("idxQuery", ctypes.c_uint32), ("idxTrain", ctypes.c_uint32), ("distance", ctypes.c_float)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rsfm_precomp_sift_sqr_norm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_bf_match": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
+    "rsfm_bf_match_ext": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_cross_check_matches": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                   ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_remove_match_conflicts": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                                      ctypes.c_void_p]),
+    "rsfm_device_error": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32)]),
+    "rsfm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "rsfm_last_launch_count": (ctypes.c_uint32, []),
+    "rsfm_profile_enable": (ctypes.c_int, [ctypes.c_int]),
+    "rsfm_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)]),
+    "rsfm_int8_mma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+}
+
+_lib = None
+
+
+def load():
+    """Loads librsfm_b200.so (once) and declares every exported prototype."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m rapidsfm_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status, what):
+    if status != RSFM_OK:
+        raise RsfmError(status, what)

@@ -1,0 +1,96 @@
+// Host helpers: tensor-map encoding, device error word, status strings, launch accounting.
+#include "common.h"
+#include <cudaTypedefs.h>
+#include <mutex>
+
+namespace rsfm_b200 {
+
+static thread_local uint32_t t_launches = 0;
+void launch_count_reset() { t_launches = 0; }
+void launch_count_add(uint32_t n) { t_launches += n; }
+
+// One word per device, written by kernels when a bounded wait gives up.
+__device__ uint32_t g_device_error = 0;
+
+uint32_t* device_error_word() {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_device_error) != cudaSuccess) return nullptr;
+    return static_cast<uint32_t*>(p);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int encode_desc_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint32_t boxRows) {
+    auto fn = get_encode_fn();
+    if (!fn) return RSFM_ERR_UNSUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0) return RSFM_ERR_INVALID_ARG;
+    cuuint64_t dims[2] = {128, rows};
+    cuuint64_t strides[1] = {128};
+    cuuint32_t box[2] = {128, boxRows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? RSFM_OK : RSFM_ERR_INVALID_ARG;
+}
+
+int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows) {
+    auto fn = get_encode_fn();
+    if (!fn) return RSFM_ERR_UNSUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0) return RSFM_ERR_INVALID_ARG;
+    cuuint64_t dims[2] = {128, rows};
+    cuuint64_t strides[1] = {128};
+    cuuint32_t box[2] = {128, 1};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? RSFM_OK : RSFM_ERR_INVALID_ARG;
+}
+
+int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    return n;
+}
+
+}  // namespace rsfm_b200
+
+using namespace rsfm_b200;
+
+extern "C" int rsfm_device_error(uint32_t* code) {
+    if (!code) return RSFM_ERR_INVALID_ARG;
+    uint32_t* w = device_error_word();
+    if (!w) return RSFM_ERR_CUDA;
+    RSFM_CUDA_TRY(cudaDeviceSynchronize());
+    RSFM_CUDA_TRY(cudaMemcpy(code, w, 4, cudaMemcpyDeviceToHost));
+    RSFM_CUDA_TRY(cudaMemset(w, 0, 4));
+    return RSFM_OK;
+}
+
+extern "C" const char* rsfm_status_string(int status) {
+    switch (status) {
+        case RSFM_OK: return "ok";
+        case RSFM_ERR_INVALID_ARG: return "invalid argument";
+        case RSFM_ERR_CAPACITY: return "size exceeds capacity";
+        case RSFM_ERR_CUDA: return "CUDA runtime error";
+        case RSFM_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case RSFM_ERR_UNSUPPORTED: return "unsupported device or driver";
+    }
+    return "unknown status";
+}
+
+extern "C" uint32_t rsfm_last_launch_count(void) { return t_launches; }

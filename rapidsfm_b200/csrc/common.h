@@ -1,0 +1,42 @@
+// Host-side helpers shared by the library's translation units: status codes, CUDA error
+// mapping, TMA tensor-map encoding through the driver entry point, launch accounting.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "../../include/rsfm_b200.h"
+
+namespace rsfm_b200 {
+
+// Kernels launched by the current rsfm_* call on this host thread.
+void launch_count_reset();
+void launch_count_add(uint32_t n);
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA; }
+
+#define RSFM_CUDA_TRY(expr)                          \
+    do {                                             \
+        cudaError_t _e = (expr);                     \
+        if (_e != cudaSuccess) return RSFM_ERR_CUDA; \
+    } while (0)
+
+// 2D uint8 tensor map over an array of `rows` descriptors of 128 bytes, tile = boxRows x 128
+// bytes, 128-byte swizzle (the K-major SW128 layout the UMMA descriptors expect). Rows past
+// `rows` read as zero.
+int encode_desc_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint32_t boxRows);
+
+// 2D uint8 tensor map for one-row gathers (tile::gather4): box = 1 x 128 bytes, no swizzle.
+int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows);
+
+int sm_count();
+
+// Dominant-kernel event bracketing (see rsfm_profile_enable). profile_begin returns false when
+// profiling is off; otherwise the caller launches the kernel and then calls profile_end.
+bool profile_begin(cudaStream_t s, void** token);
+void profile_end(cudaStream_t s, void* token);
+
+// Address of this library's device-side error word on the current device.
+uint32_t* device_error_word();
+
+}  // namespace rsfm_b200

@@ -1,0 +1,175 @@
+"""Python host interface mirroring RapidSFM's matcher API, on top of the C ABI.
+
+Reference interfaces mirrored (paths relative to the RapidSFM source tree):
+  launchPreCompSiftSqrNorm    bruteForceMatch.h:135        -> precomp_sift_sqr_norm
+  launchBruteForceMatchIMMA   bruteForceMatch.h:136        -> bf_match
+  crossCheckMatches           bruteForceMatch.h:126        -> cross_check_matches
+  removeMatchConflicts        bruteForceMatch.h:128        -> remove_match_conflicts
+  BruteForceMatcher           bruteForceMatcher.h:28-102   -> BruteForceMatcher
+    registerImage / match / matchAndFilter                 -> register_image / match / match_and_filter
+
+Device buffers are torch CUDA tensors (torch is used only to own device memory and streams).
+Descriptors are uint8 tensors of shape [n, 128]; results are int64 views of BestMatch pairs.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+RATIO_NUM_08 = 64   # ratio test 0.8 on squared distances: 100 * best < 64 * second
+RATIO_DEN_08 = 100
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+def _check_desc(d):
+    if d.dtype != torch.uint8 or d.dim() != 2 or d.shape[1] != 128 or not d.is_cuda or not d.is_contiguous():
+        raise ValueError("descriptors must be a contiguous CUDA uint8 tensor of shape [n, 128]")
+
+
+def precomp_sift_sqr_norm(desc, out=None, stream=None):
+    """Squared norm of each descriptor (uint32 stored in an int32 tensor)."""
+    _check_desc(desc)
+    lib = _lib.load()
+    n = desc.shape[0]
+    if out is None:
+        out = torch.empty(n, dtype=torch.int32, device=desc.device)
+    _lib.check(lib.rsfm_precomp_sift_sqr_norm(_ptr(out), _ptr(desc), n, _stream_ptr(stream)),
+               "rsfm_precomp_sift_sqr_norm")
+    return out
+
+
+class BFTask:
+    """One query/train pair: descA (queries) vs descB (train)."""
+
+    def __init__(self, descA, descB, sqrA=None, sqrB=None, stream=None):
+        _check_desc(descA)
+        _check_desc(descB)
+        self.descA, self.descB = descA, descB
+        self.sqrA = sqrA if sqrA is not None else precomp_sift_sqr_norm(descA, stream=stream)
+        self.sqrB = sqrB if sqrB is not None else precomp_sift_sqr_norm(descB, stream=stream)
+        dev = descA.device
+        self.bestA = torch.empty(descA.shape[0], dtype=torch.int64, device=dev)
+        self.bestB = torch.empty(descB.shape[0], dtype=torch.int64, device=dev)
+        self.secondA = None
+        self.flagsA = None
+
+    def as_ctype(self):
+        return _lib.SiftBFTask(self.descA.shape[0], self.descB.shape[0], self.descA.data_ptr(),
+                               self.descB.data_ptr(), self.bestA.data_ptr(), self.bestB.data_ptr(),
+                               self.sqrA.data_ptr(), self.sqrB.data_ptr())
+
+
+def bf_match(tasks, stream=None):
+    """Reference-compatible bidirectional top-1 (launchBruteForceMatchIMMA)."""
+    lib = _lib.load()
+    arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+    _lib.check(lib.rsfm_bf_match(arr, len(tasks), _stream_ptr(stream)), "rsfm_bf_match")
+    return tasks
+
+
+def bf_match_ext(tasks, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08, stream=None):
+    """Bidirectional top-1 plus per-query second-best distance and ratio / cross-check flags."""
+    lib = _lib.load()
+    for t in tasks:
+        n = t.descA.shape[0]
+        if t.secondA is None or t.secondA.numel() != n:
+            t.secondA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+            t.flagsA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+    arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+    sec = (ctypes.c_void_p * len(tasks))(*[t.secondA.data_ptr() for t in tasks])
+    flg = (ctypes.c_void_p * len(tasks))(*[t.flagsA.data_ptr() for t in tasks])
+    _lib.check(lib.rsfm_bf_match_ext(arr, len(tasks), sec, flg, ratio_num, ratio_den, _stream_ptr(stream)),
+               "rsfm_bf_match_ext")
+    return tasks
+
+
+def unpack_best(best):
+    """int64 BestMatch view -> (index uint32 ndarray, distance uint32 ndarray)."""
+    a = best.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    return a[:, 0].copy(), a[:, 1].copy()
+
+
+def _valid_matches(buf, n):
+    out = np.frombuffer(buf, dtype=np.dtype([("idxQuery", "<u4"), ("idxTrain", "<u4"), ("distance", "<f4")]),
+                        count=n)
+    return out.copy()
+
+
+def cross_check_matches(fwd, bwd):
+    """fwd/bwd: uint32 arrays of shape [n, 2] (index, distance) on the host."""
+    lib = _lib.load()
+    fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
+    bwd = np.ascontiguousarray(bwd, dtype=np.uint32)
+    cap = max(1, min(len(fwd), len(bwd)))
+    buf = ctypes.create_string_buffer(12 * cap)
+    n = lib.rsfm_cross_check_matches(fwd.ctypes.data, len(fwd), bwd.ctypes.data, len(bwd), buf)
+    return _valid_matches(buf, n)
+
+
+def remove_match_conflicts(fwd, nb_train):
+    lib = _lib.load()
+    fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
+    cap = max(1, min(len(fwd), nb_train))
+    buf = ctypes.create_string_buffer(12 * cap)
+    n = lib.rsfm_remove_match_conflicts(fwd.ctypes.data, len(fwd), nb_train, buf)
+    return _valid_matches(buf, n)
+
+
+def device_error():
+    lib = _lib.load()
+    code = ctypes.c_uint32(0)
+    _lib.check(lib.rsfm_device_error(ctypes.byref(code)), "rsfm_device_error")
+    return code.value
+
+
+def last_launch_count():
+    return int(_lib.load().rsfm_last_launch_count())
+
+
+class BruteForceMatcher:
+    """Mirror of rsfm::BruteForceMatcher (bruteForceMatcher.h:28-102), brute-force method.
+
+    register_image() precomputes and keeps per-image squared norms (the reference's precompute
+    blob, bruteForceMatcher.cpp:63-107); match() returns per query image the (fwd, bwd) BestMatch
+    arrays; match_and_filter() applies crossCheckMatches or removeMatchConflicts on the host
+    (bruteForceMatcher.cpp:426-442).
+    """
+
+    def __init__(self, device="cuda"):
+        self.device = torch.device(device)
+        self._images = {}
+        self.stream = torch.cuda.Stream(device=self.device)
+
+    def register_image(self, handle, desc):
+        _check_desc(desc)
+        with torch.cuda.stream(self.stream):
+            self._images[handle] = (desc, precomp_sift_sqr_norm(desc, stream=self.stream))
+
+    def _tasks(self, queries, train):
+        dt, st = self._images[train]
+        return [BFTask(self._images[q][0], dt, self._images[q][1], st) for q in queries]
+
+    def match(self, queries, train):
+        if not queries:
+            return []
+        with torch.cuda.stream(self.stream):
+            tasks = bf_match(self._tasks(queries, train), stream=self.stream)
+        self.stream.synchronize()
+        return [(np.stack(unpack_best(t.bestA), 1), np.stack(unpack_best(t.bestB), 1)) for t in tasks]
+
+    def match_and_filter(self, queries, train, cross_check=True):
+        res = []
+        for fwd, bwd in self.match(queries, train):
+            res.append(cross_check_matches(fwd, bwd) if cross_check else remove_match_conflicts(fwd, len(bwd)))
+        return res

@@ -1,0 +1,41 @@
+"""Seeded synthetic SIFT-like descriptors (128 x uint8), as specified for the matcher workloads.
+
+Each descriptor: 128 half-normal(sigma=1) floats, L2-normalised, clipped at 0.2, renormalised,
+scaled by 512, rounded and clamped to [0, 255]. A train set holds noisy copies (add N(0, sigma),
+requantise to [0, 255]) of a fraction of the query descriptors in shuffled order; the rest are
+independent descriptors. Randomness: numpy.random.Generator(PCG64(seed)).
+"""
+import numpy as np
+
+
+def _sift_like(rng, n):
+    x = np.abs(rng.standard_normal((n, 128), dtype=np.float32))
+    x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+    np.minimum(x, 0.2, out=x)
+    x /= np.maximum(np.linalg.norm(x, axis=1, keepdims=True), 1e-12)
+    x *= 512.0
+    return np.clip(np.rint(x), 0, 255).astype(np.uint8)
+
+
+def make_pair(n_query, n_train, overlap, sigma, seed):
+    """Returns (query uint8[nq,128], train uint8[nt,128], truth int64[nt]).
+
+    truth[j] is the query index train descriptor j was copied from, or -1 for independent ones.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    q = _sift_like(rng, n_query)
+    n_copy = int(round(overlap * min(n_query, n_train)))
+    src = rng.choice(n_query, size=n_copy, replace=False) if n_copy > 0 else np.zeros(0, dtype=np.int64)
+    copies = q[src].astype(np.float32) + rng.normal(0.0, sigma, size=(n_copy, 128)).astype(np.float32)
+    copies = np.clip(np.rint(copies), 0, 255).astype(np.uint8)
+    indep = _sift_like(rng, n_train - n_copy)
+    t = np.concatenate([copies, indep], axis=0)
+    truth = np.concatenate([src.astype(np.int64), np.full(n_train - n_copy, -1, dtype=np.int64)])
+    perm = rng.permutation(n_train)
+    return q, t[perm], truth[perm]
+
+
+def uniform_bytes(n, seed):
+    """Uniform random bytes (the reference's kernel tests use uniform random 32-bit words)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return rng.integers(0, 256, size=(n, 128), dtype=np.uint8)

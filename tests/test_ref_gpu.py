@@ -1,0 +1,102 @@
+"""Bit-exact comparison with RapidSFM's own GPU kernels (built from the reference sources by
+oracle/build_ref.sh into oracle/_ref/). Pins the oracle and the CUDA product to the reference
+implementation itself, including its lowest-index tie-break."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from rapidsfm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref(oracle):
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref/librsfm_ref.so not built (needs the reference sources at build time)")
+    return oracle.load_ref()
+
+
+def _ref_bf(ref, a, b):
+    dA = torch.from_numpy(a).cuda()
+    dB = torch.from_numpy(b).cuda()
+    sA = torch.empty(len(a), dtype=torch.int32, device="cuda")
+    sB = torch.empty(len(b), dtype=torch.int32, device="cuda")
+    fwd = torch.empty(len(a), dtype=torch.int64, device="cuda")
+    bwd = torch.empty(len(b), dtype=torch.int64, device="cuda")
+    assert ref.ref_precomp_sqr_norm(ctypes.c_void_p(sA.data_ptr()), ctypes.c_void_p(dA.data_ptr()), len(a), None) == 0
+    assert ref.ref_precomp_sqr_norm(ctypes.c_void_p(sB.data_ptr()), ctypes.c_void_p(dB.data_ptr()), len(b), None) == 0
+    from rapidsfm_b200._lib import SiftBFTask
+    t = SiftBFTask(len(a), len(b), dA.data_ptr(), dB.data_ptr(), fwd.data_ptr(), bwd.data_ptr(), sA.data_ptr(),
+                   sB.data_ptr())
+    assert ref.ref_bf_match_imma(ctypes.byref(t), 1, None) == 0
+    torch.cuda.synchronize()
+    f = fwd.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    g = bwd.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    return f, g, sA.cpu().numpy().view(np.uint32)
+
+
+CASES = [
+    ("uniform_897", lambda: (synth.uniform_bytes(897, 1), synth.uniform_bytes(897, 2))),
+    ("sift_4096", lambda: synth.make_pair(4096, 4096, 0.6, 8.0, seed=0)[:2]),
+    ("ragged", lambda: synth.make_pair(1300, 333, 0.5, 6.0, seed=3)[:2]),
+]
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_bf_matches_reference_kernels(ref, rsfm, oracle, name, make):
+    a, b = make()
+    rf, rb, rs = _ref_bf(ref, a, b)
+    # the oracle reproduces the reference kernels exactly
+    ef, eb, _ = oracle.bf_match(a, b)
+    np.testing.assert_array_equal(rf, ef)
+    np.testing.assert_array_equal(rb, eb)
+    np.testing.assert_array_equal(rs, oracle.sqr_norm(a))
+    # and so does the B200 kernel
+    task = rsfm.BFTask(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    rsfm.bf_match([task])
+    torch.cuda.synchronize()
+    fi, fd = rsfm.unpack_best(task.bestA)
+    bi, bd = rsfm.unpack_best(task.bestB)
+    np.testing.assert_array_equal(np.stack([fi, fd], 1), rf)
+    np.testing.assert_array_equal(np.stack([bi, bd], 1), rb)
+
+
+def test_ties_match_reference_kernels(ref, rsfm):
+    base = synth.uniform_bytes(40, 3)
+    rng = np.random.default_rng(0)
+    a = np.ascontiguousarray(base[rng.integers(0, 40, 700)])
+    b = np.ascontiguousarray(base[rng.integers(0, 40, 900)])
+    rf, rb, _ = _ref_bf(ref, a, b)
+    task = rsfm.BFTask(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    rsfm.bf_match([task])
+    torch.cuda.synchronize()
+    fi, fd = rsfm.unpack_best(task.bestA)
+    bi, bd = rsfm.unpack_best(task.bestB)
+    np.testing.assert_array_equal(np.stack([fi, fd], 1), rf)
+    np.testing.assert_array_equal(np.stack([bi, bd], 1), rb)
+
+
+def test_host_filters_match_reference(ref, rsfm):
+    rng = np.random.default_rng(5)
+    nq, nt = 700, 500
+    fwd = np.stack([rng.integers(0, nt, nq), rng.integers(0, 5000, nq)], 1).astype(np.uint32)
+    bwd = np.stack([rng.integers(0, nq, nt), rng.integers(0, 5000, nt)], 1).astype(np.uint32)
+    for j in range(0, nt, 2):
+        i = rng.integers(0, nq)
+        fwd[i, 0] = j
+        bwd[j, 0] = i
+    buf = ctypes.create_string_buffer(12 * nt)
+    n = ref.ref_cross_check(fwd.ctypes.data, nq, bwd.ctypes.data, nt, buf)
+    exp = np.frombuffer(buf, dtype=np.dtype([("q", "<u4"), ("t", "<u4"), ("d", "<f4")]), count=n)
+    got = rsfm.cross_check_matches(fwd, bwd)
+    np.testing.assert_array_equal(got["idxQuery"], exp["q"])
+    np.testing.assert_array_equal(got["idxTrain"], exp["t"])
+    np.testing.assert_array_equal(got["distance"], exp["d"])
+    n = ref.ref_remove_match_conflicts(fwd.ctypes.data, nq, nt, buf)
+    exp = np.frombuffer(buf, dtype=np.dtype([("q", "<u4"), ("t", "<u4"), ("d", "<f4")]), count=n)
+    got = rsfm.remove_match_conflicts(fwd, nt)
+    np.testing.assert_array_equal(got["idxQuery"], exp["q"])
+    np.testing.assert_array_equal(got["idxTrain"], exp["t"])
