@@ -71,7 +71,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -79,7 +79,10 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, which):
+        setattr(self, which, time.perf_counter())
 
     def stop(self):
         if self.proc is None:
@@ -91,7 +94,11 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t_begin", 0.0), getattr(self, "t_end", float("inf"))
+        window = [ln for ts, ln in self.lines if t0 <= ts <= t1 + 0.06]
+        if not window and self.lines:  # region shorter than one sampling period: nearest sample
+            window = [min(self.lines, key=lambda x: abs(x[0] - t1))[1]]
+        for ln in window:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -127,10 +134,9 @@ def run_reference(args):
         return
     q, t, _ = synth.make_pair(N_QUERY, N_TRAIN, OVERLAP, SIGMA, seed=1)
     threads = os.cpu_count() or 1
-    rows = 256
-    # size the sample to ~10 s of CPU work per step at most
-    rate, dt = cpu_baseline(q, t, 32, threads)
-    rows = int(max(32, min(4096, rate * 5.0 / len(t))))
+    # size each step's sample to at most ~5 s of CPU work (the whole pair when it is faster)
+    rate, dt = cpu_baseline(q, t, 64, threads)
+    rows = int(max(64, min(N_QUERY, rate * 5.0 / len(t))))
     vals = []
     for _ in range(args.warmup):
         cpu_baseline(q, t, min(rows, 64), threads)
@@ -213,12 +219,16 @@ def run_ours(args):
     lib.rsfm_profile_enable(1)
     step_ms, launches = [], 0
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if sampler:
+        sampler.mark("t_begin")
     for i in range(args.steps):
         flush.fill_(i & 255)
         evs[i][0].record(stream)
         launches += step()
         evs[i][1].record(stream)
     torch.cuda.synchronize()
+    if sampler:
+        sampler.mark("t_end")
     kms = ctypes.c_float(0)
     klaunch = ctypes.c_uint32(0)
     R._lib.check(lib.rsfm_profile_collect(ctypes.byref(kms), ctypes.byref(klaunch)), "rsfm_profile_collect")
@@ -300,10 +310,10 @@ def run_ours(args):
         "ops_per_launch": nops,
     }
 
-    # ---- CPU baseline: oracle port on a bounded row sample (~10 s)
+    # ---- CPU baseline: oracle port, all host threads, on as many query rows as fit in ~10 s
     threads = os.cpu_count() or 1
-    rate, _ = cpu_baseline(q, t, 32, threads)
-    rows = int(max(32, min(4096, rate * 8.0 / N_TRAIN)))
+    rate, _ = cpu_baseline(q, t, 64, threads)
+    rows = int(max(64, min(N_QUERY, rate * 10.0 / N_TRAIN)))
     cpu_val, cpu_dt = cpu_baseline(q, t, rows, threads)
 
     line = {
@@ -337,8 +347,8 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     if args.impl == "reference":

@@ -78,6 +78,23 @@ int rsfm_bf_match(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t s
 int rsfm_bf_match_ext(const rsfm_sift_bf_task* tasks, size_t nbTasks, uint32_t* const* secondDistA,
                       uint32_t* const* flagsA, uint32_t ratioNum, uint32_t ratioDen, cudaStream_t stream);
 
+/* Batched plans (no reference counterpart): many uneven pairs matched by ONE persistent launch
+ * over all (pair, row block, column range) units, captured once in a CUDA graph and replayed.
+ * Same outputs as rsfm_bf_match_ext. The plan keeps the pointers given at creation; descriptor
+ * tensor maps are encoded once. Options: 0 = automatic. */
+typedef struct rsfm_bf_plan rsfm_bf_plan;
+typedef struct rsfm_bf_plan_options {
+    uint32_t rowTiles;        /* 128-row tiles per work unit (1..8) */
+    uint32_t colBlocks;       /* 128-column blocks per work unit */
+    uint32_t epilogueGroups;  /* epilogue warpgroups per CTA: 2 or 4 */
+    uint32_t useGraph;        /* capture the launches in a CUDA graph */
+} rsfm_bf_plan_options;
+int rsfm_bf_plan_create(const rsfm_sift_bf_task* tasks, size_t nbTasks, uint32_t* const* secondDistA,
+                        uint32_t* const* flagsA, uint32_t ratioNum, uint32_t ratioDen,
+                        const rsfm_bf_plan_options* options, rsfm_bf_plan** plan);
+int rsfm_bf_plan_launch(rsfm_bf_plan* plan, cudaStream_t stream);
+int rsfm_bf_plan_destroy(rsfm_bf_plan* plan);
+
 /* Replaces crossCheckMatches (bruteForceMatch.h:126-127, bruteForceMatch.cpp:23-40). Host
  * memory in and out; `out` must hold min(nbQueryDesc, nbTrainDesc) entries. Returns the count. */
 size_t rsfm_cross_check_matches(const rsfm_best_match* matches, uint32_t nbQueryDesc,
@@ -88,12 +105,120 @@ size_t rsfm_cross_check_matches(const rsfm_best_match* matches, uint32_t nbQuery
 size_t rsfm_remove_match_conflicts(const rsfm_best_match* matches, uint32_t nbQueryDesc, uint32_t nbTrainDesc,
                                    rsfm_valid_match* out);
 
+/* ---------------------------------------------------------------- cascade hash
+ * Descriptors are nbDesc x 128 uint8, 16-byte aligned. Weights are nbChannels x 128 int8 rows
+ * (the reference's KArray<int32_t, 32> per channel), 16-byte aligned; 64 channels give the 8
+ * bucket-key bytes, 192 add the 128-bit remap code. All outputs are device memory. */
+
+/* Replaces cashash::accumuateDesc (casHash/cascadeHash.h:32, accumulateDesc.cu:120-131):
+ * acc[d] (+)= sum_i (desc[i][d] >> 1), 128 x uint64; zeroed first when initAcc != 0. */
+int rsfm_cashash_accumulate_desc(unsigned long long* acc, int initAcc, const void* desc, uint32_t nbDesc,
+                                 cudaStream_t stream);
+
+/* Replaces cashash::computeBias (cascadeHash.h:33-35, accumulateDesc.cu:176-182):
+ * bias[c] = round(-(sum_d W[c][d] acc[d]) / nbDesc) + biasBase[c], evaluated exactly (round half
+ * away from zero); the reference's fast-math float evaluation agrees within +-1, the tolerance of
+ * its own test (test/casHashAccumulateDescTest.cpp:188). */
+int rsfm_cashash_compute_bias(int32_t* bias, const void* weights, const int32_t* biasBase,
+                              const unsigned long long* acc, unsigned long long nbDesc, int nbChannels,
+                              cudaStream_t stream);
+
+/* Replaces cashash::computeHashForBucketOnly (nbChannels = 64) and computeHashForBucketAndRemap
+ * (nbChannels = 192) (cascadeHash.h:43-56, computeHash.cu:474-520). Bit c of descriptor i is
+ * [bias[c] + sum_d W[c][d] (desc[i][d] >> 1) >= 0]; bucketIndices[i][s] = bits 8s..8s+7,
+ * remap[i][w] = bits 64+32w..64+32w+31. histogram (8 x 256, optional) is zeroed and filled. */
+int rsfm_cashash_compute_hash(const void* weights, const int32_t* bias, int nbChannels, const void* desc,
+                              uint32_t nbDesc, uint8_t* bucketIndices, uint32_t* remap, uint32_t* histogram,
+                              cudaStream_t stream);
+
+/* Replaces cashash::buildHistogram (cascadeHash.h:58-60, buildBuckets.cu:107-114). */
+int rsfm_cashash_build_histogram(uint32_t* histogram, const uint8_t* bucketIndices, uint32_t nbDesc,
+                                 cudaStream_t stream);
+
+/* Replaces cashash::computeBucketBound (cascadeHash.h:62-63, buildBuckets.cu:169-172): lower =
+ * exclusive and upper = inclusive prefix sums per scheme; *maxBucketSize (device-accessible,
+ * e.g. pinned host memory) = largest bucket over all schemes. */
+int rsfm_cashash_compute_bucket_bound(uint32_t* lower, uint32_t* upper, uint32_t* maxBucketSize,
+                                      const uint32_t* histogram, cudaStream_t stream);
+
+/* Replaces cashash::buildBuckets (cascadeHash.h:65-68, buildBuckets.cu:262-269): buckets[s*nbDesc
+ * + slot] lists the members of every bucket; idxAllocator enters as the lower bounds and leaves as
+ * the upper bounds. Members are in ascending descriptor order (deterministic). Allocates
+ * stream-ordered scratch of 8 KiB per 1024 descriptors. */
+int rsfm_cashash_build_buckets(const uint8_t* bucketIndices, uint32_t nbDesc, uint32_t* idxAllocator,
+                               uint32_t* buckets, cudaStream_t stream);
+
+/* cashash::ImageDesc (casHash/cascadeHash.h:69-97): descriptors, bucketEnds [8][256] (inclusive
+ * upper bounds per scheme, bucketEnds[0][255] = nbDesc), bucket member lists, squared norms. */
+typedef struct rsfm_cashash_image {
+    const void* desc;
+    const uint32_t* bucketEnds;
+    const uint32_t* buckets;
+    const uint32_t* sqrNormDesc;
+} rsfm_cashash_image;
+
+/* cashash::MatchResult (cascadeHash.h:100-104): per query descriptor the best train match, per
+ * train descriptor the best query match (train may be NULL for one direction only). */
+typedef struct rsfm_cashash_result {
+    rsfm_best_match* query;
+    rsfm_best_match* train;
+} rsfm_cashash_result;
+
+/* Replaces cashash::findBestMatch (cascadeHash.h:106-107, findBestMatch.cu:654-676). queries,
+ * querySize, results and maxQueryBucketSize are host arrays of nbTasks entries (all tasks share
+ * the train image). Results are initialised to {~0u, ~0u}, then every (query, train) pair that
+ * shares a bucket is scored by exact L2 and the lexicographic minimum of (distance, index) is kept
+ * in both directions. Bucket lists are read exactly as the reference reads them: the list of
+ * bucket (s, b) starts at buckets[bucketBeg(s, b)] (cascadeHash.h:82-85, findBestMatch.cu:609-610),
+ * i.e. without a per-scheme offset. Equal distances go to the lowest index. */
+int rsfm_cashash_find_best_match(const rsfm_cashash_image* queries, const uint32_t* querySize,
+                                 const rsfm_cashash_image* train, uint32_t trainSize,
+                                 const rsfm_cashash_result* results, uint32_t nbTasks,
+                                 const uint32_t* maxQueryBucketSize, uint32_t maxTrainBucketSize,
+                                 cudaStream_t stream);
+
+/* rsfm_cashash_find_best_match with options (no reference counterpart).
+ * RSFM_CASHASH_PER_SCHEME_LISTS: read bucket (s, b) from buckets[s * nbDesc + bucketBeg(s, b)],
+ * the layout buildBuckets writes (buildBuckets.cu:257), so every scheme matches its own buckets. */
+#define RSFM_CASHASH_PER_SCHEME_LISTS 1u
+int rsfm_cashash_find_best_match_ex(const rsfm_cashash_image* queries, const uint32_t* querySize,
+                                    const rsfm_cashash_image* train, uint32_t trainSize,
+                                    const rsfm_cashash_result* results, uint32_t nbTasks, uint32_t flags,
+                                    cudaStream_t stream);
+
+/* Image for ranked cascade-hash matching (no reference counterpart): keys = 8 bucket-key bytes
+ * per descriptor and codes = the 128-bit remap code (rsfm_cashash_compute_hash with 192
+ * channels, or the learned hash), bucket lists per scheme at buckets[s * nbDesc + lower(s, b)]
+ * (rsfm_cashash_build_buckets), squared norms. */
+typedef struct rsfm_ranked_image {
+    const void* desc;
+    const uint8_t* keys;
+    const uint32_t* codes;
+    const uint32_t* bucketEnds;
+    const uint32_t* buckets;
+    const uint32_t* sqrNormDesc;
+    uint32_t nbDesc;
+} rsfm_ranked_image;
+
+/* Ranked cascade-hash matching (no reference counterpart): for every query descriptor, the
+ * candidates are the train descriptors sharing one of the first nbTables bucket keys; they are
+ * ranked by Hamming distance of the codes (ties: lower index), the first topK (<= 32) are scored
+ * by exact L2. best[i] = lexicographic min (distance, index) among them, secondDist[i] = smallest
+ * distance among the others (~0u if none), flags bit0 = ratioDen*best < ratioNum*second,
+ * nbCandidates[i] (optional) = distinct candidates. train->nbDesc must be < 2^24. */
+int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const rsfm_ranked_image* train, uint32_t nbTables,
+                              uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, rsfm_best_match* best,
+                              uint32_t* secondDist, uint32_t* flags, uint32_t* nbCandidates, cudaStream_t stream);
+
 /* Reads and clears the device-side error word of the current device (synchronizes the device).
  * 0 = no error; nonzero = a kernel's bounded wait timed out (code identifies the wait). */
 int rsfm_device_error(uint32_t* code);
 
 /* Human-readable text for an rsfm_status. */
 const char* rsfm_status_string(int status);
+
+/* Text of the last CUDA error an rsfm_* call on this host thread returned RSFM_ERR_CUDA for. */
+const char* rsfm_last_cuda_error(void);
 
 /* Number of kernels the last rsfm_* call on this host thread enqueued (for launch accounting). */
 uint32_t rsfm_last_launch_count(void);

@@ -43,7 +43,7 @@ def load():
         "orc_cashash_histogram": (None, [_P, u32, _P]),
         "orc_cashash_bucket_bounds": (u32, [_P, _P, _P]),
         "orc_cashash_build_buckets": (None, [_P, u32, _P, _P]),
-        "orc_cashash_find_best_match": (None, [_P, u32, _P, _P, _P, u32, _P, _P, _P, _P]),
+        "orc_cashash_find_best_match": (None, [_P, u32, _P, _P, _P, u32, _P, _P, _P, _P, ctypes.c_int]),
         "orc_cashash_match_ranked": (None, [_P, _P, _P, u32, _P, _P, _P, u32, i32, i32, u32, u32, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
@@ -159,7 +159,7 @@ def cashash_buckets(keys):
     return hist, lower, upper, int(mx), buckets[:, :n]
 
 
-def cashash_find_best_match(q_desc, q_upper, q_buckets, t_desc, t_upper, t_buckets):
+def cashash_find_best_match(q_desc, q_upper, q_buckets, t_desc, t_upper, t_buckets, per_scheme=False):
     q_desc = np.ascontiguousarray(q_desc, dtype=np.uint8)
     t_desc = np.ascontiguousarray(t_desc, dtype=np.uint8)
     q_upper = np.ascontiguousarray(q_upper, dtype=np.uint32)
@@ -169,7 +169,7 @@ def cashash_find_best_match(q_desc, q_upper, q_buckets, t_desc, t_upper, t_bucke
     qb = np.empty((len(q_desc), 2), dtype=np.uint32)
     tb = np.empty((len(t_desc), 2), dtype=np.uint32)
     load().orc_cashash_find_best_match(_c(q_desc), len(q_desc), _c(q_upper), _c(q_buckets), _c(t_desc),
-                                       len(t_desc), _c(t_upper), _c(t_buckets), _c(qb), _c(tb))
+                                       len(t_desc), _c(t_upper), _c(t_buckets), _c(qb), _c(tb), int(per_scheme))
     return qb, tb
 
 

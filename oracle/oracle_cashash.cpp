@@ -160,20 +160,23 @@ static inline uint32_t l2sqr(const uint8_t* a, const uint8_t* b) {
     return uint32_t(acc);
 }
 
-// findBestMatch (reference mode): query image vs train image, each described by descriptors,
-// bucketEnds [8][256] (inclusive upper bounds) and bucket lists [8][n].
+// findBestMatch: query image vs train image, each described by descriptors, bucketEnds [8][256]
+// (inclusive upper bounds) and bucket lists. perScheme = 0 reads bucket (s, b) at
+// buckets[bucketBeg(s, b)] exactly as the reference does (findBestMatch.cu:609-610 with
+// cascadeHash.h:82-85, and its CPU check test/casHashFindBestMatchTest.cpp:148-149);
+// perScheme = 1 reads it at buckets[s*n + bucketBeg(s, b)], where buildBuckets puts it.
 void orc_cashash_find_best_match(const uint8_t* qDesc, uint32_t nq, const uint32_t* qEnds, const uint32_t* qBuckets,
                                  const uint8_t* tDesc, uint32_t nt, const uint32_t* tEnds, const uint32_t* tBuckets,
-                                 OrcBestMatch* qBest, OrcBestMatch* tBest) {
+                                 OrcBestMatch* qBest, OrcBestMatch* tBest, int perScheme) {
     std::vector<uint64_t> qk(nq, ~0ull), tk(nt, ~0ull);
     for (int s = 0; s < 8; s++)
         for (int b = 0; b < 256; b++) {
             const uint32_t qb = b ? qEnds[s * 256 + b - 1] : 0, qe = qEnds[s * 256 + b];
             const uint32_t tb = b ? tEnds[s * 256 + b - 1] : 0, te = tEnds[s * 256 + b];
             for (uint32_t x = qb; x < qe; x++) {
-                const uint32_t i = qBuckets[size_t(s) * nq + x];
+                const uint32_t i = qBuckets[size_t(s) * nq * perScheme + x];
                 for (uint32_t y = tb; y < te; y++) {
-                    const uint32_t j = tBuckets[size_t(s) * nt + y];
+                    const uint32_t j = tBuckets[size_t(s) * nt * perScheme + y];
                     const uint64_t d = l2sqr(qDesc + size_t(i) * 128, tDesc + size_t(j) * 128);
                     qk[i] = std::min(qk[i], (d << 32) | j);
                     tk[j] = std::min(tk[j], (d << 32) | i);

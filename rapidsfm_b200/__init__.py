@@ -5,6 +5,7 @@ include/rsfm_b200.h; this package is the Python host side (ctypes + torch device
 """
 from . import _lib  # noqa: F401
 from .matcher import (  # noqa: F401
+    BFPlan,
     BFTask,
     BruteForceMatcher,
     bf_match,

@@ -45,6 +45,28 @@ class SiftBFTask(ctypes.Structure):
     ]
 
 
+class CasHashImage(ctypes.Structure):
+    """cashash::ImageDesc (casHash/cascadeHash.h:69-97)."""
+    _fields_ = [("desc", ctypes.c_void_p), ("bucketEnds", ctypes.c_void_p), ("buckets", ctypes.c_void_p),
+                ("sqrNormDesc", ctypes.c_void_p)]
+
+
+class CasHashResult(ctypes.Structure):
+    """cashash::MatchResult (casHash/cascadeHash.h:100-104)."""
+    _fields_ = [("query", ctypes.c_void_p), ("train", ctypes.c_void_p)]
+
+
+class RankedImage(ctypes.Structure):
+    _fields_ = [("desc", ctypes.c_void_p), ("keys", ctypes.c_void_p), ("codes", ctypes.c_void_p),
+                ("bucketEnds", ctypes.c_void_p), ("buckets", ctypes.c_void_p), ("sqrNormDesc", ctypes.c_void_p),
+                ("nbDesc", ctypes.c_uint32)]
+
+
+class BFPlanOptions(ctypes.Structure):
+    _fields_ = [("rowTiles", ctypes.c_uint32), ("colBlocks", ctypes.c_uint32), ("epilogueGroups", ctypes.c_uint32),
+                ("useGraph", ctypes.c_uint32)]
+
+
 class ValidMatch(ctypes.Structure):
     """ValidMatch (bruteForceMatch.h:120-125)."""
     _fields_ = [("idxQuery", ctypes.c_uint32), ("idxTrain", ctypes.c_uint32), ("distance", ctypes.c_float)]
@@ -63,7 +85,38 @@ SIGNATURES = {
                                                       ctypes.c_void_p]),
     "rsfm_device_error": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32)]),
     "rsfm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "rsfm_last_cuda_error": (ctypes.c_char_p, []),
     "rsfm_last_launch_count": (ctypes.c_uint32, []),
+    "rsfm_cashash_accumulate_desc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                                    ctypes.c_void_p]),
+    "rsfm_cashash_compute_bias": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    "rsfm_cashash_compute_hash": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                 ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+    "rsfm_cashash_build_histogram": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_cashash_compute_bucket_bound": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_cashash_build_buckets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p]),
+    "rsfm_cashash_find_best_match": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,
+                                                    ctypes.POINTER(CasHashImage), ctypes.c_uint32,
+                                                    ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_void_p,
+                                                    ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,
+                                                       ctypes.POINTER(CasHashImage), ctypes.c_uint32,
+                                                       ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_uint32,
+                                                       ctypes.c_void_p]),
+    "rsfm_cashash_match_ranked": (ctypes.c_int, [ctypes.POINTER(RankedImage), ctypes.POINTER(RankedImage),
+                                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+    "rsfm_bf_plan_create": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(BFPlanOptions),
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "rsfm_bf_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_bf_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "rsfm_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)]),
     "rsfm_int8_mma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
@@ -91,4 +144,7 @@ def load():
 
 def check(status, what):
     if status != RSFM_OK:
-        raise RsfmError(status, what)
+        detail = ""
+        if status == 3 and _lib is not None:
+            detail = " [" + _lib.rsfm_last_cuda_error().decode(errors="replace") + "]"
+        raise RsfmError(status, what + detail)

@@ -18,6 +18,9 @@ SOURCES = [
     "bf_match.cu",
     "host_filters.cpp",
     "diag.cu",
+    "cashash.cu",
+    "cashash_match.cu",
+    "cashash_ranked.cu",
 ]
 
 NVCC_FLAGS = [

@@ -16,15 +16,16 @@
 //   warp 0      TMA producer: A row tiles (resident for the unit), B column blocks (3-stage ring)
 //   warp 1      TMEM allocator and UMMA issuer (one thread): per (B block, A row tile) one
 //               128x128x128 int8 product into a double-buffered TMEM accumulator
-//   warps 2..9  epilogue, two warpgroups; warpgroup w owns columns [64w, 64w+64) of every tile
-// The epilogue keeps, per warpgroup, a TMEM "column accumulator" holding for each (lane, column)
-// the best packed column key over the unit's row tiles, so the cross-lane column reduction runs
-// once per B block instead of once per tile. Row minima are thread-local (one TMEM lane = one A
-// row). The row second-best is tracked exactly only for chunks whose minimum can still enter the
-// row's global top-2 (threshold = running global second-best, read from the output at unit start).
+//   warps 2..17 epilogue, four warpgroups; warpgroup w owns columns [32w, 32w+32) of every tile
+// Each epilogue thread owns one TMEM lane (one A row of the tile). It keeps, in registers, a
+// column accumulator holding for each of its 32 columns the best packed column key over the
+// unit's row tiles, so the cross-lane column reduction runs once per B block instead of once per
+// tile. Row minima are thread-local; the exact row second-best needs per-chunk work only for
+// chunks that can still become the row's best.
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 namespace rsfm_b200 {
@@ -36,7 +37,14 @@ constexpr int kMaxTasksPerLaunch = 16;
 constexpr int kMaxRowTiles = 8;        // A row tiles per unit (p fits 3 bits of the column key)
 constexpr int kBStages = 3;
 constexpr int kTileBytes = 128 * 128;  // 128 descriptors x 128 bytes
-constexpr int kThreads = 320;
+// Epilogue warpgroups kWG in {2, 4}: warpgroup w owns 128/kWG columns of every tile, i.e.
+// kCPW = 4/kWG chunks of 32 columns per warp.
+template <int kWG>
+struct Cfg {
+    static constexpr int kEpiWarps = 4 * kWG;
+    static constexpr int kThreads = 32 * (2 + kEpiWarps);
+    static constexpr int kCPW = 4 / kWG;
+};
 constexpr uint32_t kMaxDist = 128u * 255u * 255u;  // largest possible squared L2 of uint8x128
 constexpr uint32_t kVBias = 1u << 23;                // makes (|b|^2 - d) + bias positive
 
@@ -48,6 +56,7 @@ struct alignas(64) TaskDev {
     unsigned long long* bestA;  // rsfm_best_match viewed as (distance << 32 | index)
     unsigned long long* bestB;
     uint32_t* secondA;
+    uint32_t* flagsA;  // batched plans only (the per-call path passes flags separately)
     uint32_t nA, nB;
     uint32_t rowBlocks, colRanges;
     uint32_t unitBegin;
@@ -55,9 +64,10 @@ struct alignas(64) TaskDev {
 
 struct Params {
     TaskDev tasks[kMaxTasksPerLaunch];
+    const TaskDev* gtasks;  // when non-null: any number of tasks, in global memory
     uint32_t nTasks;
     uint32_t totalUnits;
-    uint32_t rowTiles;  // row tiles per unit (even, <= kMaxRowTiles)
+    uint32_t rowTiles;  // row tiles per unit (<= kMaxRowTiles)
     uint32_t colBlocks; // 128-column blocks per unit
     uint32_t* err;
 };
@@ -66,10 +76,24 @@ struct Unit {
     uint32_t task, r0, c0, pt, cb;
 };
 
+__device__ __forceinline__ const TaskDev& task_of(const Params& P, uint32_t t) {
+    return P.gtasks ? P.gtasks[t] : P.tasks[t];
+}
+
 __device__ __forceinline__ Unit decode_unit(const Params& P, uint32_t u) {
     uint32_t t = 0;
-    while (t + 1 < P.nTasks && u >= P.tasks[t + 1].unitBegin) ++t;
-    const TaskDev& T = P.tasks[t];
+    if (P.gtasks) {  // last task whose first unit is <= u
+        uint32_t lo = 0, hi = P.nTasks - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (P.gtasks[mid].unitBegin <= u) lo = mid; else hi = mid - 1;
+        }
+        t = lo;
+        while (t + 1 < P.nTasks && P.gtasks[t + 1].unitBegin <= u) ++t;
+    } else {
+        while (t + 1 < P.nTasks && u >= P.tasks[t + 1].unitBegin) ++t;
+    }
+    const TaskDev& T = task_of(P, t);
     const uint32_t local = u - T.unitBegin;
     const uint32_t cr = local / T.rowBlocks;
     const uint32_t rb = local - cr * T.rowBlocks;
@@ -78,8 +102,7 @@ __device__ __forceinline__ Unit decode_unit(const Params& P, uint32_t u) {
     U.r0 = rb * 128u * P.rowTiles;
     U.c0 = cr * 128u * P.colBlocks;
     uint32_t pt = (T.nA - U.r0 + 127u) / 128u;
-    pt = pt < P.rowTiles ? pt : P.rowTiles;
-    U.pt = (pt + 1u) & ~1u;
+    U.pt = pt < P.rowTiles ? pt : P.rowTiles;
     uint32_t cb = (T.nB - U.c0 + 127u) / 128u;
     U.cb = cb < P.colBlocks ? cb : P.colBlocks;
     return U;
@@ -89,8 +112,10 @@ struct Smem {
     // A row tiles and B stages are 1024-byte aligned (128-byte swizzle atoms).
     uint8_t a[kMaxRowTiles][kTileBytes];
     uint8_t b[kBStages][kTileBytes];
-    uint32_t nbk[2][2][64];                 // [block parity][warpgroup][column]: |b_j|^2 << 8
-    unsigned long long colmin[2][2][64];    // [flush parity][warpgroup][column]
+    uint32_t nbk[2][128];                        // [block parity][column]: row-key addend
+    unsigned long long colmin[2][128];           // [flush parity][column]
+    unsigned long long rowbest[2][kMaxRowTiles * 128];  // [unit parity][row]: (d << 32 | j)
+    uint32_t rowsecond[2][kMaxRowTiles * 128];
     uint64_t aFull[kMaxRowTiles], aEmpty[kMaxRowTiles];
     uint64_t bFull[kBStages], bEmpty[kBStages];
     uint64_t accFull[2], accEmpty[2];
@@ -107,7 +132,11 @@ __device__ __forceinline__ int redux_max_s32(int v) {
     return r;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_constant__ Params P) {
+template <int kWG>
+__global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const __grid_constant__ Params P) {
+    constexpr int kEpiWarps = Cfg<kWG>::kEpiWarps;
+    constexpr int kThreads = Cfg<kWG>::kThreads;
+    constexpr int kCPW = Cfg<kWG>::kCPW;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t warp = threadIdx.x >> 5;
@@ -124,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(&S.accFull[s], 1);
-            mbar_init(&S.accEmpty[s], 8);
+            mbar_init(&S.accEmpty[s], kEpiWarps);
         }
         mbar_init(&S.mmaDone, 1);
         fence_mbar_init();
@@ -133,8 +162,11 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
         tmem_alloc(&S.tmemBase, 512);
         tmem_relinquish();
     }
-    static_assert(sizeof(S.colmin) / sizeof(S.colmin[0][0][0]) <= kThreads, "one thread per entry");
-    if (threadIdx.x < sizeof(S.colmin) / sizeof(S.colmin[0][0][0])) (&S.colmin[0][0][0])[threadIdx.x] = ~0ull;
+    for (uint32_t x = threadIdx.x; x < 2 * 128; x += kThreads) (&S.colmin[0][0])[x] = ~0ull;
+    for (uint32_t x = threadIdx.x; x < 2 * kMaxRowTiles * 128; x += kThreads) {
+        (&S.rowbest[0][0])[x] = ~0ull;
+        (&S.rowsecond[0][0])[x] = ~0u;
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -148,7 +180,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
             uint32_t aUse = 0;  // bit p: parity of loads issued into A slot p
             uint32_t stage = 0, bPhase = 0;
             auto loadA = [&](const Unit& U) {
-                const TaskDev& T = P.tasks[U.task];
+                const TaskDev& T = task_of(P, U.task);
                 for (uint32_t p = 0; p < U.pt; ++p) {
                     const uint32_t par = ((aUse >> p) & 1u) ^ 1u;
                     if (!mbar_wait(&S.aEmpty[p], par, err, kDevTimeoutTmaEmpty)) ok = false;
@@ -160,13 +192,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
             uint32_t u = blockIdx.x;
             if (u < P.totalUnits) {
                 const Unit U0 = decode_unit(P, u);
-                tma_prefetch_desc(&P.tasks[U0.task].tmA);
-                tma_prefetch_desc(&P.tasks[U0.task].tmB);
+                tma_prefetch_desc(&task_of(P, U0.task).tmA);
+                tma_prefetch_desc(&task_of(P, U0.task).tmB);
                 loadA(U0);
             }
             for (; u < P.totalUnits; u += gridDim.x) {
                 const Unit U = decode_unit(P, u);
-                const TaskDev& T = P.tasks[U.task];
+                const TaskDev& T = task_of(P, U.task);
                 for (uint32_t b = 0; b < U.cb; ++b) {
                     if (!mbar_wait(&S.bEmpty[stage], bPhase ^ 1u, err, kDevTimeoutTmaEmpty)) ok = false;
                     mbar_arrive_expect_tx(&S.bFull[stage], kTileBytes);
@@ -214,109 +246,125 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const uint32_t wg = (warp - 2u) >> 2;           // warpgroup: column half
+        // Keys are kept in "max is better" form so that the x512 scaling is a shift-add:
+        //   column key  ck = (2 a.b - |a|^2) * 256 + (7 - p)
+        //   row key     rk = ck - |b|^2 * 256 + (31 - k) * 8 = -d * 256 + (31 - k) * 8 + (7 - p)
+        // (p = row tile within the unit, k = column within the 32-column chunk). For a column, a
+        // larger ck means a smaller d, ties going to the smaller row tile; at the column flush the
+        // lane (row within the tile) is packed into bits 3..7 before the cross-lane maximum. For a
+        // row, a chunk's maximum rk gives the chunk's minimum d and, in its low bits, its lowest
+        // column.
+        //
+        // Row state per (thread, row tile), in row-key space: l1k/l1j = best key and its column,
+        // l2k = second key (only its distance matters), tk = slow-path threshold. A chunk does
+        // extra work only if its minimum could become this unit's best AND can still tie or beat
+        // the global best so far (read from bestA, refreshed every B block); every other chunk
+        // contributes its minimum to the second-best value only. This is exact: a chunk that
+        // cannot hold the best holds at most one value that matters, its minimum.
+        const uint32_t e = warp - 2u;                    // epilogue warp
+        const uint32_t wg = e >> 2;                      // warpgroup: columns [32 kCPW wg, +32 kCPW)
         const uint32_t q = warp & 3u;                    // TMEM lane quarter
-        const uint32_t t128 = ((warp - 2u) & 3u) * 32u + lane;
+        const uint32_t t512 = e * 32u + lane;
+        const uint32_t t128 = (e & 3u) * 32u + lane;
         const uint32_t laneBase = (32u * q) << 16;
-        const uint32_t colAccCol = 256u + 64u * wg;
-        uint32_t acc = 0, blk = 0;
-        for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x) {
+        uint32_t acc = 0, blk = 0, unitPar = 0;
+        for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x, unitPar ^= 1u) {
             const Unit U = decode_unit(P, u);
-            const TaskDev& T = P.tasks[U.task];
-            // Keys are kept in "max is better" form so that the x512 scaling is a shift-add:
-            //   column key  ck = (2 a.b - |a|^2) * 256 + hi,  hi = 255 - ((p << 5) | lane)
-            //   row key     rk = ck - |b|^2 * 256 = -d * 256 + hi
-            // Larger ck means smaller d for the column; ties prefer the smaller (p, lane), i.e. the
-            // smaller row index. A chunk's maximum row key gives the chunk's minimum distance.
-            //
-            // Row state per (thread, row tile), in row-key space: l1k/l1j = best key and its column,
-            // l2k = second key (value only), tk = slow-path threshold. A chunk enters the exact slow
-            // path only if its minimum could become this unit's best AND can still tie or beat the
-            // global best so far (read from bestA at unit start); every other chunk contributes its
-            // minimum to the second-best value only (exact: a chunk that cannot hold the best holds
-            // at most one relevant value, its minimum).
+            const TaskDev& T = task_of(P, U.task);
             int32_t rowc[kMaxRowTiles], tk[kMaxRowTiles], l1k[kMaxRowTiles], l2k[kMaxRowTiles];
             uint32_t l1j[kMaxRowTiles];
 #pragma unroll
             for (int p = 0; p < kMaxRowTiles; ++p) {
                 const uint32_t i = U.r0 + 128u * p + 32u * q + lane;
-                const int32_t hi = 255 - ((p << 5) | int32_t(lane));
                 const bool valid = (uint32_t(p) < U.pt) && (i < T.nA);
-                rowc[p] = valid ? int32_t(uint32_t(hi) - (T.sqrA[i] << 8)) : (INT32_MIN + hi);
-                const uint32_t h1 = valid ? min(uint32_t(__ldcg(&T.bestA[i]) >> 32), kMaxDist) : 0u;
-                tk[p] = valid ? int32_t(uint32_t(hi) - (h1 << 8)) : INT32_MAX;
+                rowc[p] = valid ? int32_t(uint32_t(7 - p) - (T.sqrA[i] << 8)) : (INT32_MIN + 7 - p);
+                tk[p] = valid ? INT32_MIN : INT32_MAX;
                 l1k[p] = INT32_MIN;
                 l2k[p] = INT32_MIN;
                 l1j[p] = ~0u;
             }
             for (uint32_t b = 0; b < U.cb; ++b, ++blk) {
                 const uint32_t bpar = blk & 1u;
-                const uint32_t colBase = U.c0 + 128u * b + 64u * wg;
-                if (t128 < 64) {
-                    const uint32_t j = colBase + t128;
-                    S.nbk[bpar][wg][t128] = j < T.nB ? (0u - (T.sqrB[j] << 8)) : 0u;
+                const uint32_t blockBase = U.c0 + 128u * b;
+                const uint32_t jw = blockBase + 32u * kCPW * wg;  // first column of this warp
+                if (t512 < 128) {
+                    const uint32_t j = blockBase + t512;
+                    S.nbk[bpar][t512] = j < T.nB ? (((31u - (j & 31u)) << 3) - (T.sqrB[j] << 8)) : 0u;
                 }
-                named_bar(1 + wg, 128);
+                // Refresh the slow-path thresholds from the global best so far.
+#pragma unroll
+                for (int p = 0; p < kMaxRowTiles; ++p) {
+                    const uint32_t i = U.r0 + 128u * p + 32u * q + lane;
+                    if (uint32_t(p) < U.pt && i < T.nA) {
+                        const uint32_t h1 = min(uint32_t(__ldcg(&T.bestA[i]) >> 32), kMaxDist);
+                        tk[p] = max(tk[p], int32_t(0u - (h1 << 8)));
+                    }
+                }
+                named_bar(1, 32 * kEpiWarps);
+                int32_t ca[32 * kCPW];
+#pragma unroll
+                for (int k = 0; k < 32 * kCPW; ++k) ca[k] = INT32_MIN;
 #pragma unroll 1
                 for (uint32_t p = 0; p < U.pt; ++p) {
-                    const uint32_t buf = acc & 1u;
-                    if (!mbar_wait(&S.accFull[buf], (acc >> 1) & 1u, err, kDevTimeoutAccFull)) ok = false;
-                    tc_fence_after();
                     const int32_t rowcP = rowc[p];
                     int32_t tkP = tk[p], l1kP = l1k[p], l2kP = l2k[p];
                     uint32_t l1jP = l1j[p];
+                    const uint32_t buf = acc & 1u;
+                    if (!mbar_wait(&S.accFull[buf], (acc >> 1) & 1u, err, kDevTimeoutAccFull)) ok = false;
+                    tc_fence_after();
+                    uint32_t x[32 * kCPW];
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        const uint32_t j0 = colBase + 32u * c;
-                        uint32_t x[32], ca[32];
-                        tmem_ld32(tmem + laneBase + buf * 128u + 64u * wg + 32u * c, x);
-                        if (p > 0) tmem_ld32(tmem + laneBase + colAccCol + 32u * c, ca);
-                        tmem_wait_ld();
-                        if (p == 0) {
+                    for (int c = 0; c < kCPW; ++c)
+                        tmem_ld32(tmem + laneBase + buf * 128u + 32u * (kCPW * wg + c),
+                                  *reinterpret_cast<uint32_t(*)[32]>(&x[32 * c]));
+                    tmem_wait_ld();
+                    // The accumulator is in registers now: hand the TMEM buffer back to the MMA.
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
+                    ++acc;
 #pragma unroll
-                            for (int k = 0; k < 32; ++k) ca[k] = uint32_t(INT32_MIN);
-                        }
-                        int32_t rmax = INT32_MIN;
-                        const uint4* nb4 = reinterpret_cast<const uint4*>(&S.nbk[bpar][wg][32 * c]);
+                    for (int c = 0; c < kCPW; ++c) {
+                        const uint32_t j0 = jw + 32u * c;
+                        int32_t m[4] = {INT32_MIN, INT32_MIN, INT32_MIN, INT32_MIN};
+                        const uint4* nb4 = reinterpret_cast<const uint4*>(&S.nbk[bpar][j0 - blockBase]);
 #pragma unroll
                         for (int k4 = 0; k4 < 8; ++k4) {
                             const uint4 nb = nb4[k4];
                             const uint32_t nbv[4] = {nb.x, nb.y, nb.z, nb.w};
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const int k = 4 * k4 + e;
+                            for (int e4 = 0; e4 < 4; ++e4) {
+                                const int k = 32 * c + 4 * k4 + e4;
                                 // Modular 32-bit arithmetic: the true keys always fit in int32.
                                 const uint32_t ck = (x[k] << 9) + uint32_t(rowcP);
-                                ca[k] = uint32_t(max(int32_t(ca[k]), int32_t(ck)));
-                                const int32_t rk = int32_t(ck + nbv[e]);
-                                rmax = max(rmax, rk);
+                                ca[k] = max(ca[k], int32_t(ck));
+                                const int32_t rk = int32_t(ck + nbv[e4]);
+                                m[e4] = max(m[e4], rk);
                                 x[k] = uint32_t(rk);
                             }
                         }
-                        tmem_st32(tmem + laneBase + colAccCol + 32u * c, ca);
+                        int32_t rmax = max(max(m[0], m[1]), max(m[2], m[3]));
                         // Columns past nbDescB only occur in a task's last block: drop them there.
                         if (j0 + 32u > T.nB) {
                             rmax = INT32_MIN;
 #pragma unroll
                             for (int k = 0; k < 32; ++k) {
-                                if (j0 + k >= T.nB) x[k] = uint32_t(INT32_MIN);
-                                rmax = max(rmax, int32_t(x[k]));
+                                if (j0 + k >= T.nB) x[32 * c + k] = uint32_t(INT32_MIN);
+                                rmax = max(rmax, int32_t(x[32 * c + k]));
                             }
                         }
                         if (__any_sync(0xffffffffu, rmax >= tkP)) {
-                            // Exact: position of the chunk maximum (lowest column on ties) and the
-                            // chunk's second key.
-                            uint32_t pos = 31;
+                            // Second key of the chunk: keys within a chunk are distinct, so
+                            // min over k of (rmax - 1 - key) (unsigned) skips exactly the maximum.
+                            uint32_t mn = 0xFFFFFFFFu;
 #pragma unroll
-                            for (int k = 31; k >= 0; --k) pos = (int32_t(x[k]) == rmax) ? uint32_t(k) : pos;
-                            int32_t s2 = INT32_MIN;
-#pragma unroll
-                            for (int k = 0; k < 32; ++k) s2 = max(s2, uint32_t(k) == pos ? INT32_MIN : int32_t(x[k]));
+                            for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(rmax) - 1u - x[32 * c + k]);
+                            const int32_t s2 = int32_t(uint32_t(rmax) - 1u - mn);
                             if (rmax >= tkP) {
                                 l2kP = max(max(l2kP, l1kP), s2);
                                 l1kP = rmax;
-                                l1jP = j0 + pos;
-                                tkP = max(tkP, rmax + 1);
+                                l1jP = j0 + 31u - ((uint32_t(rmax) >> 3) & 31u);
+                                tkP = max(tkP, int32_t((uint32_t(rmax) & ~255u) + 256u));
                             } else {
                                 l2kP = max(l2kP, rmax);
                             }
@@ -328,37 +376,35 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
                     l1k[p] = l1kP;
                     l2k[p] = l2kP;
                     l1j[p] = l1jP;
-                    tmem_wait_st();
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
-                    ++acc;
                 }
-                // ---- column flush: reduce the column accumulator over the 128 lanes.
-                const uint32_t fpar = bpar;
+                // ---- column flush: best key per column over the 128 lanes of this warpgroup. The
+                // flush key orders equal values by row tile, then lane (= by row index):
+                // (value << 8) | (7 - p) << 5 | (31 - lane).
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    uint32_t ca[32];
-                    tmem_ld32(tmem + laneBase + colAccCol + 32u * c, ca);
-                    tmem_wait_ld();
-                    int32_t mine = 0;
+                for (int c = 0; c < kCPW; ++c) {
+                    int32_t mine = INT32_MIN;
 #pragma unroll
                     for (int k = 0; k < 32; ++k) {
-                        const int32_t m = redux_max_s32(int32_t(ca[k]));
-                        mine = (lane == uint32_t(k)) ? m : mine;
+                        const uint32_t v = uint32_t(ca[32 * c + k]);
+                        const int32_t fk = int32_t((v & ~255u) | ((v & 7u) << 5) | (31u - lane));
+                        const int32_t mx = redux_max_s32(fk);
+                        mine = (lane == uint32_t(k)) ? mx : mine;
                     }
-                    const int32_t v = mine >> 8;  // 2 a_i.b_j - |a_i|^2  =  |b_j|^2 - d
-                    const uint32_t low = 255u - (uint32_t(mine) & 255u);
-                    const uint32_t rr = 128u * (low >> 5) + 32u * q + (low & 31u);
+                    // (2 a.b - |a|^2) = |b|^2 - d; row = 128 p + 32 q + lane
+                    const int32_t v = mine >> 8;
+                    const uint32_t pp = 7u - ((uint32_t(mine) >> 5) & 7u);
+                    const uint32_t ln = 31u - (uint32_t(mine) & 31u);
+                    const uint32_t rr = 128u * pp + 32u * q + ln;
                     const unsigned long long key =
                         (static_cast<unsigned long long>(uint32_t(int32_t(kVBias) - v)) << 32) | rr;
-                    atomicMin(&S.colmin[fpar][wg][32 * c + lane], key);
+                    atomicMin(&S.colmin[bpar][jw - blockBase + 32 * c + lane], key);
                 }
-                named_bar(1 + wg, 128);
-                if (t128 < 64) {
-                    const unsigned long long key = S.colmin[fpar][wg][t128];
-                    S.colmin[fpar][wg][t128] = ~0ull;
-                    const uint32_t j = colBase + t128;
+                named_bar(2 + wg, 128);
+                if (t128 < 32 * kCPW) {
+                    const uint32_t cc = jw - blockBase + t128;
+                    const unsigned long long key = S.colmin[bpar][cc];
+                    S.colmin[bpar][cc] = ~0ull;
+                    const uint32_t j = blockBase + cc;
                     const uint32_t i = U.r0 + uint32_t(key & 0xFFFFFFFFu);
                     if (j < T.nB && i < T.nA) {
                         const uint32_t d = uint32_t(key >> 32) - kVBias + T.sqrB[j];
@@ -366,19 +412,35 @@ __global__ void __launch_bounds__(kThreads, 1) bf_match_kernel(const __grid_cons
                     }
                 }
             }
-            // ---- publish this unit's row top-2 (exact two-slot merge, see rsfm_bf_match_ext).
+            // ---- merge the warpgroups' row top-2 in shared memory, then publish each row
+            // once (exact two-slot merge: old = min(best, b); second = min(second, max(old, b), s)).
 #pragma unroll
             for (int p = 0; p < kMaxRowTiles; ++p) {
-                const uint32_t i = U.r0 + 128u * p + 32u * q + lane;
-                if (uint32_t(p) < U.pt && i < T.nA) {
-                    const uint32_t hi = uint32_t(255 - ((p << 5) | int32_t(lane)));
+                const uint32_t r = 128u * p + 32u * q + lane;
+                if (uint32_t(p) < U.pt) {
                     if (l1k[p] != INT32_MIN) {
-                        const uint32_t d1 = (hi - uint32_t(l1k[p])) >> 8;
+                        const uint32_t d1 = ((uint32_t(l1k[p]) & 255u) - uint32_t(l1k[p])) >> 8;
                         const unsigned long long old =
-                            atomicMin(&T.bestA[i], (static_cast<unsigned long long>(d1) << 32) | l1j[p]);
-                        atomicMin(&T.secondA[i], max(uint32_t(old >> 32), d1));
+                            atomicMin(&S.rowbest[unitPar][r], (static_cast<unsigned long long>(d1) << 32) | l1j[p]);
+                        atomicMin(&S.rowsecond[unitPar][r], max(uint32_t(old >> 32), d1));
                     }
-                    if (l2k[p] != INT32_MIN) atomicMin(&T.secondA[i], (hi - uint32_t(l2k[p])) >> 8);
+                    if (l2k[p] != INT32_MIN)
+                        atomicMin(&S.rowsecond[unitPar][r], ((uint32_t(l2k[p]) & 255u) - uint32_t(l2k[p])) >> 8);
+                }
+            }
+            named_bar(1, 32 * kEpiWarps);
+            for (uint32_t r = t512; r < 128u * U.pt; r += 32u * kEpiWarps) {
+                const unsigned long long bst = S.rowbest[unitPar][r];
+                const uint32_t sec = S.rowsecond[unitPar][r];
+                S.rowbest[unitPar][r] = ~0ull;
+                S.rowsecond[unitPar][r] = ~0u;
+                const uint32_t i = U.r0 + r;
+                if (i < T.nA) {
+                    if (bst != ~0ull) {
+                        const unsigned long long old = atomicMin(&T.bestA[i], bst);
+                        atomicMin(&T.secondA[i], max(uint32_t(old >> 32), uint32_t(bst >> 32)));
+                    }
+                    if (sec != ~0u) atomicMin(&T.secondA[i], sec);
                 }
             }
         }
@@ -481,14 +543,37 @@ static void choose_shape(const std::vector<std::pair<uint32_t, uint32_t>>& sizes
     colBlocks = 1;
 }
 
-int launch_chunk(const rsfm_sift_bf_task* tasks, size_t n, uint32_t* const* second, uint32_t* const* flags,
-                 uint32_t ratioNum, uint32_t ratioDen, cudaStream_t stream) {
+// Epilogue warpgroups (2 or 4); RSFM_BF_EPILOGUE_GROUPS overrides the default for tuning runs.
+static int epilogue_groups() {
+    static int g = [] {
+        const char* e = getenv("RSFM_BF_EPILOGUE_GROUPS");
+        return (e && atoi(e) == 4) ? 4 : 2;
+    }();
+    return g;
+}
+
+template <int kWG>
+static int ensure_attr() {
     static bool attrSet = false;
     if (!attrSet) {
-        RSFM_CUDA_TRY(cudaFuncSetAttribute(bf_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RSFM_CUDA_TRY(cudaFuncSetAttribute(bf_match_kernel<kWG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            int(smem_bytes())));
         attrSet = true;
     }
+    return RSFM_OK;
+}
+
+template <int kWG>
+static int launch_main(const Params& P, uint32_t grid, cudaStream_t stream) {
+    const int st = ensure_attr<kWG>();
+    if (st != RSFM_OK) return st;
+    bf_match_kernel<kWG><<<grid, Cfg<kWG>::kThreads, smem_bytes(), stream>>>(P);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    return RSFM_OK;
+}
+
+int launch_chunk(const rsfm_sift_bf_task* tasks, size_t n, uint32_t* const* second, uint32_t* const* flags,
+                 uint32_t ratioNum, uint32_t ratioDen, cudaStream_t stream) {
     const int nsm = sm_count();
     if (nsm <= 0) return RSFM_ERR_CUDA;
 
@@ -547,8 +632,8 @@ int launch_chunk(const rsfm_sift_bf_task* tasks, size_t n, uint32_t* const* seco
         const uint32_t grid = std::min<uint32_t>(units, uint32_t(nsm));
         void* tok = nullptr;
         const bool prof = profile_begin(stream, &tok);
-        bf_match_kernel<<<grid, kThreads, smem_bytes(), stream>>>(P);
-        RSFM_CUDA_TRY(cudaGetLastError());
+        const int st = epilogue_groups() == 4 ? launch_main<4>(P, grid, stream) : launch_main<2>(P, grid, stream);
+        if (st != RSFM_OK) return st;
         if (prof) profile_end(stream, tok);
         launch_count_add(1);
     }
@@ -573,6 +658,68 @@ int launch_chunk(const rsfm_sift_bf_task* tasks, size_t n, uint32_t* const* seco
             launch_count_add(1);
         }
     }
+    return RSFM_OK;
+}
+
+// ---------------------------------------------------------------- batched plans
+// A plan holds the tasks of a whole batch (any count) in device memory, so the matcher runs as
+// one persistent launch over all (task, row block, column range) units; init, match and flags
+// are captured once in a CUDA graph and replayed.
+__global__ void plan_init_kernel(const TaskDev* __restrict__ tasks) {
+    const TaskDev& T = tasks[blockIdx.y];
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < max(T.nA, T.nB); x += gridDim.x * blockDim.x) {
+        if (x < T.nA) {
+            T.bestA[x] = ~0ull;
+            T.secondA[x] = ~0u;
+        }
+        if (x < T.nB) T.bestB[x] = ~0ull;
+    }
+}
+__global__ void plan_flags_kernel(const TaskDev* __restrict__ tasks, uint32_t ratioNum, uint32_t ratioDen) {
+    const TaskDev& T = tasks[blockIdx.y];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < T.nA; i += gridDim.x * blockDim.x) {
+        const unsigned long long bm = T.bestA[i];
+        const uint32_t j = uint32_t(bm & 0xFFFFFFFFu), d = uint32_t(bm >> 32);
+        uint32_t f = 0;
+        if (j != ~0u) {
+            if (uint64_t(ratioDen) * d < uint64_t(ratioNum) * T.secondA[i]) f |= 1u;
+            if (j < T.nB && uint32_t(T.bestB[j] & 0xFFFFFFFFu) == i) f |= 2u;
+        }
+        T.flagsA[i] = f;
+    }
+}
+
+static int validate(const rsfm_sift_bf_task* tasks, size_t n);
+
+}  // namespace bf
+}  // namespace rsfm_b200
+
+struct rsfm_bf_plan {
+    rsfm_b200::bf::TaskDev* dTasks = nullptr;
+    rsfm_b200::bf::Params P;
+    uint32_t grid = 0, nTasks = 0, ratioNum = 64, ratioDen = 100, groups = 2;
+    uint32_t blocksX = 1;
+    cudaStream_t capture = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;
+};
+
+namespace rsfm_b200 {
+namespace bf {
+
+static int plan_enqueue(rsfm_bf_plan* pl, cudaStream_t s) {
+    launch_count_add(1);
+    plan_init_kernel<<<dim3(pl->blocksX, pl->nTasks), 256, 0, s>>>(pl->dTasks);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    if (pl->P.totalUnits > 0) {
+        const int st = pl->groups == 4 ? launch_main<4>(pl->P, pl->grid, s) : launch_main<2>(pl->P, pl->grid, s);
+        if (st != RSFM_OK) return st;
+        launch_count_add(1);
+    }
+    plan_flags_kernel<<<dim3(pl->blocksX, pl->nTasks), 256, 0, s>>>(pl->dTasks, pl->ratioNum, pl->ratioDen);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
     return RSFM_OK;
 }
 
@@ -651,4 +798,125 @@ extern "C" int rsfm_bf_match(const rsfm_sift_bf_task* tasks, size_t nbTasks, cud
         if (st == RSFM_OK && e != cudaSuccess) st = RSFM_ERR_CUDA;
     }
     return st;
+}
+
+extern "C" int rsfm_bf_plan_create(const rsfm_sift_bf_task* tasks, size_t nbTasks, uint32_t* const* secondDistA,
+                                   uint32_t* const* flagsA, uint32_t ratioNum, uint32_t ratioDen,
+                                   const rsfm_bf_plan_options* opts, rsfm_bf_plan** out) {
+    launch_count_reset();
+    if (!out || nbTasks == 0 || nbTasks > 65535 || !secondDistA || !flagsA) return RSFM_ERR_INVALID_ARG;
+    int st = bf::validate(tasks, nbTasks);
+    if (st != RSFM_OK) return st;
+    for (size_t t = 0; t < nbTasks; ++t)
+        if (tasks[t].nbDescA > 0 && (!secondDistA[t] || !flagsA[t])) return RSFM_ERR_INVALID_ARG;
+    const int nsm = sm_count();
+    if (nsm <= 0) return RSFM_ERR_CUDA;
+    auto* pl = new rsfm_bf_plan();
+    memset(&pl->P, 0, sizeof(pl->P));
+    std::vector<std::pair<uint32_t, uint32_t>> sizes;
+    uint32_t maxN = 1;
+    for (size_t t = 0; t < nbTasks; ++t) {
+        sizes.emplace_back(tasks[t].nbDescA, tasks[t].nbDescB);
+        maxN = std::max(maxN, std::max(tasks[t].nbDescA, tasks[t].nbDescB));
+    }
+    uint32_t rt = 0, cb = 0;
+    bf::choose_shape(sizes, nsm, rt, cb);
+    if (opts && opts->rowTiles) rt = std::min<uint32_t>(opts->rowTiles, bf::kMaxRowTiles);
+    if (opts && opts->colBlocks) cb = opts->colBlocks;
+    pl->groups = (opts && opts->epilogueGroups == 4) ? 4u : (opts && opts->epilogueGroups == 2) ? 2u
+                                                                                                : uint32_t(bf::epilogue_groups());
+    std::vector<bf::TaskDev> host(nbTasks);
+    uint32_t units = 0;
+    for (size_t t = 0; t < nbTasks; ++t) {
+        bf::TaskDev& T = host[t];
+        memset(&T, 0, sizeof(T));
+        const rsfm_sift_bf_task& in = tasks[t];
+        T.nA = in.nbDescA;
+        T.nB = in.nbDescB;
+        T.sqrA = in.sqrNormDescA;
+        T.sqrB = in.sqrNormDescB;
+        T.bestA = reinterpret_cast<unsigned long long*>(in.bestMatchA);
+        T.bestB = reinterpret_cast<unsigned long long*>(in.bestMatchB);
+        T.secondA = secondDistA[t];
+        T.flagsA = flagsA[t];
+        T.unitBegin = units;
+        T.rowBlocks = 1;
+        if (T.nA && T.nB) {
+            if ((st = encode_desc_tmap(&T.tmA, in.descA, T.nA, 128)) != RSFM_OK ||
+                (st = encode_desc_tmap(&T.tmB, in.descB, T.nB, 128)) != RSFM_OK) {
+                delete pl;
+                return st;
+            }
+            T.rowBlocks = (T.nA + 128u * rt - 1) / (128u * rt);
+            T.colRanges = (T.nB + 128u * cb - 1) / (128u * cb);
+            units += T.rowBlocks * T.colRanges;
+        }
+    }
+    if (cudaMalloc(reinterpret_cast<void**>(&pl->dTasks), sizeof(bf::TaskDev) * nbTasks) != cudaSuccess ||
+        cudaMemcpy(pl->dTasks, host.data(), sizeof(bf::TaskDev) * nbTasks, cudaMemcpyHostToDevice) != cudaSuccess) {
+        rsfm_bf_plan_destroy(pl);
+        return RSFM_ERR_CUDA;
+    }
+    pl->nTasks = uint32_t(nbTasks);
+    pl->P.gtasks = pl->dTasks;
+    pl->P.nTasks = uint32_t(nbTasks);
+    pl->P.totalUnits = units;
+    pl->P.rowTiles = rt;
+    pl->P.colBlocks = cb;
+    pl->P.err = device_error_word();
+    pl->grid = std::min<uint32_t>(units, uint32_t(nsm));
+    pl->ratioNum = ratioNum;
+    pl->ratioDen = ratioDen;
+    pl->blocksX = std::min<uint32_t>((maxN + 255) / 256, 64);
+    const bool useGraph = !opts || opts->useGraph;
+    if (useGraph) {
+        // Set kernel attributes outside the capture, then record the three launches once.
+        st = pl->groups == 4 ? bf::ensure_attr<4>() : bf::ensure_attr<2>();
+        if (st != RSFM_OK) {
+            rsfm_bf_plan_destroy(pl);
+            return st;
+        }
+        if (cudaStreamCreateWithFlags(&pl->capture, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamBeginCapture(pl->capture, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rsfm_bf_plan_destroy(pl);
+            return RSFM_ERR_CUDA;
+        }
+        st = bf::plan_enqueue(pl, pl->capture);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(pl->capture, &g);
+        pl->graph = g;
+        if (st != RSFM_OK || e != cudaSuccess ||
+            cudaGraphInstantiate(&pl->exec, pl->graph, 0) != cudaSuccess) {
+            rsfm_bf_plan_destroy(pl);
+            return st != RSFM_OK ? st : RSFM_ERR_CUDA;
+        }
+    }
+    *out = pl;
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_bf_plan_launch(rsfm_bf_plan* plan, cudaStream_t stream) {
+    launch_count_reset();
+    if (!plan) return RSFM_ERR_INVALID_ARG;
+    void* tok = nullptr;
+    const bool prof = profile_begin(stream, &tok);
+    if (plan->exec) {
+        RSFM_CUDA_TRY(cudaGraphLaunch(plan->exec, stream));
+        launch_count_add(plan->P.totalUnits > 0 ? 3 : 2);
+    } else {
+        const int st = bf::plan_enqueue(plan, stream);
+        if (st != RSFM_OK) return st;
+    }
+    if (prof) profile_end(stream, tok);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_bf_plan_destroy(rsfm_bf_plan* plan) {
+    if (!plan) return RSFM_OK;
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    if (plan->capture) cudaStreamDestroy(plan->capture);
+    if (plan->dTasks) cudaFree(plan->dTasks);
+    delete plan;
+    return RSFM_OK;
 }

@@ -1,0 +1,418 @@
+// Cascade hashing for B200 (sm_100a): descriptor statistics, projection to bucket keys (and the
+// optional 128-bit remap code), histogram, bucket bounds and deterministic bucket lists.
+//
+// Semantics follow RapidSFM's casHash (paths relative to its source tree):
+//   accumulate  acc[d] += sum_i (x_id >> 1)                      casHash/accumulateDesc.cu:33-131
+//   bias[c]     round(-(sum_d W[c][d] acc[d]) / n) + base[c]     casHash/accumulateDesc.cu:136-174
+//   hash bit c  [bias_c + sum_d W[c][d] (x_d >> 1) >= 0]         casHash/computeHash.cu:237-268,324-327
+//               bucket byte s = bits 8s..8s+7; remap word w = bits 64+32w..64+32w+31
+//                                                                 test/casHashComputeHashTest.cpp:120-139
+//   histogram   [8][256] counts                                  casHash/buildBuckets.cu:29-114
+//   bounds      exclusive lower / inclusive upper, max size      casHash/buildBuckets.cu:116-172
+//   buckets     [8][n] member lists, allocator advanced to upper casHash/buildBuckets.cu:178-269
+// Differences by design: the bias is evaluated exactly in integer arithmetic (the reference uses
+// float under --use_fast_math and its own test accepts +-1); bucket members are written in
+// ascending descriptor order (the reference's order depends on atomic scheduling).
+#include "common.h"
+#include "sm100.cuh"
+#include <algorithm>
+#include <vector>
+
+namespace rsfm_b200 {
+namespace ch {
+
+using namespace sm100;
+
+// ---------------------------------------------------------------- accumulate
+// 256 threads: thread t sums dims [16 (t%8), +16) of descriptors t/8, t/8 + 32, ... of the block's
+// range; 32 partial rows are then reduced in shared memory and added to acc with 64-bit atomics.
+constexpr int kAccThreads = 256;
+constexpr int kAccDescPerBlock = 2048;
+__global__ void __launch_bounds__(kAccThreads) accumulate_kernel(unsigned long long* __restrict__ acc,
+                                                                 const uint4* __restrict__ desc, uint32_t n) {
+    __shared__ uint32_t part[32][128 + 4];
+    const uint32_t t = threadIdx.x;
+    const uint32_t lane8 = t & 7u, row = t >> 3;
+    uint32_t s[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s[k] = 0;
+    const uint32_t base = blockIdx.x * kAccDescPerBlock;
+    const uint32_t end = min(n, base + kAccDescPerBlock);
+    for (uint32_t i = base + row; i < end; i += 32) {
+        uint4 v = __ldg(&desc[size_t(i) * 8 + lane8]);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t h = (w[k] & 0xFEFEFEFEu) >> 1;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) s[4 * k + b] += (h >> (8 * b)) & 0xFFu;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) part[row][16 * lane8 + k] = s[k];
+    __syncthreads();
+    if (t < 128) {
+        unsigned long long tot = 0;
+        for (int r = 0; r < 32; ++r) tot += part[r][t];
+        if (tot) atomicAdd(&acc[t], tot);
+    }
+}
+
+// ---------------------------------------------------------------- bias
+__global__ void bias_kernel(int32_t* __restrict__ bias, const int8_t* __restrict__ w, const int32_t* __restrict__ base,
+                            const unsigned long long* __restrict__ acc, unsigned long long n, int channels) {
+    const int c = threadIdx.x;
+    if (c >= channels) return;
+    long long num = 0;
+    for (int d = 0; d < 128; ++d) num += (long long)w[c * 128 + d] * (long long)acc[d];
+    num = -num;  // rounding of num / n, half away from zero
+    const unsigned long long a = num < 0 ? (unsigned long long)(-num) : (unsigned long long)num;
+    long long qv = (long long)((2 * a + n) / (2 * n));
+    if (num < 0) qv = -qv;
+    bias[c] = int32_t(qv) + base[c];
+}
+
+// ---------------------------------------------------------------- projection (tcgen05)
+// 128 descriptors per tile: TMA loads the raw bytes (128-byte swizzle), threads halve them in
+// place (x >> 1 fits int8), one thread issues s8 x s8 UMMAs (M=128, N=channels, K=128) against
+// the weights (s8, loaded once per CTA), each thread reads its descriptor's channel sums from
+// its TMEM lane and packs the sign bits.
+constexpr int kHashThreads = 128;
+struct HashSmem {
+    uint8_t desc[2][128 * 128];
+    uint8_t w[192 * 128];
+    int32_t bias[192];
+    uint32_t hist[8][256];
+    uint64_t full[2];
+    uint64_t mma;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ uint32_t idesc_s8s8_s32(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kHashThreads, 1)
+hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ CUtensorMap tmW,
+            const int32_t* __restrict__ bias, int channels, uint32_t n, uint8_t* __restrict__ keys,
+            uint32_t* __restrict__ remap, uint32_t* __restrict__ histogram, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    HashSmem& S = *reinterpret_cast<HashSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t tiles = (n + 127) / 128;
+    for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) (&S.hist[0][0])[x] = 0;
+    for (int c = tid; c < channels; c += kHashThreads) S.bias[c] = bias[c];
+    if (tid == 0) {
+        mbar_init(&S.full[0], 1);
+        mbar_init(&S.full[1], 1);
+        mbar_init(&S.mma, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&S.tmem, 256);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    uint32_t* err_ = err;
+    // weights once (channels rows of 128 bytes), then the first descriptor tile
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&S.mma, uint32_t(channels) * 128u);
+        for (int r = 0; r < channels; r += 64) tma_load_2d(S.w + r * 128, &tmW, &S.mma, 0, r);
+        if (blockIdx.x < tiles) {
+            mbar_arrive_expect_tx(&S.full[0], 128u * 128u);
+            tma_load_2d(S.desc[0], &tmDesc, &S.full[0], 0, int32_t(blockIdx.x * 128u));
+        }
+    }
+    mbar_wait(&S.mma, 0, err_, kDevTimeoutTmaFull);
+    uint32_t it = 0, mmaPhase = 1;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+        const uint32_t buf = it & 1u;
+        // prefetch the next tile into the other buffer (its previous MMA has completed)
+        if (tid == 0 && tile + gridDim.x < tiles) {
+            mbar_arrive_expect_tx(&S.full[buf ^ 1u], 128u * 128u);
+            tma_load_2d(S.desc[buf ^ 1u], &tmDesc, &S.full[buf ^ 1u], 0, int32_t((tile + gridDim.x) * 128u));
+        }
+        mbar_wait(&S.full[buf], (it >> 1) & 1u, err_, kDevTimeoutTmaFull);
+        // halve every byte in place: (x & 0xFE) >> 1
+        uint4* d4 = reinterpret_cast<uint4*>(S.desc[buf]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            uint4 v = d4[tid + 128 * k];
+            v.x = (v.x & 0xFEFEFEFEu) >> 1;
+            v.y = (v.y & 0xFEFEFEFEu) >> 1;
+            v.z = (v.z & 0xFEFEFEFEu) >> 1;
+            v.w = (v.w & 0xFEFEFEFEu) >> 1;
+            d4[tid + 128 * k] = v;
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t idesc = idesc_s8s8_s32(128, channels);
+            const uint32_t a = smem_u32(S.desc[buf]), b = smem_u32(S.w);
+#pragma unroll
+            for (uint32_t k = 0; k < 4; ++k)
+                umma_i8(tmem, umma_desc_k_sw128(a + 32u * k), umma_desc_k_sw128(b + 32u * k), idesc, k);
+            umma_commit(&S.mma);
+        }
+        __syncwarp();
+        mbar_wait(&S.mma, mmaPhase, err_, kDevTimeoutAccFull);
+        mmaPhase ^= 1u;
+        tc_fence_after();
+        const uint32_t i = tile * 128u + tid;  // descriptor of this thread's TMEM lane
+        uint32_t words[6];
+        for (int cw = 0; cw < channels / 32; ++cw) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((32u * warp) << 16) + 32u * cw, v);
+            tmem_wait_ld();
+            uint32_t bits = 0;
+#pragma unroll
+            for (int k = 0; k < 32; ++k) bits |= (int32_t(v[k]) + S.bias[32 * cw + k] >= 0 ? 1u : 0u) << k;
+            words[cw] = bits;
+        }
+        if (i < n) {
+            *reinterpret_cast<uint2*>(keys + size_t(i) * 8) = make_uint2(words[0], words[1]);
+            if (remap && channels == 192)
+                *reinterpret_cast<uint4*>(remap + size_t(i) * 4) = make_uint4(words[2], words[3], words[4], words[5]);
+            if (histogram) {
+#pragma unroll
+                for (int s = 0; s < 8; ++s) atomicAdd(&S.hist[s][(words[s >> 2] >> (8 * (s & 3))) & 0xFFu], 1u);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM and the descriptor buffer are reused by the next iteration
+    }
+    if (histogram) {
+        __syncthreads();
+        for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) {
+            const uint32_t c = (&S.hist[0][0])[x];
+            if (c) atomicAdd(&histogram[x], c);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// ---------------------------------------------------------------- histogram
+__global__ void histogram_kernel(uint32_t* __restrict__ hist, const uint2* __restrict__ keys, uint32_t n) {
+    __shared__ uint32_t h[8][256];
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) (&h[0][0])[x] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint2 k = keys[i];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) atomicAdd(&h[s][((s < 4 ? k.x : k.y) >> (8 * (s & 3))) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) {
+        const uint32_t c = (&h[0][0])[x];
+        if (c) atomicAdd(&hist[x], c);
+    }
+}
+
+// ---------------------------------------------------------------- bucket bounds (one block)
+// Warp s scans scheme s: lane l owns buckets [8l, 8l+8).
+__global__ void bounds_kernel(uint32_t* __restrict__ lower, uint32_t* __restrict__ upper, uint32_t* maxBucket,
+                              const uint32_t* __restrict__ hist) {
+    __shared__ uint32_t wmax[8];
+    const uint32_t s = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t v[8], sum = 0, mx = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        v[k] = hist[s * 256 + 8 * lane + k];
+        sum += v[k];
+        mx = max(mx, v[k]);
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= uint32_t(o)) incl += y;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        lower[s * 256 + 8 * lane + k] = run;
+        run += v[k];
+        upper[s * 256 + 8 * lane + k] = run;
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (lane == 0) wmax[s] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int k = 0; k < 8; ++k) m = max(m, wmax[k]);
+        *maxBucket = m;
+    }
+}
+
+// ---------------------------------------------------------------- buckets (stable)
+constexpr uint32_t kChunk = 1024;
+// (1) per-chunk histograms: chunkHist[c][8][256]
+__global__ void chunk_hist_kernel(uint32_t* __restrict__ chunkHist, const uint2* __restrict__ keys, uint32_t n) {
+    __shared__ uint32_t h[8][256];
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) (&h[0][0])[x] = 0;
+    __syncthreads();
+    const uint32_t c = blockIdx.x;
+    for (uint32_t i = c * kChunk + threadIdx.x; i < min(n, (c + 1) * kChunk); i += blockDim.x) {
+        const uint2 k = keys[i];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) atomicAdd(&h[s][((s < 4 ? k.x : k.y) >> (8 * (s & 3))) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) chunkHist[size_t(c) * 2048 + x] = (&h[0][0])[x];
+}
+// (2) per (scheme, bucket): exclusive offsets over chunks, starting at the allocator's lower
+// bound; the allocator ends at the upper bound, like the reference's buildBuckets.
+__global__ void chunk_offsets_kernel(uint32_t* __restrict__ chunkHist, uint32_t* __restrict__ idxAllocator,
+                                     uint32_t chunks) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= 2048) return;
+    uint32_t run = idxAllocator[x];
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t h = chunkHist[size_t(c) * 2048 + x];
+        chunkHist[size_t(c) * 2048 + x] = run;
+        run += h;
+    }
+    idxAllocator[x] = run;
+}
+// (3) fill: warp s of block c walks chunk c in order for scheme s; ranks within a step come from
+// __match_any_sync, so members land in ascending descriptor order.
+__global__ void __launch_bounds__(256) fill_kernel(const uint8_t* __restrict__ keys, uint32_t n,
+                                                   const uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ buckets) {
+    __shared__ uint32_t cnt[8][256];
+    const uint32_t s = threadIdx.x >> 5, lane = threadIdx.x & 31u, c = blockIdx.x;
+    for (uint32_t x = lane; x < 256; x += 32) cnt[s][x] = 0;
+    __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t end = min(n, (c + 1) * kChunk);
+    for (uint32_t i0 = c * kChunk; i0 < end; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool in = i < end;
+        const uint32_t key = in ? keys[size_t(i) * 8 + s] : 256u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (in) {
+            const uint32_t rank = __popc(peers & lt);
+            const uint32_t slot = chunkOff[size_t(c) * 2048 + s * 256 + key] + cnt[s][key] + rank;
+            buckets[size_t(s) * n + slot] = i;
+        }
+        __syncwarp();
+        if (in && (peers & lt) == 0) cnt[s][key] += __popc(peers);
+        __syncwarp();
+    }
+}
+
+int hash_launch(const void* weights, const int32_t* bias, int channels, const void* desc, uint32_t n, uint8_t* keys,
+                uint32_t* remap, uint32_t* histogram, cudaStream_t stream) {
+    if (channels != 64 && channels != 192) return RSFM_ERR_INVALID_ARG;
+    if (histogram) RSFM_CUDA_TRY(cudaMemsetAsync(histogram, 0, 8 * 256 * 4, stream));
+    if (n == 0) return RSFM_OK;
+    CUtensorMap tmD, tmW;
+    int st = encode_desc_tmap(&tmD, desc, n, 128);
+    if (st != RSFM_OK) return st;
+    st = encode_desc_tmap(&tmW, weights, uint64_t(channels), 64);
+    if (st != RSFM_OK) return st;
+    const size_t smem = sizeof(HashSmem) + 1024;
+    static bool attr = false;
+    if (!attr) {
+        RSFM_CUDA_TRY(cudaFuncSetAttribute(hash_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        attr = true;
+    }
+    const uint32_t tiles = (n + 127) / 128;
+    const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(2 * sm_count()));
+    void* tok = nullptr;
+    const bool prof = profile_begin(stream, &tok);
+    hash_kernel<<<grid, kHashThreads, smem, stream>>>(tmD, tmW, bias, channels, n, keys, remap, histogram,
+                                                       device_error_word());
+    RSFM_CUDA_TRY(cudaGetLastError());
+    if (prof) profile_end(stream, tok);
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+}  // namespace ch
+}  // namespace rsfm_b200
+
+using namespace rsfm_b200;
+
+extern "C" int rsfm_cashash_accumulate_desc(unsigned long long* acc, int initAcc, const void* desc, uint32_t nbDesc,
+                                            cudaStream_t stream) {
+    launch_count_reset();
+    if (!acc || (nbDesc && (!desc || (reinterpret_cast<uintptr_t>(desc) & 15u)))) return RSFM_ERR_INVALID_ARG;
+    if (initAcc) RSFM_CUDA_TRY(cudaMemsetAsync(acc, 0, 128 * 8, stream));
+    if (nbDesc == 0) return RSFM_OK;
+    const uint32_t grid = (nbDesc + ch::kAccDescPerBlock - 1) / ch::kAccDescPerBlock;
+    ch::accumulate_kernel<<<grid, ch::kAccThreads, 0, stream>>>(acc, static_cast<const uint4*>(desc), nbDesc);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_compute_bias(int32_t* bias, const void* weights, const int32_t* biasBase,
+                                         const unsigned long long* acc, unsigned long long nbDesc, int nbChannels,
+                                         cudaStream_t stream) {
+    launch_count_reset();
+    if (!bias || !weights || !biasBase || !acc || nbDesc == 0 || nbChannels <= 0 || nbChannels > 192)
+        return RSFM_ERR_INVALID_ARG;
+    ch::bias_kernel<<<1, 192, 0, stream>>>(bias, static_cast<const int8_t*>(weights), biasBase, acc, nbDesc,
+                                           nbChannels);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_compute_hash(const void* weights, const int32_t* bias, int nbChannels, const void* desc,
+                                         uint32_t nbDesc, uint8_t* bucketIndices, uint32_t* remap,
+                                         uint32_t* histogram, cudaStream_t stream) {
+    launch_count_reset();
+    if (!weights || !bias || (nbDesc && (!desc || !bucketIndices))) return RSFM_ERR_INVALID_ARG;
+    if (nbChannels == 192 && nbDesc && !remap) return RSFM_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(bucketIndices) & 7u) || (reinterpret_cast<uintptr_t>(remap) & 15u))
+        return RSFM_ERR_INVALID_ARG;
+    return ch::hash_launch(weights, bias, nbChannels, desc, nbDesc, bucketIndices, remap, histogram, stream);
+}
+
+extern "C" int rsfm_cashash_build_histogram(uint32_t* histogram, const uint8_t* bucketIndices, uint32_t nbDesc,
+                                            cudaStream_t stream) {
+    launch_count_reset();
+    if (!histogram || (nbDesc && !bucketIndices) || (reinterpret_cast<uintptr_t>(bucketIndices) & 7u))
+        return RSFM_ERR_INVALID_ARG;
+    RSFM_CUDA_TRY(cudaMemsetAsync(histogram, 0, 8 * 256 * 4, stream));
+    if (nbDesc == 0) return RSFM_OK;
+    const uint32_t grid = std::min<uint32_t>((nbDesc + 2047) / 2048, 1024);
+    ch::histogram_kernel<<<grid, 256, 0, stream>>>(histogram, reinterpret_cast<const uint2*>(bucketIndices), nbDesc);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_compute_bucket_bound(uint32_t* lower, uint32_t* upper, uint32_t* maxBucketSize,
+                                                 const uint32_t* histogram, cudaStream_t stream) {
+    launch_count_reset();
+    if (!lower || !upper || !maxBucketSize || !histogram) return RSFM_ERR_INVALID_ARG;
+    ch::bounds_kernel<<<1, 256, 0, stream>>>(lower, upper, maxBucketSize, histogram);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_build_buckets(const uint8_t* bucketIndices, uint32_t nbDesc, uint32_t* idxAllocator,
+                                          uint32_t* buckets, cudaStream_t stream) {
+    launch_count_reset();
+    if (!idxAllocator || (nbDesc && (!bucketIndices || !buckets))) return RSFM_ERR_INVALID_ARG;
+    if (nbDesc == 0) return RSFM_OK;
+    const uint32_t chunks = (nbDesc + ch::kChunk - 1) / ch::kChunk;
+    uint32_t* scratch = nullptr;
+    RSFM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), size_t(chunks) * 2048 * 4, stream));
+    ch::chunk_hist_kernel<<<chunks, 256, 0, stream>>>(scratch, reinterpret_cast<const uint2*>(bucketIndices), nbDesc);
+    ch::chunk_offsets_kernel<<<8, 256, 0, stream>>>(scratch, idxAllocator, chunks);
+    ch::fill_kernel<<<chunks, 256, 0, stream>>>(bucketIndices, nbDesc, scratch, buckets);
+    cudaError_t e = cudaGetLastError();
+    cudaError_t f = cudaFreeAsync(scratch, stream);
+    launch_count_add(3);
+    return (e == cudaSuccess && f == cudaSuccess) ? RSFM_OK : RSFM_ERR_CUDA;
+}

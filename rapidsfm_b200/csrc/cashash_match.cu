@@ -1,0 +1,367 @@
+// Cascade-hash matching for B200 (sm_100a): for every (scheme s, bucket k), every query
+// descriptor in bucket (s,k) of a query image is compared with every train descriptor in bucket
+// (s,k) of the train image by exact L2; per query and per train descriptor the lexicographic
+// minimum of (distance, index) over all shared buckets is kept.
+//
+// Semantics follow RapidSFM's cashash::findBestMatch (casHash/findBestMatch.cu:570-676, results
+// initialised by kernelInitCasHashMatch :619-632; CPU check test/casHashFindBestMatchTest.cpp:138-184).
+// The reference resolves equal distances by the position inside a bucket, which depends on how
+// buildBuckets ordered the bucket; here ties always go to the lowest descriptor index, whatever
+// the bucket order (the two agree whenever bucket lists are in ascending order).
+//
+// Work decomposition. A work item is one (scheme, bucket) pair, taken from an atomic counter by
+// persistent CTAs of 4 warps. The item's query members of all tasks are cut into 32-row segments
+// (one task per segment, members sorted by index inside the warp), four segments form a 128-row A
+// tile gathered with cp.async into the 128-byte-swizzled layout; the train members form 64-column
+// B blocks (sorted by index). One thread issues the u8 x u8 UMMA (M=128, N=64, K=128) into TMEM;
+// each warp reads its segment's 32 TMEM lanes: row minima are thread-local, column minima use a
+// warp reduction per column; results go out with 64-bit atomicMin as in the reference.
+#include "common.h"
+#include "sm100.cuh"
+#include <algorithm>
+
+namespace rsfm_b200 {
+namespace chm {
+
+using namespace sm100;
+
+constexpr int kMaxTasks = 64;
+constexpr int kThreads = 128;
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+// Padding rows/columns get this squared norm: their distances land in [2^23, 2^24), above every
+// real distance (at most 128*255^2 < 2^23) and small enough to shift left by 6 without overflow.
+constexpr uint32_t kBigNorm = 1u << 23;
+constexpr uint32_t kValidD = 1u << 23;
+
+struct ImageDev {
+    const uint8_t* desc;
+    const uint32_t* ends;     // [8][256] inclusive upper bounds
+    const uint32_t* buckets;  // [8][n]
+    const uint32_t* sqr;
+};
+
+struct Params {
+    ImageDev q[kMaxTasks];
+    unsigned long long* qBest[kMaxTasks];
+    unsigned long long* tBest[kMaxTasks];
+    ImageDev t;
+    uint32_t nTasks;
+    uint32_t schemeOffset;  // 1: bucket lists of scheme s start at s*n; 0: reference indexing
+    uint32_t* counter;      // work-item counter (zeroed by the init kernel)
+    uint32_t* err;
+};
+
+struct Smem {
+    uint8_t a[128 * 128];
+    uint8_t b[64 * 128];
+    uint32_t rowQ[128], rowNA[128];
+    uint32_t colT[64], colNB[64];
+    uint32_t segTask[kMaxTasks], segBase[kMaxTasks + 1];  // per task: first segment (prefix)
+    uint32_t qBeg[kMaxTasks], qCnt[kMaxTasks];
+    uint64_t mma;
+    uint32_t item;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ uint32_t sw128(uint32_t row, uint32_t chunk) {
+    return (row >> 3) * 1024u + (row & 7u) * 128u + (((chunk ^ row) & 7u) << 4);
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem)), "l"(gmem),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Ascending sort of one value per lane (bitonic network over the warp).
+__device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
+#pragma unroll
+    for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool up = ((lane & size) == 0);
+            const bool lower = ((lane & stride) == 0);
+            v = (lower == up) ? min(v, o) : max(v, o);
+        }
+    }
+    return v;
+}
+
+__global__ void init_kernel(const __grid_constant__ Params P, uint32_t nTrain, uint32_t maxQ,
+                            const uint32_t* __restrict__ qSizes) {
+    const uint32_t t = blockIdx.y;
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < qSizes[t]) P.qBest[t][x] = ~0ull;
+    if (P.tBest[t] && x < nTrain) P.tBest[t][x] = ~0ull;
+    if (t == 0 && x == 0) *P.counter = 0;
+}
+
+__global__ void __launch_bounds__(kThreads) match_kernel(const __grid_constant__ Params P, uint32_t nTrain,
+                                                         const uint32_t* __restrict__ qSizes) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    if (tid == 0) {
+        mbar_init(&S.mma, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&S.tmem, 64);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    const uint32_t idesc = idesc_u8u8_s32(128, 64);
+    uint32_t mmaPhase = 0;
+    const bool bidir = P.tBest[0] != nullptr;
+
+    for (;;) {
+        if (tid == 0) S.item = atomicAdd(P.counter, 1u);
+        __syncthreads();
+        const uint32_t item = S.item;
+        if (item >= 8u * 256u) break;
+        // Spread schemes: consecutive items are different buckets of different schemes.
+        const uint32_t s = item & 7u, k = item >> 3;
+        const uint32_t* tEnds = P.t.ends + s * 256;
+        const uint32_t tb = k ? tEnds[k - 1] : 0u, te = tEnds[k];
+        const uint32_t nT = te - tb;
+        if (nT == 0) {
+            __syncthreads();
+            continue;
+        }
+        // Query members of every task in this bucket, cut into 32-row segments.
+        if (tid < P.nTasks) {
+            const uint32_t* qe = P.q[tid].ends + s * 256;
+            const uint32_t b0 = k ? qe[k - 1] : 0u;
+            S.qBeg[tid] = b0;
+            S.qCnt[tid] = qe[k] - b0;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t g = 0;
+            for (uint32_t t = 0; t < P.nTasks; ++t) {
+                S.segBase[t] = g;
+                g += (S.qCnt[t] + 31u) / 32u;
+            }
+            S.segBase[P.nTasks] = g;
+        }
+        __syncthreads();
+        const uint32_t nSeg = S.segBase[P.nTasks];
+        const uint32_t nColBlocks = (nT + 63u) / 64u;
+        for (uint32_t g0 = 0; g0 < nSeg; g0 += 4) {
+            // ---- gather this tile's 4 segments (one per warp), rows sorted by query index
+            const uint32_t g = g0 + warp;
+            uint32_t task = 0;
+            if (g < nSeg)
+                while (task + 1 < P.nTasks && S.segBase[task + 1] <= g) ++task;
+            uint32_t q = kNoRow;
+            if (g < nSeg) {
+                const uint32_t m = (g - S.segBase[task]) * 32u + lane;
+                if (m < S.qCnt[task]) {
+                    const uint32_t nQ = P.q[task].ends[255];
+                    q = P.q[task].buckets[size_t(s) * nQ * P.schemeOffset + S.qBeg[task] + m];
+                }
+            }
+            q = warp_sort(q, lane);
+            const uint32_t row = 32u * warp + lane;
+            S.rowQ[row] = q;
+            S.rowNA[row] = q != kNoRow ? P.q[task].sqr[q] : kBigNorm;
+            {
+                const uint8_t* src = q != kNoRow ? P.q[task].desc + size_t(q) * 128 : P.q[0].desc;
+#pragma unroll
+                for (uint32_t c = 0; c < 8; ++c) cp_async16(S.a + sw128(row, c), src + 16 * c, q != kNoRow);
+            }
+            const uint32_t rowTask = task;
+            const bool rowValid = q != kNoRow;
+            // row state across column blocks: best (d, train index)
+            uint32_t bestD = 0xFFFFFFFFu, bestT = 0xFFFFFFFFu;
+            for (uint32_t cb = 0; cb < nColBlocks; ++cb) {
+                // ---- train block: up to 64 members, sorted by index (rank sort in shared memory)
+                if (cb > 0 || g0 == 0 || nColBlocks > 1) {
+                    if (tid < 64) {
+                        const uint32_t c = cb * 64u + tid;
+                        S.colT[tid] = c < nT ? P.t.buckets[size_t(s) * nTrain * P.schemeOffset + tb + c] : kNoRow;
+                    }
+                    __syncthreads();
+                    uint32_t v = kNoRow, rank = 0;
+                    if (tid < 64) {
+                        v = S.colT[tid];
+                        for (uint32_t o = 0; o < 64; ++o) {
+                            const uint32_t w = S.colT[o];
+                            rank += (w < v) || (w == v && o < tid);
+                        }
+                    }
+                    __syncthreads();
+                    if (tid < 64) {
+                        S.colT[rank] = v;
+                        S.colNB[rank] = v != kNoRow ? P.t.sqr[v] : kBigNorm;
+                    }
+                    __syncthreads();
+                    // gather: 64 rows x 8 chunks, 4 per thread
+#pragma unroll
+                    for (uint32_t x = 0; x < 4; ++x) {
+                        const uint32_t r = (tid >> 3) + 16u * x, c = tid & 7u;
+                        const uint32_t tv = S.colT[r];
+                        const uint8_t* src = tv != kNoRow ? P.t.desc + size_t(tv) * 128 + 16 * c : P.t.desc;
+                        cp_async16(S.b + sw128(r, c), src, tv != kNoRow);
+                    }
+                }
+                cp_async_wait_all();
+                fence_proxy_async_smem();
+                __syncthreads();
+                if (tid == 0) {
+                    tc_fence_after();
+                    const uint32_t a = smem_u32(S.a), b = smem_u32(S.b);
+#pragma unroll
+                    for (uint32_t kk = 0; kk < 4; ++kk)
+                        umma_i8(tmem, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk), idesc, kk);
+                    umma_commit(&S.mma);
+                }
+                __syncwarp();
+                mbar_wait(&S.mma, mmaPhase, P.err, kDevTimeoutAccFull);
+                mmaPhase ^= 1u;
+                tc_fence_after();
+                // ---- epilogue: warp = segment (32 rows), 64 columns in two chunks
+                const uint32_t nA = S.rowNA[row];
+#pragma unroll
+                for (uint32_t ch = 0; ch < 2; ++ch) {
+                    uint32_t x[32];
+                    tmem_ld32(tmem + ((32u * warp) << 16) + 32u * ch, x);
+                    tmem_wait_ld();
+                    uint32_t rmin = 0xFFFFFFFFu;
+#pragma unroll
+                    for (uint32_t c = 0; c < 32; ++c) {
+                        const uint32_t d = nA + S.colNB[32 * ch + c] - 2u * x[c];
+                        x[c] = d;
+                        rmin = min(rmin, (d << 6) | (32u * ch + c));
+                    }
+                    // row: chunk minimum (ties -> lowest column = lowest train index in the block)
+                    const uint32_t cd = rmin >> 6, cc = rmin & 63u;
+                    if (rowValid && cd < kValidD) {
+                        const uint32_t tIdx = S.colT[cc];
+                        if (cd < bestD || (cd == bestD && tIdx < bestT)) {
+                            bestD = cd;
+                            bestT = tIdx;
+                        }
+                    }
+                    // columns: warp minimum of (d, lane) (lanes sorted by query index)
+                    if (bidir) {
+                        uint32_t mine = 0xFFFFFFFFu;
+#pragma unroll
+                        for (uint32_t c = 0; c < 32; ++c) {
+                            const uint32_t key = rowValid && x[c] < kValidD ? ((x[c] << 5) | lane) : 0xFFFFFFFFu;
+                            const uint32_t m = __reduce_min_sync(0xffffffffu, key);
+                            mine = (lane == c) ? m : mine;
+                        }
+                        const uint32_t tIdx = S.colT[32 * ch + lane];
+                        if (mine != 0xFFFFFFFFu && tIdx != kNoRow) {
+                            const uint32_t qIdx = S.rowQ[32 * warp + (mine & 31u)];
+                            atomicMin(&P.tBest[rowTask][tIdx], (static_cast<unsigned long long>(mine >> 5) << 32) | qIdx);
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncthreads();  // TMEM and the B block are reused by the next block / tile
+            }
+            if (rowValid && bestD != 0xFFFFFFFFu)
+                atomicMin(&P.qBest[rowTask][q], (static_cast<unsigned long long>(bestD) << 32) | bestT);
+            __syncthreads();  // the A tile is reused by the next tile
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+}  // namespace chm
+}  // namespace rsfm_b200
+
+using namespace rsfm_b200;
+
+static int find_best_match_impl(const rsfm_cashash_image* queries, const uint32_t* querySize,
+                                const rsfm_cashash_image* train, uint32_t trainSize,
+                                const rsfm_cashash_result* results, uint32_t nbTasks, uint32_t flags,
+                                cudaStream_t stream) {
+    launch_count_reset();
+    if (nbTasks == 0) return RSFM_OK;
+    if (!queries || !querySize || !train || !results) return RSFM_ERR_INVALID_ARG;
+    const bool bidir = results[0].train != nullptr;
+    uint32_t* counter = nullptr;
+    uint32_t* qSizes = nullptr;
+    RSFM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&counter), 4 + 4 * chm::kMaxTasks, stream));
+    qSizes = counter + 1;
+    static bool attr = false;
+    const size_t smem = sizeof(chm::Smem) + 1024;
+    if (!attr) {
+        RSFM_CUDA_TRY(cudaFuncSetAttribute(chm::match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        attr = true;
+    }
+    int st = RSFM_OK;
+    for (uint32_t i0 = 0; i0 < nbTasks && st == RSFM_OK; i0 += chm::kMaxTasks) {
+        const uint32_t n = std::min<uint32_t>(chm::kMaxTasks, nbTasks - i0);
+        chm::Params P;
+        memset(&P, 0, sizeof(P));
+        uint32_t maxQ = 0;
+        uint32_t sizes[chm::kMaxTasks];
+        for (uint32_t t = 0; t < n; ++t) {
+            const rsfm_cashash_image& q = queries[i0 + t];
+            if (!q.desc || !q.bucketEnds || !q.buckets || !q.sqrNormDesc || !results[i0 + t].query ||
+                (bidir && !results[i0 + t].train) || (reinterpret_cast<uintptr_t>(q.desc) & 15u)) {
+                st = RSFM_ERR_INVALID_ARG;
+                break;
+            }
+            P.q[t] = {static_cast<const uint8_t*>(q.desc), q.bucketEnds, q.buckets, q.sqrNormDesc};
+            P.qBest[t] = reinterpret_cast<unsigned long long*>(results[i0 + t].query);
+            P.tBest[t] = bidir ? reinterpret_cast<unsigned long long*>(results[i0 + t].train) : nullptr;
+            sizes[t] = querySize[i0 + t];
+            maxQ = std::max(maxQ, sizes[t]);
+        }
+        if (st != RSFM_OK) break;
+        if (!train->desc || !train->bucketEnds || !train->buckets || !train->sqrNormDesc ||
+            (reinterpret_cast<uintptr_t>(train->desc) & 15u)) {
+            st = RSFM_ERR_INVALID_ARG;
+            break;
+        }
+        P.t = {static_cast<const uint8_t*>(train->desc), train->bucketEnds, train->buckets, train->sqrNormDesc};
+        P.nTasks = n;
+        P.schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+        P.counter = counter;
+        P.err = device_error_word();
+        if (cudaMemcpyAsync(qSizes, sizes, 4 * n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+            st = RSFM_ERR_CUDA;
+            break;
+        }
+        const uint32_t maxN = std::max(std::max(maxQ, trainSize), 1u);
+        chm::init_kernel<<<dim3((maxN + 255) / 256, n), 256, 0, stream>>>(P, trainSize, maxQ, qSizes);
+        const uint32_t grid = uint32_t(4 * sm_count());
+        void* tok = nullptr;
+        const bool prof = profile_begin(stream, &tok);
+        chm::match_kernel<<<grid, chm::kThreads, smem, stream>>>(P, trainSize, qSizes);
+        if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
+        if (prof) profile_end(stream, tok);
+        launch_count_add(2);
+        // The counter and sizes are reused by the next chunk: keep launches ordered on the stream.
+    }
+    cudaFreeAsync(counter, stream);
+    return st;
+}
+
+extern "C" int rsfm_cashash_find_best_match(const rsfm_cashash_image* queries, const uint32_t* querySize,
+                                            const rsfm_cashash_image* train, uint32_t trainSize,
+                                            const rsfm_cashash_result* results, uint32_t nbTasks,
+                                            const uint32_t* maxQueryBucketSize, uint32_t maxTrainBucketSize,
+                                            cudaStream_t stream) {
+    (void)maxQueryBucketSize;  // the persistent kernel sizes its tiles from the buckets themselves
+    (void)maxTrainBucketSize;
+    return find_best_match_impl(queries, querySize, train, trainSize, results, nbTasks, 0u, stream);
+}
+
+extern "C" int rsfm_cashash_find_best_match_ex(const rsfm_cashash_image* queries, const uint32_t* querySize,
+                                               const rsfm_cashash_image* train, uint32_t trainSize,
+                                               const rsfm_cashash_result* results, uint32_t nbTasks, uint32_t flags,
+                                               cudaStream_t stream) {
+    return find_best_match_impl(queries, querySize, train, trainSize, results, nbTasks, flags, stream);
+}

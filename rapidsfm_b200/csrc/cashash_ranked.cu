@@ -1,0 +1,184 @@
+// Ranked cascade-hash matching (no reference counterpart; the north star's "config 3" matcher):
+// per query descriptor the candidates are the train descriptors sharing at least one of the first
+// `tables` 8-bit bucket keys; they are ranked by the Hamming distance of their 128-bit codes (ties
+// by lower index), the best `topK` are re-ranked by exact L2, and the query gets the best match,
+// the second-best distance and the ratio-test flag.
+//
+// One warp per query. Duplicate candidates (a train descriptor colliding in several tables) are
+// dropped without a set: a candidate found in table s is kept only if it collides with the query
+// in no table before s. Candidate keys (hamming << 24 | index) go to a per-warp shared buffer; the
+// top-K are extracted by K rounds of a warp minimum (keys are distinct), merging buffer flushes
+// with the running top-K when a query has more candidates than the buffer holds.
+#include "common.h"
+#include <algorithm>
+
+namespace rsfm_b200 {
+namespace chr {
+
+constexpr int kWarps = 8;
+constexpr int kBuf = 1024;   // candidate keys per warp buffer
+constexpr int kMaxTopK = 32;
+
+struct Img {
+    const uint8_t* desc;
+    const uint2* keys;     // n x 8 bytes
+    const uint4* codes;    // n x 128 bits
+    const uint32_t* ends;  // [8][256] inclusive upper bounds
+    const uint32_t* buckets;  // [8][n]: bucket (s, b) at buckets[s*n + lower(s,b)]
+    const uint32_t* sqr;
+    uint32_t n;
+};
+
+// Bytes equal in a and b -> bit set per byte (4 bits for 4 bytes of each word).
+__device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
+    const uint32_t x = a ^ b;
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) m |= ((x >> (8 * k)) & 0xFFu) == 0 ? (1u << k) : 0u;
+    return m;
+}
+
+__global__ void __launch_bounds__(32 * kWarps) ranked_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
+                                                             uint32_t ratioNum, uint32_t ratioDen,
+                                                             unsigned long long* __restrict__ best,
+                                                             uint32_t* __restrict__ second, uint32_t* __restrict__ flags,
+                                                             uint32_t* __restrict__ nbCand) {
+    __shared__ uint32_t buf[kWarps][kBuf];
+    __shared__ uint32_t top[kWarps][kMaxTopK];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t* B = buf[warp];
+    uint32_t* TOP = top[warp];
+    const uint32_t lt = (1u << lane) - 1u;
+
+    for (uint32_t i = blockIdx.x * kWarps + warp; i < Q.n; i += gridDim.x * kWarps) {
+        const uint2 qk = Q.keys[i];
+        const uint4 qc = Q.codes[i];
+        uint32_t cnt = 0, nTop = 0, total = 0;
+
+        // Extract the topK smallest keys of buffer + running top into TOP (lane r keeps round r's).
+        auto select = [&]() {
+            uint32_t prev = 0, have = 0, mine = 0xFFFFFFFFu;
+            const uint32_t want = min(topK, cnt + nTop);
+            for (uint32_t r = 0; r < want; ++r) {
+                uint32_t mn = 0xFFFFFFFFu;
+                for (uint32_t x = lane; x < cnt; x += 32) {
+                    const uint32_t v = B[x];
+                    if ((have == 0 || v > prev) && v < mn) mn = v;
+                }
+                if (lane < nTop) {
+                    const uint32_t v = TOP[lane];
+                    if ((have == 0 || v > prev) && v < mn) mn = v;
+                }
+                mn = __reduce_min_sync(0xffffffffu, mn);
+                prev = mn;
+                have = 1;
+                if (lane == r) mine = mn;
+            }
+            __syncwarp();
+            if (lane < want) TOP[lane] = mine;
+            __syncwarp();
+            nTop = want;
+            cnt = 0;
+        };
+
+        for (uint32_t s = 0; s < tables; ++s) {
+            const uint32_t bk = s < 4 ? (qk.x >> (8 * s)) & 0xFFu : (qk.y >> (8 * (s - 4))) & 0xFFu;
+            const uint32_t lo = bk ? T.ends[s * 256 + bk - 1] : 0u, hi = T.ends[s * 256 + bk];
+            const uint32_t* list = T.buckets + size_t(s) * T.n;
+            for (uint32_t x0 = lo; x0 < hi; x0 += 32) {
+                const uint32_t x = x0 + lane;
+                bool keep = false;
+                uint32_t key = 0;
+                if (x < hi) {
+                    const uint32_t j = list[x];
+                    const uint2 tk = T.keys[j];
+                    const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
+                    keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
+                    if (keep) {
+                        const uint4 tc = T.codes[j];
+                        const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
+                                           __popc(tc.w ^ qc.w);
+                        key = (h << 24) | j;
+                    }
+                }
+                const uint32_t m = __ballot_sync(0xffffffffu, keep);
+                if (cnt + __popc(m) > kBuf) select();
+                if (keep) B[cnt + __popc(m & lt)] = key;
+                cnt += __popc(m);
+                total += __popc(m);
+                __syncwarp();
+            }
+        }
+        select();
+        // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
+        const uint32_t qw = reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128)[lane];
+        const uint32_t nq = Q.sqr[i];
+        uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+        for (uint32_t r = 0; r < nTop; ++r) {
+            const uint32_t j = TOP[r] & 0xFFFFFFu;
+            const uint32_t tw = reinterpret_cast<const uint32_t*>(T.desc + size_t(j) * 128)[lane];
+            uint32_t dot = __dp4a(qw, tw, 0u);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            const uint32_t d = nq + T.sqr[j] - 2u * dot;
+            if (d < bd || (d == bd && j < bj)) {
+                sd = bd;
+                bd = d;
+                bj = j;
+            } else if (d < sd) {
+                sd = d;
+            }
+        }
+        if (lane == 0) {
+            best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
+            second[i] = sd;
+            uint32_t f = 0;
+            if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+            flags[i] = f;
+            if (nbCand) nbCand[i] = total;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace chr
+}  // namespace rsfm_b200
+
+using namespace rsfm_b200;
+
+extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const rsfm_ranked_image* train,
+                                         uint32_t nbTables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
+                                         rsfm_best_match* best, uint32_t* secondDist, uint32_t* flags,
+                                         uint32_t* nbCandidates, cudaStream_t stream) {
+    launch_count_reset();
+    if (!query || !train || nbTables == 0 || nbTables > 8 || topK == 0 || topK > uint32_t(chr::kMaxTopK))
+        return RSFM_ERR_INVALID_ARG;
+    if (query->nbDesc == 0) return RSFM_OK;
+    if (!best || !secondDist || !flags) return RSFM_ERR_INVALID_ARG;
+    if (train->nbDesc >= (1u << 24)) return RSFM_ERR_CAPACITY;  // index shares a word with the distance
+    auto mk = [](const rsfm_ranked_image* m) {
+        chr::Img I;
+        I.desc = static_cast<const uint8_t*>(m->desc);
+        I.keys = reinterpret_cast<const uint2*>(m->keys);
+        I.codes = reinterpret_cast<const uint4*>(m->codes);
+        I.ends = m->bucketEnds;
+        I.buckets = m->buckets;
+        I.sqr = m->sqrNormDesc;
+        I.n = m->nbDesc;
+        return I;
+    };
+    const chr::Img Q = mk(query), T = mk(train);
+    if (!Q.desc || !Q.keys || !Q.codes || !Q.sqr) return RSFM_ERR_INVALID_ARG;
+    if (train->nbDesc && (!T.desc || !T.keys || !T.codes || !T.ends || !T.buckets || !T.sqr))
+        return RSFM_ERR_INVALID_ARG;
+    const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
+    void* tok = nullptr;
+    const bool prof = profile_begin(stream, &tok);
+    chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen,
+                                                             reinterpret_cast<unsigned long long*>(best), secondDist,
+                                                             flags, nbCandidates);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    if (prof) profile_end(stream, tok);
+    launch_count_add(1);
+    return RSFM_OK;
+}

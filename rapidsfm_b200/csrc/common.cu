@@ -2,10 +2,16 @@
 #include "common.h"
 #include <cudaTypedefs.h>
 #include <mutex>
+#include <cstdio>
 
 namespace rsfm_b200 {
 
 static thread_local uint32_t t_launches = 0;
+static thread_local char t_last_error[256] = "";
+
+void set_last_cuda_error(cudaError_t e, const char* where) {
+    snprintf(t_last_error, sizeof(t_last_error), "%s (%s)", cudaGetErrorString(e), where);
+}
 void launch_count_reset() { t_launches = 0; }
 void launch_count_add(uint32_t n) { t_launches += n; }
 
@@ -94,3 +100,5 @@ extern "C" const char* rsfm_status_string(int status) {
 }
 
 extern "C" uint32_t rsfm_last_launch_count(void) { return t_launches; }
+
+extern "C" const char* rsfm_last_cuda_error(void) { return t_last_error; }

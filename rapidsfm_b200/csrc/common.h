@@ -13,12 +13,18 @@ namespace rsfm_b200 {
 void launch_count_reset();
 void launch_count_add(uint32_t n);
 
+// Remembers the last failing CUDA call of this host thread (rsfm_last_cuda_error).
+void set_last_cuda_error(cudaError_t e, const char* where);
+
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA; }
 
-#define RSFM_CUDA_TRY(expr)                          \
-    do {                                             \
-        cudaError_t _e = (expr);                     \
-        if (_e != cudaSuccess) return RSFM_ERR_CUDA; \
+#define RSFM_CUDA_TRY(expr)                        \
+    do {                                           \
+        cudaError_t _e = (expr);                   \
+        if (_e != cudaSuccess) {                   \
+            ::rsfm_b200::set_last_cuda_error(_e, #expr); \
+            return RSFM_ERR_CUDA;                  \
+        }                                          \
     } while (0)
 
 // 2D uint8 tensor map over an array of `rows` descriptors of 128 bytes, tile = boxRows x 128

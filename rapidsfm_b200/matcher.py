@@ -94,6 +94,41 @@ def bf_match_ext(tasks, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08, stream=N
     return tasks
 
 
+class BFPlan:
+    """A batch of pairs matched by one persistent, CUDA-graph-captured launch (rsfm_bf_plan_*)."""
+
+    def __init__(self, tasks, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08, row_tiles=0, col_blocks=0,
+                 epilogue_groups=0, use_graph=True):
+        lib = _lib.load()
+        self.tasks = tasks
+        for t in tasks:
+            n = t.descA.shape[0]
+            if t.secondA is None or t.secondA.numel() != n:
+                t.secondA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+                t.flagsA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+        arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+        sec = (ctypes.c_void_p * len(tasks))(*[t.secondA.data_ptr() for t in tasks])
+        flg = (ctypes.c_void_p * len(tasks))(*[t.flagsA.data_ptr() for t in tasks])
+        opts = _lib.BFPlanOptions(row_tiles, col_blocks, epilogue_groups, 1 if use_graph else 0)
+        self._h = ctypes.c_void_p(0)
+        _lib.check(lib.rsfm_bf_plan_create(arr, len(tasks), sec, flg, ratio_num, ratio_den, ctypes.byref(opts),
+                                           ctypes.byref(self._h)), "rsfm_bf_plan_create")
+
+    def launch(self, stream=None):
+        _lib.check(_lib.load().rsfm_bf_plan_launch(self._h, _stream_ptr(stream)), "rsfm_bf_plan_launch")
+
+    def close(self):
+        if self._h:
+            _lib.load().rsfm_bf_plan_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def unpack_best(best):
     """int64 BestMatch view -> (index uint32 ndarray, distance uint32 ndarray)."""
     a = best.cpu().numpy().view(np.uint32).reshape(-1, 2)
