@@ -23,6 +23,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -114,16 +116,28 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(q, t, rows, threads):
-    """Times the oracle port (exhaustive exact loop + cross-check) on `rows` query rows."""
+def cpu_baseline(q, t, rows, threads, min_seconds=0.0):
+    """Times the oracle port (exhaustive exact bidirectional loop) on `rows` query rows against the
+    whole train set, repeated until `min_seconds` of CPU work have run. Returns (pairs/s, seconds)."""
     from oracle import oracle as orc
     orc.load()
-    sub = q[:rows]
+    sub = np.ascontiguousarray(q[:rows])
     orc.bf_match(sub[:8], t, threads=threads)  # warm
-    t0 = time.perf_counter()
-    fwd, bwd, sec = orc.bf_match(sub, t, threads=threads)
-    dt = time.perf_counter() - t0
-    return rows * len(t) / dt, dt
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        orc.bf_match(sub, t, threads=threads)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_seconds:
+            break
+    return reps * rows * len(t) / dt, dt
+
+
+def _cpu_sample(q, t, threads, seconds):
+    """Rows per run so one run takes about `seconds` (whole pair when faster), and the timing."""
+    rate, _ = cpu_baseline(q, t, 256, threads)
+    rows = int(max(256, min(len(q), rate * seconds / len(t))))
+    return rows, cpu_baseline(q, t, rows, threads, min_seconds=seconds)
 
 
 def run_reference(args):
@@ -134,18 +148,20 @@ def run_reference(args):
         return
     q, t, _ = synth.make_pair(N_QUERY, N_TRAIN, OVERLAP, SIGMA, seed=1)
     threads = os.cpu_count() or 1
-    # size each step's sample to at most ~5 s of CPU work (the whole pair when it is faster)
-    rate, dt = cpu_baseline(q, t, 64, threads)
-    rows = int(max(64, min(N_QUERY, rate * 5.0 / len(t))))
+    # each step: a bounded sample so the whole run stays near two minutes (whole pair per run
+    # when one pass is that fast, else the leading query rows)
+    per_step = min(10.0, max(0.3, 120.0 / max(1, args.steps)))
+    rows, _ = _cpu_sample(q, t, threads, per_step)
     vals = []
     for _ in range(args.warmup):
-        cpu_baseline(q, t, min(rows, 64), threads)
+        cpu_baseline(q, t, min(rows, 256), threads)
     for _ in range(args.steps):
-        v, _ = cpu_baseline(q, t, rows, threads)
+        v, _ = cpu_baseline(q, t, rows, threads, min_seconds=per_step)
         vals.append(v)
     value = statistics.median(vals)
     ms_per_step = N_QUERY * N_TRAIN / value * 1e3
-    sample = f"{rows} query rows x {N_TRAIN} train of the {N_QUERY}x{N_TRAIN} pair, exact bidirectional"
+    sample = (f"{rows} query rows x {N_TRAIN} train of the {N_QUERY}x{N_TRAIN} pair per run, exact bidirectional, "
+              "runs repeated to fill each step")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -310,11 +326,9 @@ def run_ours(args):
         "ops_per_launch": nops,
     }
 
-    # ---- CPU baseline: oracle port, all host threads, on as many query rows as fit in ~10 s
+    # ---- CPU baseline: oracle port, all host threads, about 10 s of work on the same pair
     threads = os.cpu_count() or 1
-    rate, _ = cpu_baseline(q, t, 64, threads)
-    rows = int(max(64, min(N_QUERY, rate * 10.0 / N_TRAIN)))
-    cpu_val, cpu_dt = cpu_baseline(q, t, rows, threads)
+    rows, (cpu_val, cpu_dt) = _cpu_sample(q, t, threads, 10.0)
 
     line = {
         "metric": METRIC,
@@ -335,7 +349,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "desc-pairs/s", "cores": threads, "kind": "port",
-                         "sample": f"{rows} query rows x {N_TRAIN} train of the pair ({cpu_dt:.1f} s)"},
+                         "sample": f"{rows} query rows x {N_TRAIN} train of the pair, repeated for {cpu_dt:.1f} s"},
         "clocks": clocks,
         "int8_tops_effective": nops / (ms_per_step * 1e-3) / 1e12,
     }

@@ -210,6 +210,45 @@ int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const rsfm_ranked_
                               uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, rsfm_best_match* best,
                               uint32_t* secondDist, uint32_t* flags, uint32_t* nbCandidates, cudaStream_t stream);
 
+/* Learned hash (no reference counterpart; replaces cascade hashing's random projection with a
+ * trained 128 -> 256 -> 128 MLP). Weights on the device: w1 bf16 [256][128], b1 f32 [256],
+ * w2 bf16 [128][256], b2 f32 [128]. x = desc / 64; h = bf16(relu(w1 x + b1)); o = w2 h + b2;
+ * code bit c = [o_c > 0]. */
+typedef struct rsfm_mlp {
+    const void* w1;
+    const float* b1;
+    const void* w2;
+    const float* b2;
+} rsfm_mlp;
+
+/* Hashes nbDesc descriptors (16-byte aligned): codes = 4 x uint32 per descriptor (required, 16-byte
+ * aligned), keys = the first 8 code bytes per descriptor (the 8 bucket keys; optional), outputs =
+ * the 128 pre-sign values as f32 (optional, for tests). Tensor cores, fp32 accumulation. */
+int rsfm_mlp_hash(const rsfm_mlp* model, const void* desc, uint32_t nbDesc, uint8_t* keys, uint32_t* codes,
+                  float* outputs, cudaStream_t stream);
+
+/* Triplet trainer for the learned hash. Parameters are one f32 block w1 | b1 | w2 | b2
+ * (32768 + 256 + 32768 + 128 floats); the trainer keeps fp32 masters, Adam moments (beta 0.9 /
+ * 0.999, eps 1e-8) and the bf16 copies the hash reads. Loss per triplet (anchor, positive,
+ * negative), z = tanh(o): max(0, margin + |z_a - z_p|^2/4 - |z_a - z_n|^2/4), averaged over the
+ * batch; gradients pass the bf16 rounding of h as the identity. A step gathers rows ia/ip/in of
+ * the descriptor sets a/p/n (device arrays of `batch` indices), computes the gradients and applies
+ * Adam, all enqueued on `stream` (no host synchronization). */
+typedef struct rsfm_mlp_trainer rsfm_mlp_trainer;
+int rsfm_mlp_trainer_create(const float* initParamsHost, uint32_t batch, float lr, float margin,
+                            rsfm_mlp_trainer** trainer);
+int rsfm_mlp_trainer_model(const rsfm_mlp_trainer* trainer, rsfm_mlp* model);
+int rsfm_mlp_trainer_step(rsfm_mlp_trainer* trainer, const void* a, const uint32_t* ia, const void* p,
+                          const uint32_t* ip, const void* n, const uint32_t* in, float* lossDevice,
+                          cudaStream_t stream);
+/* Loss and gradients of one batch without updating (synchronizes; gradsHost in the parameter
+ * block layout, lossHost one float; either may be NULL). */
+int rsfm_mlp_trainer_gradients(rsfm_mlp_trainer* trainer, const void* a, const uint32_t* ia, const void* p,
+                               const uint32_t* ip, const void* n, const uint32_t* in, float* gradsHost,
+                               float* lossHost, cudaStream_t stream);
+int rsfm_mlp_trainer_params(const rsfm_mlp_trainer* trainer, float* paramsHost);
+int rsfm_mlp_trainer_destroy(rsfm_mlp_trainer* trainer);
+
 /* Reads and clears the device-side error word of the current device (synchronizes the device).
  * 0 = no error; nonzero = a kernel's bounded wait timed out (code identifies the wait). */
 int rsfm_device_error(uint32_t* code);

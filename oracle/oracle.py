@@ -25,7 +25,8 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
+    srcs = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith(".cpp") or f == "Makefile"]
+    if not os.path.exists(LIB_PATH) or any(os.path.getmtime(f) > os.path.getmtime(LIB_PATH) for f in srcs):
         build()
     lib = ctypes.CDLL(LIB_PATH)
     u32, i32, u64 = ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint64
@@ -45,6 +46,8 @@ def load():
         "orc_cashash_build_buckets": (None, [_P, u32, _P, _P]),
         "orc_cashash_find_best_match": (None, [_P, u32, _P, _P, _P, u32, _P, _P, _P, _P, ctypes.c_int]),
         "orc_cashash_match_ranked": (None, [_P, _P, _P, u32, _P, _P, _P, u32, i32, i32, u32, u32, _P, _P, _P, _P]),
+        "orc_mlp_forward": (None, [_P, _P, _P, _P, _P, u32, _P, _P]),
+        "orc_mlp_triplet_grad": (ctypes.c_double, [_P, _P, _P, _P, _P, _P, _P, u32, ctypes.c_float, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -186,6 +189,50 @@ def cashash_match_ranked(q_desc, q_keys, q_codes, t_desc, t_keys, t_codes, table
                                     len(t_desc), tables, top_k, ratio_num, ratio_den, _c(best), _c(second),
                                     _c(flags), _c(ncand))
     return best, second, flags, ncand
+
+
+# ---------------------------------------------------------------- learned hash MLP
+MLP_SIZES = (256 * 128, 256, 128 * 256, 128)  # parameter block: w1 | b1 | w2 | b2
+
+
+def mlp_split(params):
+    """Splits an f32 parameter block into (w1, b1, w2, b2) views."""
+    out, o = [], 0
+    for n in MLP_SIZES:
+        out.append(params[o:o + n])
+        o += n
+    return out
+
+
+def bf16_round(x):
+    """Round-to-nearest-even to bfloat16, returned as float32."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def mlp_forward(params, desc):
+    """params: f32 block (w1/w2 taken at bf16 precision). Returns (outputs f32 [n,128], codes u32 [n,4])."""
+    w1, b1, w2, b2 = mlp_split(np.asarray(params, dtype=np.float32))
+    w1, w2 = bf16_round(w1), bf16_round(w2)
+    desc = np.ascontiguousarray(desc, dtype=np.uint8)
+    n = len(desc)
+    out = np.empty((n, 128), dtype=np.float32)
+    codes = np.empty((n, 4), dtype=np.uint32)
+    load().orc_mlp_forward(_c(w1), _c(np.ascontiguousarray(b1)), _c(w2), _c(np.ascontiguousarray(b2)), _c(desc), n,
+                           _c(out), _c(codes))
+    return out, codes
+
+
+def mlp_triplet_grad(params, a, p, n, margin):
+    """Loss and gradient block (same layout as params) of one triplet batch, in double precision."""
+    w1, b1, w2, b2 = mlp_split(np.asarray(params, dtype=np.float32))
+    w1, w2 = bf16_round(w1), bf16_round(w2)
+    a, p, n = (np.ascontiguousarray(x, dtype=np.uint8) for x in (a, p, n))
+    g = [np.zeros(k, dtype=np.float64) for k in MLP_SIZES]
+    loss = load().orc_mlp_triplet_grad(_c(w1), _c(np.ascontiguousarray(b1)), _c(w2), _c(np.ascontiguousarray(b2)),
+                                       _c(a), _c(p), _c(n), len(a), margin, _c(g[0]), _c(g[1]), _c(g[2]), _c(g[3]))
+    return loss, np.concatenate(g)
 
 
 # ---------------------------------------------------------------- reference kernels (GPU)

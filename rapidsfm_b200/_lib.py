@@ -67,6 +67,10 @@ class BFPlanOptions(ctypes.Structure):
                 ("useGraph", ctypes.c_uint32)]
 
 
+class MLP(ctypes.Structure):
+    _fields_ = [("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p)]
+
+
 class ValidMatch(ctypes.Structure):
     """ValidMatch (bruteForceMatch.h:120-125)."""
     _fields_ = [("idxQuery", ctypes.c_uint32), ("idxTrain", ctypes.c_uint32), ("distance", ctypes.c_float)]
@@ -117,6 +121,17 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "rsfm_bf_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rsfm_mlp_hash": (ctypes.c_int, [ctypes.POINTER(MLP), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_mlp_trainer_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_float,
+                                               ctypes.POINTER(ctypes.c_void_p)]),
+    "rsfm_mlp_trainer_model": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MLP)]),
+    "rsfm_mlp_trainer_step": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_void_p,
+                                                                                        ctypes.c_void_p]),
+    "rsfm_mlp_trainer_gradients": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6 +
+                                   [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_mlp_trainer_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_mlp_trainer_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "rsfm_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)]),
     "rsfm_int8_mma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),

@@ -21,6 +21,7 @@ SOURCES = [
     "cashash.cu",
     "cashash_match.cu",
     "cashash_ranked.cu",
+    "mlp.cu",
 ]
 
 NVCC_FLAGS = [

@@ -1,0 +1,124 @@
+"""Cascade-hash host interface on top of the C ABI.
+
+Reference interfaces mirrored (paths relative to the RapidSFM source tree):
+  cashash::accumuateDesc / computeBias        casHash/cascadeHash.h:32-35   -> CasHash.fit
+  computeHashForBucketOnly / ...AndRemap      cascadeHash.h:43-56           -> CasHash.hash
+  buildHistogram / computeBucketBound /
+  buildBuckets                                cascadeHash.h:58-68           -> build_ranked_image
+  cashash::findBestMatch                      cascadeHash.h:106-107         -> rsfm_cashash_find_best_match
+Ranked matching (6 tables x 8-bit keys, 128-bit Hamming ranking, top-K exact L2 re-rank, ratio
+test) has no reference counterpart: match_ranked.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .matcher import RATIO_DEN_08, RATIO_NUM_08, _check_desc, _stream_ptr, precomp_sift_sqr_norm
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+def gaussian_weights(seed, channels=192, sigma=32.0):
+    """Random Gaussian projection rows rounded to int8 (the reference draws N(0, 32) per weight,
+    bruteForceMatcher.cpp:128), from numpy's PCG64 seeded with `seed`."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.clip(np.rint(rng.normal(0.0, sigma, size=(channels, 128))), -128, 127).astype(np.int8)
+
+
+class RankedImage:
+    """Device buffers of one image for ranked matching: desc, squared norms, 8 key bytes and a
+    128-bit code per descriptor, per-scheme bucket bounds (inclusive upper [8][256]) and lists."""
+
+    def __init__(self, desc, keys, codes, stream=None):
+        _check_desc(desc)
+        lib = _lib.load()
+        n = desc.shape[0]
+        dev = desc.device
+        s = _stream_ptr(stream)
+        self.desc, self.keys, self.codes = desc, keys, codes
+        self.sqr = precomp_sift_sqr_norm(desc, stream=stream)
+        hist = torch.empty((8, 256), dtype=torch.int32, device=dev)
+        lower = torch.empty((8, 256), dtype=torch.int32, device=dev)
+        self.upper = torch.empty((8, 256), dtype=torch.int32, device=dev)
+        self._max = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.buckets = torch.empty((8, max(n, 1)), dtype=torch.int32, device=dev)
+        _lib.check(lib.rsfm_cashash_build_histogram(_p(hist), _p(keys), n, s), "rsfm_cashash_build_histogram")
+        _lib.check(lib.rsfm_cashash_compute_bucket_bound(_p(lower), _p(self.upper), _p(self._max), _p(hist), s),
+                   "rsfm_cashash_compute_bucket_bound")
+        _lib.check(lib.rsfm_cashash_build_buckets(_p(keys), n, _p(lower), _p(self.buckets), s),
+                   "rsfm_cashash_build_buckets")
+        self.n = n
+
+    def max_bucket_size(self):
+        return int(self._max.item())
+
+    def as_ctype(self):
+        return _lib.RankedImage(self.desc.data_ptr(), self.keys.data_ptr(), self.codes.data_ptr(),
+                                self.upper.data_ptr(), self.buckets.data_ptr(), self.sqr.data_ptr(), self.n)
+
+
+def match_ranked(query, train, tables=6, top_k=10, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08,
+                 count_candidates=False, stream=None):
+    """Ranked cascade-hash matching of two RankedImages -> (best int64 [nq] (index | distance << 32),
+    second-best distance int32 [nq], flags int32 [nq] (bit0 ratio test), candidates int32 [nq] or None)."""
+    lib = _lib.load()
+    nq = query.n
+    dev = query.desc.device
+    best = torch.empty(nq, dtype=torch.int64, device=dev)
+    sec = torch.empty(nq, dtype=torch.int32, device=dev)
+    flg = torch.empty(nq, dtype=torch.int32, device=dev)
+    cnt = torch.empty(nq, dtype=torch.int32, device=dev) if count_candidates else None
+    qi, ti = query.as_ctype(), train.as_ctype()
+    _lib.check(lib.rsfm_cashash_match_ranked(ctypes.byref(qi), ctypes.byref(ti), tables, top_k, ratio_num, ratio_den,
+                                             _p(best), _p(sec), _p(flg), _p(cnt), _stream_ptr(stream)),
+               "rsfm_cashash_match_ranked")
+    return best, sec, flg, cnt
+
+
+class CasHash:
+    """Random-projection cascade hash: 192 int8 projection rows (64 for the 8 bucket-key bytes, 128
+    for the remap code) with biases centred on the running descriptor mean, as the reference's
+    matcher keeps them (bruteForceMatcher.cpp:96-101: accumulate, then computeBias per image)."""
+
+    def __init__(self, weights, bias_base=None, device="cuda"):
+        w = np.ascontiguousarray(weights, dtype=np.int8)
+        if w.shape not in ((64, 128), (192, 128)):
+            raise ValueError("weights must be int8 [64 or 192, 128]")
+        self.channels = w.shape[0]
+        dev = torch.device(device)
+        self.w = torch.from_numpy(w.copy()).to(dev)
+        base = np.zeros(self.channels, np.int32) if bias_base is None else np.asarray(bias_base, np.int32)
+        self.base = torch.from_numpy(base.copy()).to(dev)
+        self.bias = torch.zeros(self.channels, dtype=torch.int32, device=dev)
+        self.acc = torch.zeros(128, dtype=torch.int64, device=dev)
+        self.nb_desc = 0
+
+    def fit(self, desc, stream=None):
+        """Adds `desc` to the running accumulator and recomputes the biases."""
+        _check_desc(desc)
+        lib = _lib.load()
+        s = _stream_ptr(stream)
+        _lib.check(lib.rsfm_cashash_accumulate_desc(_p(self.acc), int(self.nb_desc == 0), _p(desc), desc.shape[0], s),
+                   "rsfm_cashash_accumulate_desc")
+        self.nb_desc += desc.shape[0]
+        _lib.check(lib.rsfm_cashash_compute_bias(_p(self.bias), _p(self.w), _p(self.base), _p(self.acc), self.nb_desc,
+                                                 self.channels, s), "rsfm_cashash_compute_bias")
+
+    def hash(self, desc, stream=None):
+        """desc -> (keys uint8 [n,8], codes int32 [n,4] (None for 64 channels))."""
+        _check_desc(desc)
+        lib = _lib.load()
+        n = desc.shape[0]
+        keys = torch.empty((max(n, 1), 8), dtype=torch.uint8, device=desc.device)
+        codes = torch.empty((max(n, 1), 4), dtype=torch.int32, device=desc.device) if self.channels == 192 else None
+        _lib.check(lib.rsfm_cashash_compute_hash(_p(self.w), _p(self.bias), self.channels, _p(desc), n, _p(keys),
+                                                 _p(codes), None, _stream_ptr(stream)), "rsfm_cashash_compute_hash")
+        return keys[:n], (codes[:n] if codes is not None else None)
+
+    def ranked_image(self, desc, stream=None):
+        keys, codes = self.hash(desc, stream=stream)
+        return RankedImage(desc, keys, codes, stream=stream)
