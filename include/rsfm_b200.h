@@ -69,6 +69,13 @@ int rsfm_precomp_sift_sqr_norm(uint32_t* sqrNorm, const void* desc, uint32_t nbD
  * reference: lexicographic minimum of (distance, index) in both directions. */
 int rsfm_bf_match(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream);
 
+/* Allocation-free rsfm_bf_match (no counterpart in the reference): same results, but the per-row
+ * second-best scratch is a fixed 4 MiB device array instead of stream-ordered allocations, so no
+ * call allocates device memory. At most 1 Mi query rows (sum of nbDescA) per call, else
+ * RSFM_ERR_CAPACITY. The first call on a device looks up the array's address (make it before any
+ * stream capture). All calls share the array: calls that overlap on the GPU race. */
+int rsfm_bf_match_noalloc(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream);
+
 /* Extended form of rsfm_bf_match (no reference counterpart for the extra outputs): also writes,
  * per A descriptor i of task t, secondDistA[t][i] = smallest distance to any B descriptor other
  * than the best one (~0u if nbDescB < 2) and flagsA[t][i]: bit0 = ratio test passed

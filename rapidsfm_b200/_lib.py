@@ -80,6 +80,7 @@ class ValidMatch(ctypes.Structure):
 SIGNATURES = {
     "rsfm_precomp_sift_sqr_norm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_bf_match": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
+    "rsfm_bf_match_noalloc": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
     "rsfm_bf_match_ext": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t,
                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),

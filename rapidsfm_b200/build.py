@@ -16,6 +16,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 SOURCES = [
     "common.cu",
     "bf_match.cu",
+    "bf_match_noalloc.cu",
     "host_filters.cpp",
     "diag.cu",
     "cashash.cu",
