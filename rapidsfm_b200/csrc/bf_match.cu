@@ -11,17 +11,17 @@
 // Extension (no reference counterpart): per A row the second-smallest distance, used by the
 // ratio test; flags for the ratio test and the cross-check.
 //
-// Work decomposition. A "unit" is a block of up to kMaxRowTiles*128 A rows times a range of
-// 128-column B blocks. Persistent CTAs take units round-robin. Per CTA:
-//   warp 0      TMA producer: A row tiles (resident for the unit), B column blocks (3-stage ring)
+// Work decomposition. A "unit" is a block of up to kMaxRowTiles*128 A rows times a range of up to
+// kMaxColBlocks 128-column B blocks. Persistent CTAs take units round-robin. Per CTA:
+//   warp 0      TMA producer: A row tiles (resident for the unit), B column blocks (ring)
 //   warp 1      TMEM allocator and UMMA issuer (one thread): per (B block, A row tile) one
-//               128x128x128 int8 product into a double-buffered TMEM accumulator
-//   warps 2..17 epilogue, four warpgroups; warpgroup w owns columns [32w, 32w+32) of every tile
+//               128x128x128 int8 product into one of four TMEM accumulators
+//   warps 2..   epilogue, 2 or 4 warpgroups; warpgroup w owns 128/G columns of every tile
 // Each epilogue thread owns one TMEM lane (one A row of the tile). It keeps, in registers, a
-// column accumulator holding for each of its 32 columns the best packed column key over the
-// unit's row tiles, so the cross-lane column reduction runs once per B block instead of once per
-// tile. Row minima are thread-local; the exact row second-best needs per-chunk work only for
-// chunks that can still become the row's best.
+// column accumulator holding for each of its columns the best packed column key over the unit's
+// row tiles, so the cross-lane column reduction runs once per B block instead of once per tile.
+// Row maxima are thread-local; the exact row second-best needs per-chunk work only for chunks
+// that can still become the row's best. Row state lives in shared memory per (warpgroup, row).
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
@@ -34,16 +34,20 @@ namespace bf {
 using namespace sm100;
 
 constexpr int kMaxTasksPerLaunch = 16;
-constexpr int kMaxRowTiles = 8;        // A row tiles per unit (p fits 3 bits of the column key)
-constexpr int kBStages = 3;
+constexpr int kMaxRowTiles = 8;        // A row tiles per unit (p fits 3 bits of the keys)
 constexpr int kTileBytes = 128 * 128;  // 128 descriptors x 128 bytes
+constexpr int kUnitRows = kMaxRowTiles * 128;
+constexpr int kMaxColBlocks = 8;       // B blocks per unit
+constexpr int kUnitCols = kMaxColBlocks * 128;
+constexpr int kAccBufs = 4;            // TMEM accumulators of 128 columns (all 512 columns)
 // Epilogue warpgroups kWG in {2, 4}: warpgroup w owns 128/kWG columns of every tile, i.e.
-// kCPW = 4/kWG chunks of 32 columns per warp.
+// kCPW = 4/kWG chunks of 32 columns per warp. Four warpgroups leave room for two B stages.
 template <int kWG>
 struct Cfg {
     static constexpr int kEpiWarps = 4 * kWG;
     static constexpr int kThreads = 32 * (2 + kEpiWarps);
     static constexpr int kCPW = 4 / kWG;
+    static constexpr int kBStages = kWG == 4 ? 2 : 3;
 };
 constexpr uint32_t kMaxDist = 128u * 255u * 255u;  // largest possible squared L2 of uint8x128
 constexpr uint32_t kVBias = 1u << 23;                // makes (|b|^2 - d) + bias positive
@@ -68,7 +72,7 @@ struct Params {
     uint32_t nTasks;
     uint32_t totalUnits;
     uint32_t rowTiles;  // row tiles per unit (<= kMaxRowTiles)
-    uint32_t colBlocks; // 128-column blocks per unit
+    uint32_t colBlocks; // 128-column blocks per unit (<= kMaxColBlocks)
     uint32_t* err;
 };
 
@@ -108,17 +112,22 @@ __device__ __forceinline__ Unit decode_unit(const Params& P, uint32_t u) {
     return U;
 }
 
+template <int kWG>
 struct Smem {
     // A row tiles and B stages are 1024-byte aligned (128-byte swizzle atoms).
     uint8_t a[kMaxRowTiles][kTileBytes];
-    uint8_t b[kBStages][kTileBytes];
-    uint32_t nbk[2][128];                        // [block parity][column]: row-key addend
-    unsigned long long colmin[2][128];           // [flush parity][column]
-    unsigned long long rowbest[2][kMaxRowTiles * 128];  // [unit parity][row]: (d << 32 | j)
-    uint32_t rowsecond[2][kMaxRowTiles * 128];
+    uint8_t b[Cfg<kWG>::kBStages][kTileBytes];
+    int32_t nbk[kUnitCols];              // per unit column: row-key addend (31 - j % 32) - |b|^2 * 256
+    unsigned long long colmin[2][128];   // [block parity][column]: merge of the 4 lane quarters
+    // Row state of the current unit, per unit row r = 128 p + 32 q + lane:
+    int32_t rowc[kUnitRows];             // column-key addend ((7-p) << 5 | (31-lane)) - |a|^2 * 256
+    int32_t hint[kUnitRows];             // -(global best distance at unit start) * 256
+    int32_t l1k[kWG][kUnitRows];         // per warpgroup: best row key, second row key
+    int32_t l2k[kWG][kUnitRows];
+    uint16_t l1j[kWG][kUnitRows];        // column of the best key, relative to the unit's first column
     uint64_t aFull[kMaxRowTiles], aEmpty[kMaxRowTiles];
-    uint64_t bFull[kBStages], bEmpty[kBStages];
-    uint64_t accFull[2], accEmpty[2];
+    uint64_t bFull[Cfg<kWG>::kBStages], bEmpty[Cfg<kWG>::kBStages];
+    uint64_t accFull[kAccBufs], accEmpty[kAccBufs];
     uint64_t mmaDone;
     uint32_t tmemBase;
 };
@@ -126,19 +135,31 @@ struct Smem {
 __device__ __forceinline__ void named_bar(uint32_t id, uint32_t n) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
-__device__ __forceinline__ int redux_max_s32(int v) {
-    int r;
-    asm volatile("redux.sync.max.s32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
-    return r;
+
+// Cross-lane maximum of 32 per-lane columns: afterwards v[0] of lane l holds the maximum over
+// the 32 lanes of column l. Five butterfly levels; at each, a lane keeps the half of its
+// remaining columns selected by its lane bit and takes the maximum with its partner's copy.
+__device__ __forceinline__ void column_max_butterfly(int32_t (&v)[32], uint32_t lane) {
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool up = (lane & uint32_t(s)) != 0u;
+#pragma unroll
+        for (int i = 0; i < s; ++i) {
+            const int32_t lo = v[i], hi = v[i + s];
+            const int32_t r = __shfl_xor_sync(0xffffffffu, up ? lo : hi, s);
+            v[i] = max(up ? hi : lo, r);
+        }
+    }
 }
 
 template <int kWG>
 __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const __grid_constant__ Params P) {
     constexpr int kEpiWarps = Cfg<kWG>::kEpiWarps;
-    constexpr int kThreads = Cfg<kWG>::kThreads;
     constexpr int kCPW = Cfg<kWG>::kCPW;
+    constexpr int kBStages = Cfg<kWG>::kBStages;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    Smem<kWG>& S =
+        *reinterpret_cast<Smem<kWG>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
 
@@ -151,7 +172,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
             mbar_init(&S.bFull[s], 1);
             mbar_init(&S.bEmpty[s], 1);
         }
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < kAccBufs; ++s) {
             mbar_init(&S.accFull[s], 1);
             mbar_init(&S.accEmpty[s], kEpiWarps);
         }
@@ -162,17 +183,12 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         tmem_alloc(&S.tmemBase, 512);
         tmem_relinquish();
     }
-    for (uint32_t x = threadIdx.x; x < 2 * 128; x += kThreads) (&S.colmin[0][0])[x] = ~0ull;
-    for (uint32_t x = threadIdx.x; x < 2 * kMaxRowTiles * 128; x += kThreads) {
-        (&S.rowbest[0][0])[x] = ~0ull;
-        (&S.rowsecond[0][0])[x] = ~0u;
-    }
+    for (uint32_t x = threadIdx.x; x < 2 * 128; x += blockDim.x) (&S.colmin[0][0])[x] = ~0ull;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmemBase;
     uint32_t* err = P.err;
-    bool ok = true;
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
@@ -183,7 +199,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 const TaskDev& T = task_of(P, U.task);
                 for (uint32_t p = 0; p < U.pt; ++p) {
                     const uint32_t par = ((aUse >> p) & 1u) ^ 1u;
-                    if (!mbar_wait(&S.aEmpty[p], par, err, kDevTimeoutTmaEmpty)) ok = false;
+                    mbar_wait(&S.aEmpty[p], par, err, kDevTimeoutTmaEmpty);
                     mbar_arrive_expect_tx(&S.aFull[p], kTileBytes);
                     tma_load_2d(S.a[p], &T.tmA, &S.aFull[p], 0, int32_t(U.r0 + 128u * p));
                     aUse ^= 1u << p;
@@ -200,10 +216,10 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 const Unit U = decode_unit(P, u);
                 const TaskDev& T = task_of(P, U.task);
                 for (uint32_t b = 0; b < U.cb; ++b) {
-                    if (!mbar_wait(&S.bEmpty[stage], bPhase ^ 1u, err, kDevTimeoutTmaEmpty)) ok = false;
+                    mbar_wait(&S.bEmpty[stage], bPhase ^ 1u, err, kDevTimeoutTmaEmpty);
                     mbar_arrive_expect_tx(&S.bFull[stage], kTileBytes);
                     tma_load_2d(S.b[stage], &T.tmB, &S.bFull[stage], 0, int32_t(U.c0 + 128u * b));
-                    if (++stage == kBStages) { stage = 0; bPhase ^= 1u; }
+                    if (++stage == uint32_t(kBStages)) { stage = 0; bPhase ^= 1u; }
                 }
                 const uint32_t un = u + gridDim.x;
                 if (un < P.totalUnits) loadA(decode_unit(P, un));
@@ -217,15 +233,15 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
             for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x) {
                 const Unit U = decode_unit(P, u);
                 for (uint32_t b = 0; b < U.cb; ++b) {
-                    if (!mbar_wait(&S.bFull[stage], bPhase, err, kDevTimeoutTmaFull)) ok = false;
+                    mbar_wait(&S.bFull[stage], bPhase, err, kDevTimeoutTmaFull);
                     const uint32_t bAddr = smem_u32(S.b[stage]);
                     for (uint32_t p = 0; p < U.pt; ++p) {
                         if (b == 0) {
-                            if (!mbar_wait(&S.aFull[p], (aUse >> p) & 1u, err, kDevTimeoutTmaFull)) ok = false;
+                            mbar_wait(&S.aFull[p], (aUse >> p) & 1u, err, kDevTimeoutTmaFull);
                             aUse ^= 1u << p;
                         }
-                        const uint32_t buf = acc & 1u;
-                        if (!mbar_wait(&S.accEmpty[buf], ((acc >> 1) & 1u) ^ 1u, err, kDevTimeoutAccEmpty)) ok = false;
+                        const uint32_t buf = acc % kAccBufs;
+                        mbar_wait(&S.accEmpty[buf], ((acc / kAccBufs) & 1u) ^ 1u, err, kDevTimeoutAccEmpty);
                         tc_fence_after();
                         const uint32_t aAddr = smem_u32(S.a[p]);
                         const uint32_t d = tmem + buf * 128u;
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                         ++acc;
                     }
                     umma_commit(&S.bEmpty[stage]);
-                    if (++stage == kBStages) { stage = 0; bPhase ^= 1u; }
+                    if (++stage == uint32_t(kBStages)) { stage = 0; bPhase ^= 1u; }
                 }
             }
             // Drain: every commit issued above has arrived once this one has.
@@ -246,77 +262,98 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        // Keys are kept in "max is better" form so that the x512 scaling is a shift-add:
-        //   column key  ck = (2 a.b - |a|^2) * 256 + (7 - p)
-        //   row key     rk = ck - |b|^2 * 256 + (31 - k) * 8 = -d * 256 + (31 - k) * 8 + (7 - p)
-        // (p = row tile within the unit, k = column within the 32-column chunk). For a column, a
-        // larger ck means a smaller d, ties going to the smaller row tile; at the column flush the
-        // lane (row within the tile) is packed into bits 3..7 before the cross-lane maximum. For a
-        // row, a chunk's maximum rk gives the chunk's minimum d and, in its low bits, its lowest
-        // column.
+        // Keys are kept in "max is better" form. For thread (q, lane) and row tile p let
+        //   c = (7 - p) << 5 | (31 - lane)                 (8 bits, constant per thread and tile)
+        //   column key  ck = (2 a.b - |a|^2) * 256 + c     = (dot << 9) + rowc
+        //   row key     rk = ck + (31 - k) - |b|^2 * 256   = -d * 256 + c + (31 - k)
+        // (k = column within the 32-column chunk). A column's maximum ck over (p, lane) is its
+        // smallest d, ties going to the smallest row (p first, then lane): the column flush needs
+        // no repacking. Within one thread and tile c is constant and c + (31 - k) < 287, so row
+        // keys of one chunk order by (d, k); u = rk - c = -d * 256 + (31 - k) decodes both.
         //
-        // Row state per (thread, row tile), in row-key space: l1k/l1j = best key and its column,
-        // l2k = second key (only its distance matters), tk = slow-path threshold. A chunk does
-        // extra work only if its minimum could become this unit's best AND can still tie or beat
-        // the global best so far (read from bestA, refreshed every B block); every other chunk
-        // contributes its minimum to the second-best value only. This is exact: a chunk that
-        // cannot hold the best holds at most one value that matters, its minimum.
+        // Row state lives in shared memory, per warpgroup and unit row: l1k = best row key,
+        // l1j = its column, l2k = max over the other keys that can matter for the second-best.
+        // A chunk does extra work only if its maximum beats this warpgroup's best AND can still
+        // tie or beat the global best known at unit start (hint); every other chunk contributes
+        // its maximum to l2k only. This is exact: a chunk that cannot hold the best holds at most
+        // one value that matters, its maximum.
         const uint32_t e = warp - 2u;                    // epilogue warp
         const uint32_t wg = e >> 2;                      // warpgroup: columns [32 kCPW wg, +32 kCPW)
         const uint32_t q = warp & 3u;                    // TMEM lane quarter
-        const uint32_t t512 = e * 32u + lane;
-        const uint32_t t128 = (e & 3u) * 32u + lane;
+        const uint32_t tE = e * 32u + lane;              // 0 .. 32 kEpiWarps - 1
+        const uint32_t t128 = q * 32u + lane;            // row within a tile
         const uint32_t laneBase = (32u * q) << 16;
-        uint32_t acc = 0, blk = 0, unitPar = 0;
-        for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x, unitPar ^= 1u) {
+        constexpr int kRowIt = kUnitRows / (32 * kEpiWarps);
+        constexpr int kColIt = (kUnitCols + 32 * kEpiWarps - 1) / (32 * kEpiWarps);
+        uint32_t acc = 0, blk = 0;
+        for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x) {
             const Unit U = decode_unit(P, u);
             const TaskDev& T = task_of(P, U.task);
-            int32_t rowc[kMaxRowTiles], tk[kMaxRowTiles], l1k[kMaxRowTiles], l2k[kMaxRowTiles];
-            uint32_t l1j[kMaxRowTiles];
+            // ---- unit start: row state, row hints, column addends (all loads issued together)
+            uint32_t na[kRowIt], h1[kRowIt], nb[kColIt];
 #pragma unroll
-            for (int p = 0; p < kMaxRowTiles; ++p) {
-                const uint32_t i = U.r0 + 128u * p + 32u * q + lane;
-                const bool valid = (uint32_t(p) < U.pt) && (i < T.nA);
-                rowc[p] = valid ? int32_t(uint32_t(7 - p) - (T.sqrA[i] << 8)) : (INT32_MIN + 7 - p);
-                tk[p] = valid ? INT32_MIN : INT32_MAX;
-                l1k[p] = INT32_MIN;
-                l2k[p] = INT32_MIN;
-                l1j[p] = ~0u;
+            for (int it = 0; it < kRowIt; ++it) {
+                const uint32_t r = tE + uint32_t(it) * 32u * kEpiWarps;
+                const uint32_t i = U.r0 + r;
+                const bool valid = (r >> 7) < U.pt && i < T.nA;
+                na[it] = valid ? __ldg(&T.sqrA[i]) : 0u;
+                h1[it] = valid ? uint32_t(__ldcg(&T.bestA[i]) >> 32) : kMaxDist;
             }
+#pragma unroll
+            for (int it = 0; it < kColIt; ++it) {
+                const uint32_t x = tE + uint32_t(it) * 32u * kEpiWarps;
+                const uint32_t j = U.c0 + x;
+                nb[it] = (x < 128u * U.cb && j < T.nB) ? __ldg(&T.sqrB[j]) : 0u;
+            }
+#pragma unroll
+            for (int it = 0; it < kRowIt; ++it) {
+                const uint32_t r = tE + uint32_t(it) * 32u * kEpiWarps;
+                const uint32_t p = r >> 7, ln = r & 31u;
+                const uint32_t c = ((7u - p) << 5) | (31u - ln);
+                const uint32_t i = U.r0 + r;
+                const bool valid = p < U.pt && i < T.nA;
+                S.rowc[r] = valid ? int32_t(c - (na[it] << 8)) : int32_t(0x80000000u | c);
+                S.hint[r] = int32_t(0u - (min(h1[it], kMaxDist) << 8));
+#pragma unroll
+                for (int w = 0; w < kWG; ++w) {
+                    S.l1k[w][r] = INT32_MIN;
+                    S.l2k[w][r] = INT32_MIN;
+                    S.l1j[w][r] = 0xFFFFu;
+                }
+            }
+#pragma unroll
+            for (int it = 0; it < kColIt; ++it) {
+                const uint32_t x = tE + uint32_t(it) * 32u * kEpiWarps;
+                if (x < uint32_t(kUnitCols)) S.nbk[x] = int32_t((31u - (x & 31u)) - (nb[it] << 8));
+            }
+            named_bar(1, 32 * kEpiWarps);
             for (uint32_t b = 0; b < U.cb; ++b, ++blk) {
                 const uint32_t bpar = blk & 1u;
                 const uint32_t blockBase = U.c0 + 128u * b;
                 const uint32_t jw = blockBase + 32u * kCPW * wg;  // first column of this warp
-                if (t512 < 128) {
-                    const uint32_t j = blockBase + t512;
-                    S.nbk[bpar][t512] = j < T.nB ? (((31u - (j & 31u)) << 3) - (T.sqrB[j] << 8)) : 0u;
-                }
-                // Refresh the slow-path thresholds from the global best so far.
-#pragma unroll
-                for (int p = 0; p < kMaxRowTiles; ++p) {
-                    const uint32_t i = U.r0 + 128u * p + 32u * q + lane;
-                    if (uint32_t(p) < U.pt && i < T.nA) {
-                        const uint32_t h1 = min(uint32_t(__ldcg(&T.bestA[i]) >> 32), kMaxDist);
-                        tk[p] = max(tk[p], int32_t(0u - (h1 << 8)));
-                    }
-                }
-                named_bar(1, 32 * kEpiWarps);
                 int32_t ca[32 * kCPW];
 #pragma unroll
                 for (int k = 0; k < 32 * kCPW; ++k) ca[k] = INT32_MIN;
 #pragma unroll 1
                 for (uint32_t p = 0; p < U.pt; ++p) {
-                    const int32_t rowcP = rowc[p];
-                    int32_t tkP = tk[p], l1kP = l1k[p], l2kP = l2k[p];
-                    uint32_t l1jP = l1j[p];
-                    const uint32_t buf = acc & 1u;
-                    if (!mbar_wait(&S.accFull[buf], (acc >> 1) & 1u, err, kDevTimeoutAccFull)) ok = false;
+                    const uint32_t r = 128u * p + t128;
+                    const int32_t rowcP = S.rowc[r];
+                    const uint32_t c = uint32_t(rowcP) & 255u;
+                    int32_t l1kP = S.l1k[wg][r], l2kP = S.l2k[wg][r];
+                    uint32_t l1jP = S.l1j[wg][r];
+                    // Trigger threshold: strictly better than this warpgroup's best (its columns
+                    // come in increasing order), and no worse than the global best.
+                    const int32_t own = l1kP == INT32_MIN ? INT32_MIN
+                                                          : int32_t((uint32_t(l1kP) - ((uint32_t(l1kP) - c) & 255u)) + 256u);
+                    int32_t tkP = (U.r0 + r < T.nA) ? max(own, int32_t(uint32_t(S.hint[r]) + c)) : INT32_MAX;
+                    const uint32_t buf = acc % kAccBufs;
+                    mbar_wait(&S.accFull[buf], (acc / kAccBufs) & 1u, err, kDevTimeoutAccFull);
                     tc_fence_after();
                     uint32_t x[32 * kCPW];
 #pragma unroll
-                    for (int c = 0; c < kCPW; ++c)
-                        tmem_ld32(tmem + laneBase + buf * 128u + 32u * (kCPW * wg + c),
-                                  *reinterpret_cast<uint32_t(*)[32]>(&x[32 * c]));
+                    for (int cc = 0; cc < kCPW; ++cc)
+                        tmem_ld32(tmem + laneBase + buf * 128u + 32u * (kCPW * wg + cc),
+                                  *reinterpret_cast<uint32_t(*)[32]>(&x[32 * cc]));
                     tmem_wait_ld();
                     // The accumulator is in registers now: hand the TMEM buffer back to the MMA.
                     tc_fence_before();
@@ -324,24 +361,26 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                     if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
                     ++acc;
 #pragma unroll
-                    for (int c = 0; c < kCPW; ++c) {
-                        const uint32_t j0 = jw + 32u * c;
+                    for (int cc = 0; cc < kCPW; ++cc) {
+                        const uint32_t j0 = jw + 32u * cc;
                         int32_t m[4] = {INT32_MIN, INT32_MIN, INT32_MIN, INT32_MIN};
-                        const uint4* nb4 = reinterpret_cast<const uint4*>(&S.nbk[bpar][j0 - blockBase]);
+                        const int4* nb4 = reinterpret_cast<const int4*>(&S.nbk[j0 - U.c0]);
 #pragma unroll
-                        for (int k4 = 0; k4 < 8; ++k4) {
-                            const uint4 nb = nb4[k4];
-                            const uint32_t nbv[4] = {nb.x, nb.y, nb.z, nb.w};
+                        for (int k8 = 0; k8 < 4; ++k8) {
+                            const int4 va = nb4[2 * k8], vb = nb4[2 * k8 + 1];
+                            const int32_t nbv[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+                            int32_t rk[8];
 #pragma unroll
-                            for (int e4 = 0; e4 < 4; ++e4) {
-                                const int k = 32 * c + 4 * k4 + e4;
+                            for (int e8 = 0; e8 < 8; ++e8) {
+                                const int k = 32 * cc + 8 * k8 + e8;
                                 // Modular 32-bit arithmetic: the true keys always fit in int32.
-                                const uint32_t ck = (x[k] << 9) + uint32_t(rowcP);
-                                ca[k] = max(ca[k], int32_t(ck));
-                                const int32_t rk = int32_t(ck + nbv[e4]);
-                                m[e4] = max(m[e4], rk);
-                                x[k] = uint32_t(rk);
+                                const int32_t ck = int32_t((x[k] << 9) + uint32_t(rowcP));
+                                ca[k] = max(ca[k], ck);
+                                rk[e8] = int32_t(uint32_t(ck) + uint32_t(nbv[e8]));
+                                x[k] = uint32_t(rk[e8]);
                             }
+#pragma unroll
+                            for (int e4 = 0; e4 < 4; ++e4) m[e4] = __vimax3_s32(m[e4], rk[e4], rk[e4 + 4]);
                         }
                         int32_t rmax = max(max(m[0], m[1]), max(m[2], m[3]));
                         // Columns past nbDescB only occur in a task's last block: drop them there.
@@ -349,8 +388,8 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             rmax = INT32_MIN;
 #pragma unroll
                             for (int k = 0; k < 32; ++k) {
-                                if (j0 + k >= T.nB) x[32 * c + k] = uint32_t(INT32_MIN);
-                                rmax = max(rmax, int32_t(x[32 * c + k]));
+                                if (j0 + k >= T.nB) x[32 * cc + k] = uint32_t(INT32_MIN);
+                                rmax = max(rmax, int32_t(x[32 * cc + k]));
                             }
                         }
                         if (__any_sync(0xffffffffu, rmax >= tkP)) {
@@ -358,13 +397,13 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             // min over k of (rmax - 1 - key) (unsigned) skips exactly the maximum.
                             uint32_t mn = 0xFFFFFFFFu;
 #pragma unroll
-                            for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(rmax) - 1u - x[32 * c + k]);
+                            for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(rmax) - 1u - x[32 * cc + k]);
                             const int32_t s2 = int32_t(uint32_t(rmax) - 1u - mn);
                             if (rmax >= tkP) {
                                 l2kP = max(max(l2kP, l1kP), s2);
                                 l1kP = rmax;
-                                l1jP = j0 + 31u - ((uint32_t(rmax) >> 3) & 31u);
-                                tkP = max(tkP, int32_t((uint32_t(rmax) & ~255u) + 256u));
+                                l1jP = (j0 - U.c0) + 31u - ((uint32_t(rmax) - c) & 255u);
+                                tkP = max(tkP, int32_t((uint32_t(rmax) - ((uint32_t(rmax) - c) & 255u)) + 256u));
                             } else {
                                 l2kP = max(l2kP, rmax);
                             }
@@ -372,32 +411,27 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             l2kP = max(l2kP, rmax);
                         }
                     }
-                    tk[p] = tkP;
-                    l1k[p] = l1kP;
-                    l2k[p] = l2kP;
-                    l1j[p] = l1jP;
+                    S.l1k[wg][r] = l1kP;
+                    S.l2k[wg][r] = l2kP;
+                    S.l1j[wg][r] = uint16_t(l1jP);
                 }
-                // ---- column flush: best key per column over the 128 lanes of this warpgroup. The
-                // flush key orders equal values by row tile, then lane (= by row index):
-                // (value << 8) | (7 - p) << 5 | (31 - lane).
+                // ---- column flush: best key per column over this warp's 32 lanes, then over the
+                // four lane quarters in shared memory, then one global atomic per column.
 #pragma unroll
-                for (int c = 0; c < kCPW; ++c) {
-                    int32_t mine = INT32_MIN;
+                for (int cc = 0; cc < kCPW; ++cc) {
+                    int32_t v[32];
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) {
-                        const uint32_t v = uint32_t(ca[32 * c + k]);
-                        const int32_t fk = int32_t((v & ~255u) | ((v & 7u) << 5) | (31u - lane));
-                        const int32_t mx = redux_max_s32(fk);
-                        mine = (lane == uint32_t(k)) ? mx : mine;
-                    }
+                    for (int k = 0; k < 32; ++k) v[k] = ca[32 * cc + k];
+                    column_max_butterfly(v, lane);
+                    const int32_t mine = v[0];
                     // (2 a.b - |a|^2) = |b|^2 - d; row = 128 p + 32 q + lane
-                    const int32_t v = mine >> 8;
+                    const int32_t val = mine >> 8;
                     const uint32_t pp = 7u - ((uint32_t(mine) >> 5) & 7u);
                     const uint32_t ln = 31u - (uint32_t(mine) & 31u);
                     const uint32_t rr = 128u * pp + 32u * q + ln;
                     const unsigned long long key =
-                        (static_cast<unsigned long long>(uint32_t(int32_t(kVBias) - v)) << 32) | rr;
-                    atomicMin(&S.colmin[bpar][jw - blockBase + 32 * c + lane], key);
+                        (static_cast<unsigned long long>(uint32_t(int32_t(kVBias) - val)) << 32) | rr;
+                    atomicMin(&S.colmin[bpar][jw - blockBase + 32 * cc + lane], key);
                 }
                 named_bar(2 + wg, 128);
                 if (t128 < 32 * kCPW) {
@@ -407,42 +441,46 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                     const uint32_t j = blockBase + cc;
                     const uint32_t i = U.r0 + uint32_t(key & 0xFFFFFFFFu);
                     if (j < T.nB && i < T.nA) {
-                        const uint32_t d = uint32_t(key >> 32) - kVBias + T.sqrB[j];
+                        const uint32_t xj = j - U.c0;  // |b_j|^2 from the staged row-key addend
+                        const uint32_t nbj = ((31u - (xj & 31u)) - uint32_t(S.nbk[xj])) >> 8;
+                        const uint32_t d = uint32_t(key >> 32) - kVBias + nbj;
                         atomicMin(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
                     }
                 }
             }
-            // ---- merge the warpgroups' row top-2 in shared memory, then publish each row
-            // once (exact two-slot merge: old = min(best, b); second = min(second, max(old, b), s)).
+            // ---- unit end: merge the warpgroups' row states (exact two-slot merge) and publish
+            // each row once: old = atomicMin(best, b); second = min(second, max(old, b), s).
+            named_bar(1, 32 * kEpiWarps);
+#pragma unroll 1
+            for (uint32_t r = tE; r < 128u * U.pt; r += 32u * kEpiWarps) {
+                const uint32_t i = U.r0 + r;
+                if (i >= T.nA) continue;
+                const uint32_t c = uint32_t(S.rowc[r]) & 255u;
+                unsigned long long bst = ~0ull;
+                uint32_t sec = ~0u;
 #pragma unroll
-            for (int p = 0; p < kMaxRowTiles; ++p) {
-                const uint32_t r = 128u * p + 32u * q + lane;
-                if (uint32_t(p) < U.pt) {
-                    if (l1k[p] != INT32_MIN) {
-                        const uint32_t d1 = ((uint32_t(l1k[p]) & 255u) - uint32_t(l1k[p])) >> 8;
-                        const unsigned long long old =
-                            atomicMin(&S.rowbest[unitPar][r], (static_cast<unsigned long long>(d1) << 32) | l1j[p]);
-                        atomicMin(&S.rowsecond[unitPar][r], max(uint32_t(old >> 32), d1));
+                for (int w = 0; w < kWG; ++w) {
+                    const int32_t k1 = S.l1k[w][r], k2 = S.l2k[w][r];
+                    if (k1 != INT32_MIN) {
+                        const uint32_t d1 = 0u - uint32_t(int32_t(uint32_t(k1) - c) >> 8);
+                        const unsigned long long key =
+                            (static_cast<unsigned long long>(d1) << 32) | (U.c0 + uint32_t(S.l1j[w][r]));
+                        if (key < bst) {
+                            sec = min(sec, uint32_t(bst >> 32));
+                            bst = key;
+                        } else {
+                            sec = min(sec, d1);
+                        }
                     }
-                    if (l2k[p] != INT32_MIN)
-                        atomicMin(&S.rowsecond[unitPar][r], ((uint32_t(l2k[p]) & 255u) - uint32_t(l2k[p])) >> 8);
+                    if (k2 != INT32_MIN) sec = min(sec, 0u - uint32_t(int32_t(uint32_t(k2) - c) >> 8));
                 }
+                if (bst != ~0ull) {
+                    const unsigned long long old = atomicMin(&T.bestA[i], bst);
+                    atomicMin(&T.secondA[i], max(uint32_t(old >> 32), uint32_t(bst >> 32)));
+                }
+                if (sec != ~0u) atomicMin(&T.secondA[i], sec);
             }
             named_bar(1, 32 * kEpiWarps);
-            for (uint32_t r = t512; r < 128u * U.pt; r += 32u * kEpiWarps) {
-                const unsigned long long bst = S.rowbest[unitPar][r];
-                const uint32_t sec = S.rowsecond[unitPar][r];
-                S.rowbest[unitPar][r] = ~0ull;
-                S.rowsecond[unitPar][r] = ~0u;
-                const uint32_t i = U.r0 + r;
-                if (i < T.nA) {
-                    if (bst != ~0ull) {
-                        const unsigned long long old = atomicMin(&T.bestA[i], bst);
-                        atomicMin(&T.secondA[i], max(uint32_t(old >> 32), uint32_t(bst >> 32)));
-                    }
-                    if (sec != ~0u) atomicMin(&T.secondA[i], sec);
-                }
-            }
         }
     }
 
@@ -514,7 +552,8 @@ __global__ void sqr_norm_kernel(uint32_t* __restrict__ out, const uint4* __restr
     if (i < n && part == 0) out[i] = acc;
 }
 
-static size_t smem_bytes() { return sizeof(Smem) + 1024; }
+template <int kWG>
+static size_t smem_bytes() { return sizeof(Smem<kWG>) + 1024; }
 
 // Unit shape: as many A rows per unit as possible (fewer column flushes), then columns, keeping
 // at least ~2 units per SM when the problem allows.
@@ -557,7 +596,7 @@ static int ensure_attr() {
     static bool attrSet = false;
     if (!attrSet) {
         RSFM_CUDA_TRY(cudaFuncSetAttribute(bf_match_kernel<kWG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(smem_bytes())));
+                                           int(smem_bytes<kWG>())));
         attrSet = true;
     }
     return RSFM_OK;
@@ -567,7 +606,7 @@ template <int kWG>
 static int launch_main(const Params& P, uint32_t grid, cudaStream_t stream) {
     const int st = ensure_attr<kWG>();
     if (st != RSFM_OK) return st;
-    bf_match_kernel<kWG><<<grid, Cfg<kWG>::kThreads, smem_bytes(), stream>>>(P);
+    bf_match_kernel<kWG><<<grid, Cfg<kWG>::kThreads, smem_bytes<kWG>(), stream>>>(P);
     RSFM_CUDA_TRY(cudaGetLastError());
     return RSFM_OK;
 }
@@ -822,7 +861,7 @@ extern "C" int rsfm_bf_plan_create(const rsfm_sift_bf_task* tasks, size_t nbTask
     uint32_t rt = 0, cb = 0;
     bf::choose_shape(sizes, nsm, rt, cb);
     if (opts && opts->rowTiles) rt = std::min<uint32_t>(opts->rowTiles, bf::kMaxRowTiles);
-    if (opts && opts->colBlocks) cb = opts->colBlocks;
+    if (opts && opts->colBlocks) cb = std::min<uint32_t>(opts->colBlocks, bf::kMaxColBlocks);
     pl->groups = (opts && opts->epilogueGroups == 4) ? 4u : (opts && opts->epilogueGroups == 2) ? 2u
                                                                                                 : uint32_t(bf::epilogue_groups());
     std::vector<bf::TaskDev> host(nbTasks);

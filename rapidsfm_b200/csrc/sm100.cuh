@@ -63,7 +63,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     if (mbar_try_wait(bar, parity)) return true;
     for (uint32_t i = 0; i < kSpinLimit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
+        if (i > 512) __nanosleep(32);
         if ((i & 1023u) == 0 && *reinterpret_cast<volatile uint32_t*>(err) != 0u) return false;
     }
     atomicCAS(err, 0u, code);
