@@ -95,12 +95,24 @@ typedef struct rsfm_bf_plan_options {
     uint32_t colBlocks;       /* 128-column blocks per work unit */
     uint32_t epilogueGroups;  /* epilogue warpgroups per CTA: 2 or 4 */
     uint32_t useGraph;        /* capture the launches in a CUDA graph */
+    uint32_t schedule;        /* unit order: 0 = pairs in the given order, 1 = largest pairs first */
 } rsfm_bf_plan_options;
 int rsfm_bf_plan_create(const rsfm_sift_bf_task* tasks, size_t nbTasks, uint32_t* const* secondDistA,
                         uint32_t* const* flagsA, uint32_t ratioNum, uint32_t ratioDen,
                         const rsfm_bf_plan_options* options, rsfm_bf_plan** plan);
 int rsfm_bf_plan_launch(rsfm_bf_plan* plan, cudaStream_t stream);
 int rsfm_bf_plan_destroy(rsfm_bf_plan* plan);
+
+/* Autotuner for batched plans (no reference counterpart). Times candidate options (unit shape
+ * rowTiles x colBlocks, epilogue warpgroups, schedule) on this batch: each candidate is a graph
+ * plan launched once to warm up and `reps` times under CUDA events on `stream` (so the batch's
+ * outputs are written as a side effect); returns the fastest in *best and its time per launch in
+ * *bestMs. With cachePath non-NULL, choices are kept in that text file keyed by a signature of
+ * the batch (device SM count, pair count and log2 histograms of both sides' sizes): a batch whose
+ * signature is found is not timed again (*bestMs is then the cached time). Synchronizes. */
+int rsfm_bf_plan_autotune(const rsfm_sift_bf_task* tasks, size_t nbTasks, uint32_t* const* secondDistA,
+                          uint32_t* const* flagsA, uint32_t ratioNum, uint32_t ratioDen, const char* cachePath,
+                          uint32_t reps, cudaStream_t stream, rsfm_bf_plan_options* best, float* bestMs);
 
 /* Replaces crossCheckMatches (bruteForceMatch.h:126-127, bruteForceMatch.cpp:23-40). Host
  * memory in and out; `out` must hold min(nbQueryDesc, nbTrainDesc) entries. Returns the count. */

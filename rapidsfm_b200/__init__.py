@@ -8,6 +8,7 @@ from .matcher import (  # noqa: F401
     BFPlan,
     BFTask,
     BruteForceMatcher,
+    autotune_plan,
     bf_match,
     bf_match_ext,
     cross_check_matches,

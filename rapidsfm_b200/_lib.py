@@ -64,7 +64,7 @@ class RankedImage(ctypes.Structure):
 
 class BFPlanOptions(ctypes.Structure):
     _fields_ = [("rowTiles", ctypes.c_uint32), ("colBlocks", ctypes.c_uint32), ("epilogueGroups", ctypes.c_uint32),
-                ("useGraph", ctypes.c_uint32)]
+                ("useGraph", ctypes.c_uint32), ("schedule", ctypes.c_uint32)]
 
 
 class MLP(ctypes.Structure):
@@ -120,6 +120,11 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                                            ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(BFPlanOptions),
                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "rsfm_bf_plan_autotune": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t,
+                                             ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32,
+                                             ctypes.c_void_p, ctypes.POINTER(BFPlanOptions),
+                                             ctypes.POINTER(ctypes.c_float)]),
     "rsfm_bf_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_mlp_hash": (ctypes.c_int, [ctypes.POINTER(MLP), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,

@@ -864,10 +864,19 @@ extern "C" int rsfm_bf_plan_create(const rsfm_sift_bf_task* tasks, size_t nbTask
     if (opts && opts->colBlocks) cb = std::min<uint32_t>(opts->colBlocks, bf::kMaxColBlocks);
     pl->groups = (opts && opts->epilogueGroups == 4) ? 4u : (opts && opts->epilogueGroups == 2) ? 2u
                                                                                                 : uint32_t(bf::epilogue_groups());
+    // Unit order: pairs in the given order, or largest pairs first (their units are spread over
+    // every CTA before the small pairs fill the tail).
+    std::vector<size_t> order(nbTasks);
+    for (size_t t = 0; t < nbTasks; ++t) order[t] = t;
+    if (opts && opts->schedule == 1)
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+            return uint64_t(tasks[x].nbDescA) * tasks[x].nbDescB > uint64_t(tasks[y].nbDescA) * tasks[y].nbDescB;
+        });
     std::vector<bf::TaskDev> host(nbTasks);
     uint32_t units = 0;
-    for (size_t t = 0; t < nbTasks; ++t) {
-        bf::TaskDev& T = host[t];
+    for (size_t o = 0; o < nbTasks; ++o) {
+        const size_t t = order[o];
+        bf::TaskDev& T = host[o];
         memset(&T, 0, sizeof(T));
         const rsfm_sift_bf_task& in = tasks[t];
         T.nA = in.nbDescA;

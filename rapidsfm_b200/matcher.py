@@ -98,7 +98,7 @@ class BFPlan:
     """A batch of pairs matched by one persistent, CUDA-graph-captured launch (rsfm_bf_plan_*)."""
 
     def __init__(self, tasks, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08, row_tiles=0, col_blocks=0,
-                 epilogue_groups=0, use_graph=True):
+                 epilogue_groups=0, use_graph=True, schedule=0, options=None):
         lib = _lib.load()
         self.tasks = tasks
         for t in tasks:
@@ -109,7 +109,8 @@ class BFPlan:
         arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
         sec = (ctypes.c_void_p * len(tasks))(*[t.secondA.data_ptr() for t in tasks])
         flg = (ctypes.c_void_p * len(tasks))(*[t.flagsA.data_ptr() for t in tasks])
-        opts = _lib.BFPlanOptions(row_tiles, col_blocks, epilogue_groups, 1 if use_graph else 0)
+        opts = options if options is not None else _lib.BFPlanOptions(row_tiles, col_blocks, epilogue_groups,
+                                                                      1 if use_graph else 0, schedule)
         self._h = ctypes.c_void_p(0)
         _lib.check(lib.rsfm_bf_plan_create(arr, len(tasks), sec, flg, ratio_num, ratio_den, ctypes.byref(opts),
                                            ctypes.byref(self._h)), "rsfm_bf_plan_create")
@@ -127,6 +128,32 @@ class BFPlan:
             self.close()
         except Exception:
             pass
+
+
+def _ext_outputs(tasks):
+    for t in tasks:
+        n = t.descA.shape[0]
+        if t.secondA is None or t.secondA.numel() != n:
+            t.secondA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+            t.flagsA = torch.empty(n, dtype=torch.int32, device=t.descA.device)
+    arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+    sec = (ctypes.c_void_p * len(tasks))(*[t.secondA.data_ptr() for t in tasks])
+    flg = (ctypes.c_void_p * len(tasks))(*[t.flagsA.data_ptr() for t in tasks])
+    return arr, sec, flg
+
+
+def autotune_plan(tasks, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08, cache_path=None, reps=3, stream=None):
+    """Times candidate plan options on this batch (rsfm_bf_plan_autotune); returns (options, ms per
+    launch). The batch's outputs are written as a side effect."""
+    lib = _lib.load()
+    arr, sec, flg = _ext_outputs(tasks)
+    best = _lib.BFPlanOptions()
+    ms = ctypes.c_float(0)
+    path = cache_path.encode() if cache_path else None
+    _lib.check(lib.rsfm_bf_plan_autotune(arr, len(tasks), sec, flg, ratio_num, ratio_den, path, reps,
+                                         _stream_ptr(stream), ctypes.byref(best), ctypes.byref(ms)),
+               "rsfm_bf_plan_autotune")
+    return best, float(ms.value)
 
 
 def unpack_best(best):

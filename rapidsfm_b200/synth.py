@@ -39,3 +39,27 @@ def uniform_bytes(n, seed):
     """Uniform random bytes (the reference's kernel tests use uniform random 32-bit words)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return rng.integers(0, 256, size=(n, 128), dtype=np.uint8)
+
+
+def _sift_like_torch(n, gen, device):
+    import torch
+    x = torch.randn((n, 128), generator=gen, device=device, dtype=torch.float32).abs_()
+    x /= x.norm(dim=1, keepdim=True).clamp_min_(1e-12)
+    x.clamp_max_(0.2)
+    x /= x.norm(dim=1, keepdim=True).clamp_min_(1e-12)
+    return (x * 512.0).round_().clamp_(0, 255).to(torch.uint8)
+
+
+def make_pair_torch(n_query, n_train, overlap, sigma, gen, device="cuda"):
+    """make_pair's distribution drawn on the device from a torch.Generator (large batched
+    workloads, where host generation would dominate). Returns CUDA tensors (query, train, truth)."""
+    import torch
+    q = _sift_like_torch(n_query, gen, device)
+    n_copy = int(round(overlap * min(n_query, n_train)))
+    src = torch.randperm(n_query, generator=gen, device=device)[:n_copy]
+    noise = torch.randn((n_copy, 128), generator=gen, device=device) * sigma
+    copies = (q[src].float() + noise).round_().clamp_(0, 255).to(torch.uint8)
+    t = torch.cat([copies, _sift_like_torch(n_train - n_copy, gen, device)])
+    truth = torch.cat([src, torch.full((n_train - n_copy,), -1, dtype=torch.int64, device=device)])
+    perm = torch.randperm(n_train, generator=gen, device=device)
+    return q, t[perm].contiguous(), truth[perm]

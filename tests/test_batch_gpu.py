@@ -60,3 +60,59 @@ def test_plan_shapes(rsfm, oracle):
             np.testing.assert_array_equal(bwd, ebwd)
             np.testing.assert_array_equal(sec, esec)
         plan.close()
+
+
+def test_plan_largest_first_schedule(rsfm, oracle):
+    pairs = _pairs(23, 50, 3000, 13)
+    tasks = [rsfm.BFTask(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in pairs]
+    plan = rsfm.BFPlan(tasks, schedule=1)
+    plan.launch()
+    torch.cuda.synchronize()
+    for (a, b), t in zip(pairs, tasks):
+        fwd, bwd, sec, flg = _res(rsfm, t)
+        efwd, ebwd, esec = oracle.bf_match(a, b)
+        np.testing.assert_array_equal(fwd, efwd)
+        np.testing.assert_array_equal(bwd, ebwd)
+        np.testing.assert_array_equal(sec, esec)
+    plan.close()
+
+
+def test_autotune_and_cache(rsfm, oracle, tmp_path):
+    pairs = _pairs(12, 200, 4000, 17)
+    tasks = [rsfm.BFTask(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in pairs]
+    cache = str(tmp_path / "bf_tune.txt")
+    opts, ms = rsfm.autotune_plan(tasks, cache_path=cache, reps=2)
+    assert opts.rowTiles in (2, 4, 8) and opts.colBlocks in (1, 2, 4, 8) and opts.epilogueGroups in (2, 4)
+    assert ms > 0
+    assert len(open(cache).read().splitlines()) == 1
+    # the same kind of batch is answered from the cache, without timing
+    opts2, ms2 = rsfm.autotune_plan(tasks, cache_path=cache)
+    assert (opts2.rowTiles, opts2.colBlocks, opts2.epilogueGroups, opts2.schedule) == \
+        (opts.rowTiles, opts.colBlocks, opts.epilogueGroups, opts.schedule)
+    assert abs(ms2 - ms) <= 1e-3 * ms + 1e-4
+    assert len(open(cache).read().splitlines()) == 1
+    # a plan built with the tuned options gives the exact results
+    plan = rsfm.BFPlan(tasks, options=opts)
+    plan.launch()
+    torch.cuda.synchronize()
+    for (a, b), t in zip(pairs, tasks):
+        fwd, bwd, sec, flg = _res(rsfm, t)
+        efwd, ebwd, esec = oracle.bf_match(a, b)
+        np.testing.assert_array_equal(fwd, efwd)
+        np.testing.assert_array_equal(bwd, ebwd)
+        np.testing.assert_array_equal(sec, esec)
+        np.testing.assert_array_equal(flg, oracle.match_flags(efwd, esec, ebwd))
+    plan.close()
+
+
+def test_device_generator_distribution(rsfm):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    q, t, truth = synth.make_pair_torch(3000, 2500, 0.5, 8.0, g)
+    assert q.dtype == torch.uint8 and q.shape == (3000, 128) and t.shape == (2500, 128)
+    assert int((truth >= 0).sum()) == 1250
+    # norms match the host generator's (both: |N(0,1)| rows, clipped at 0.2, scaled to 512)
+    hq, _, _ = synth.make_pair(3000, 2500, 0.5, 8.0, seed=3)
+    dn = q.float().norm(dim=1).mean().item()
+    hn = float(np.linalg.norm(hq.astype(np.float32), axis=1).mean())
+    assert abs(dn - hn) < 0.01 * hn
