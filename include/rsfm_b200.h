@@ -229,6 +229,24 @@ int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const rsfm_ranked_
                               uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, rsfm_best_match* best,
                               uint32_t* secondDist, uint32_t* flags, uint32_t* nbCandidates, cudaStream_t stream);
 
+/* Batched ranked matching (no reference counterpart): many (query image, train image) pairs in
+ * one launch, every query descriptor of every pair by one warp, same results as
+ * rsfm_cashash_match_ranked per pair. Creation copies the image descriptions and output pointers
+ * to device memory (the buffers they point to must stay valid while the batch is used). */
+typedef struct rsfm_ranked_pair {
+    const rsfm_ranked_image* query;  /* host pointers, read at creation */
+    const rsfm_ranked_image* train;
+    rsfm_best_match* best;           /* device outputs, query->nbDesc entries each */
+    uint32_t* secondDist;
+    uint32_t* flags;
+    uint32_t* nbCandidates;          /* optional */
+} rsfm_ranked_pair;
+typedef struct rsfm_ranked_batch rsfm_ranked_batch;
+int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t nbPairs, uint32_t nbTables, uint32_t topK,
+                             uint32_t ratioNum, uint32_t ratioDen, rsfm_ranked_batch** batch);
+int rsfm_ranked_batch_launch(rsfm_ranked_batch* batch, cudaStream_t stream);
+int rsfm_ranked_batch_destroy(rsfm_ranked_batch* batch);
+
 /* Learned hash (no reference counterpart; replaces cascade hashing's random projection with a
  * trained 128 -> 256 -> 128 MLP). Weights on the device: w1 bf16 [256][128], b1 f32 [256],
  * w2 bf16 [128][256], b2 f32 [128]. x = desc / 64; h = bf16(relu(w1 x + b1)); o = w2 h + b2;

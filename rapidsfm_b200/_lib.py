@@ -62,6 +62,12 @@ class RankedImage(ctypes.Structure):
                 ("nbDesc", ctypes.c_uint32)]
 
 
+class RankedPair(ctypes.Structure):
+    _fields_ = [("query", ctypes.POINTER(RankedImage)), ("train", ctypes.POINTER(RankedImage)),
+                ("best", ctypes.c_void_p), ("secondDist", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+                ("nbCandidates", ctypes.c_void_p)]
+
+
 class BFPlanOptions(ctypes.Structure):
     _fields_ = [("rowTiles", ctypes.c_uint32), ("colBlocks", ctypes.c_uint32), ("epilogueGroups", ctypes.c_uint32),
                 ("useGraph", ctypes.c_uint32), ("schedule", ctypes.c_uint32)]
@@ -125,6 +131,11 @@ SIGNATURES = {
                                              ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32,
                                              ctypes.c_void_p, ctypes.POINTER(BFPlanOptions),
                                              ctypes.POINTER(ctypes.c_float)]),
+    "rsfm_ranked_batch_create": (ctypes.c_int, [ctypes.POINTER(RankedPair), ctypes.c_uint32, ctypes.c_uint32,
+                                                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "rsfm_ranked_batch_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_ranked_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_bf_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_mlp_hash": (ctypes.c_int, [ctypes.POINTER(MLP), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,

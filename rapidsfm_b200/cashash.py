@@ -122,3 +122,98 @@ class CasHash:
     def ranked_image(self, desc, stream=None):
         keys, codes = self.hash(desc, stream=stream)
         return RankedImage(desc, keys, codes, stream=stream)
+
+
+class RankedBatch:
+    """Many (query, train) RankedImage pairs matched by one launch (rsfm_ranked_batch_*); results
+    per pair as in match_ranked. The batch keeps references to the images and its outputs."""
+
+    def __init__(self, pairs, tables=6, top_k=10, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08,
+                 count_candidates=False):
+        lib = _lib.load()
+        self.pairs = list(pairs)
+        self.results = []
+        self._imgs = []
+        arr = (_lib.RankedPair * len(self.pairs))()
+        for k, (q, t) in enumerate(self.pairs):
+            dev = q.desc.device
+            best = torch.empty(q.n, dtype=torch.int64, device=dev)
+            sec = torch.empty(q.n, dtype=torch.int32, device=dev)
+            flg = torch.empty(q.n, dtype=torch.int32, device=dev)
+            cnt = torch.empty(q.n, dtype=torch.int32, device=dev) if count_candidates else None
+            self.results.append((best, sec, flg, cnt))
+            qi, ti = q.as_ctype(), t.as_ctype()
+            self._imgs += [qi, ti]
+            arr[k] = _lib.RankedPair(ctypes.pointer(qi), ctypes.pointer(ti), best.data_ptr(), sec.data_ptr(),
+                                     flg.data_ptr(), cnt.data_ptr() if cnt is not None else None)
+        self._h = ctypes.c_void_p(0)
+        _lib.check(lib.rsfm_ranked_batch_create(arr, len(self.pairs), tables, top_k, ratio_num, ratio_den,
+                                                ctypes.byref(self._h)), "rsfm_ranked_batch_create")
+
+    def launch(self, stream=None):
+        _lib.check(_lib.load().rsfm_ranked_batch_launch(self._h, _stream_ptr(stream)), "rsfm_ranked_batch_launch")
+        return self.results
+
+    def close(self):
+        if self._h:
+            _lib.load().rsfm_ranked_batch_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CascadeMatcher:
+    """Cascade-hash matching over registered images, in the manner of the reference matcher's
+    cascade-hash method (bruteForceMatcher.cpp:63-107 registers; findBestMatch matches), with the
+    ranked pipeline: `hasher` (CasHash, or a learned_hash.LearnedHash) gives each image its 8 key
+    bytes and 128-bit code at registration; match() runs all pairs in one ranked launch. A pair
+    whose train image has a bucket larger than `bucket_limit` in one of the tables used falls back
+    to the exact brute-force matcher."""
+
+    def __init__(self, hasher, tables=6, top_k=10, bucket_limit=512, ratio_num=RATIO_NUM_08,
+                 ratio_den=RATIO_DEN_08):
+        self.hasher = hasher
+        self.tables, self.top_k, self.bucket_limit = tables, top_k, bucket_limit
+        self.ratio = (ratio_num, ratio_den)
+        self.images = {}
+        self.fallback_pairs = []
+
+    def register_image(self, handle, desc, stream=None):
+        if isinstance(self.hasher, CasHash):
+            self.hasher.fit(desc, stream=stream)
+            keys, codes = self.hasher.hash(desc, stream=stream)
+        else:
+            keys, codes, _ = self.hasher.hash(desc, stream=stream)
+        self.images[handle] = RankedImage(desc, keys, codes, stream=stream)
+
+    def _bucket_overflow(self, img):
+        # largest bucket over the tables in use (bucket sizes from the inclusive upper bounds)
+        up = img.upper[: self.tables].to(torch.int64)
+        sizes = torch.diff(up, dim=1, prepend=torch.zeros_like(up[:, :1]))
+        return int(sizes.max().item()) > self.bucket_limit
+
+    def match(self, pairs, count_candidates=False):
+        """pairs: [(query handle, train handle)] -> list of (best int64, second int32, flags int32)."""
+        from .matcher import BFTask, bf_match_ext
+        over = {h: self._bucket_overflow(self.images[h]) for _, h in pairs}
+        ranked = [k for k, (_, th) in enumerate(pairs) if not over[th]]
+        brute = [k for k, (_, th) in enumerate(pairs) if over[th]]
+        out = [None] * len(pairs)
+        if ranked:
+            batch = RankedBatch([(self.images[pairs[k][0]], self.images[pairs[k][1]]) for k in ranked], self.tables,
+                                self.top_k, *self.ratio, count_candidates=count_candidates)
+            for k, res in zip(ranked, batch.launch()):
+                out[k] = res[:3]
+            self._last_batch = batch
+        if brute:
+            tasks = [BFTask(self.images[pairs[k][0]].desc, self.images[pairs[k][1]].desc,
+                            self.images[pairs[k][0]].sqr, self.images[pairs[k][1]].sqr) for k in brute]
+            bf_match_ext(tasks, *self.ratio)
+            for k, t in zip(brute, tasks):
+                out[k] = (t.bestA, t.secondA, t.flagsA & 1)
+        self.fallback_pairs = brute
+        return out

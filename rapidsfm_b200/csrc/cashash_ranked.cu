@@ -11,6 +11,7 @@
 // with the running top-K when a query has more candidates than the buffer holds.
 #include "common.h"
 #include <algorithm>
+#include <vector>
 
 namespace rsfm_b200 {
 namespace chr {
@@ -38,106 +39,136 @@ __device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
     return m;
 }
 
+struct Out {
+    unsigned long long* best;
+    uint32_t* second;
+    uint32_t* flags;
+    uint32_t* nbCand;
+};
+
+// One query descriptor i of image Q against image T, by one warp; B / TOP are the warp's buffers.
+__device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t i, uint32_t tables, uint32_t topK,
+                                            uint32_t ratioNum, uint32_t ratioDen, const Out& O, uint32_t* B,
+                                            uint32_t* TOP, uint32_t lane) {
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint2 qk = Q.keys[i];
+    const uint4 qc = Q.codes[i];
+    uint32_t cnt = 0, nTop = 0, total = 0;
+
+    // Extract the topK smallest keys of buffer + running top into TOP (lane r keeps round r's).
+    auto select = [&]() {
+        uint32_t prev = 0, have = 0, mine = 0xFFFFFFFFu;
+        const uint32_t want = min(topK, cnt + nTop);
+        for (uint32_t r = 0; r < want; ++r) {
+            uint32_t mn = 0xFFFFFFFFu;
+            for (uint32_t x = lane; x < cnt; x += 32) {
+                const uint32_t v = B[x];
+                if ((have == 0 || v > prev) && v < mn) mn = v;
+            }
+            if (lane < nTop) {
+                const uint32_t v = TOP[lane];
+                if ((have == 0 || v > prev) && v < mn) mn = v;
+            }
+            mn = __reduce_min_sync(0xffffffffu, mn);
+            prev = mn;
+            have = 1;
+            if (lane == r) mine = mn;
+        }
+        __syncwarp();
+        if (lane < want) TOP[lane] = mine;
+        __syncwarp();
+        nTop = want;
+        cnt = 0;
+    };
+
+    for (uint32_t s = 0; s < tables; ++s) {
+        const uint32_t bk = s < 4 ? (qk.x >> (8 * s)) & 0xFFu : (qk.y >> (8 * (s - 4))) & 0xFFu;
+        const uint32_t lo = bk ? T.ends[s * 256 + bk - 1] : 0u, hi = T.ends[s * 256 + bk];
+        const uint32_t* list = T.buckets + size_t(s) * T.n;
+        for (uint32_t x0 = lo; x0 < hi; x0 += 32) {
+            const uint32_t x = x0 + lane;
+            bool keep = false;
+            uint32_t key = 0;
+            if (x < hi) {
+                const uint32_t j = list[x];
+                const uint2 tk = T.keys[j];
+                const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
+                keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
+                if (keep) {
+                    const uint4 tc = T.codes[j];
+                    const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
+                                       __popc(tc.w ^ qc.w);
+                    key = (h << 24) | j;
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (cnt + __popc(m) > kBuf) select();
+            if (keep) B[cnt + __popc(m & lt)] = key;
+            cnt += __popc(m);
+            total += __popc(m);
+            __syncwarp();
+        }
+    }
+    select();
+    // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
+    const uint32_t qw = reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128)[lane];
+    const uint32_t nq = Q.sqr[i];
+    uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+    for (uint32_t r = 0; r < nTop; ++r) {
+        const uint32_t j = TOP[r] & 0xFFFFFFu;
+        const uint32_t tw = reinterpret_cast<const uint32_t*>(T.desc + size_t(j) * 128)[lane];
+        uint32_t dot = __dp4a(qw, tw, 0u);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+        const uint32_t d = nq + T.sqr[j] - 2u * dot;
+        if (d < bd || (d == bd && j < bj)) {
+            sd = bd;
+            bd = d;
+            bj = j;
+        } else if (d < sd) {
+            sd = d;
+        }
+    }
+    if (lane == 0) {
+        O.best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
+        O.second[i] = sd;
+        uint32_t f = 0;
+        if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+        O.flags[i] = f;
+        if (O.nbCand) O.nbCand[i] = total;
+    }
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(32 * kWarps) ranked_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
-                                                             uint32_t ratioNum, uint32_t ratioDen,
-                                                             unsigned long long* __restrict__ best,
-                                                             uint32_t* __restrict__ second, uint32_t* __restrict__ flags,
-                                                             uint32_t* __restrict__ nbCand) {
+                                                             uint32_t ratioNum, uint32_t ratioDen, Out O) {
     __shared__ uint32_t buf[kWarps][kBuf];
     __shared__ uint32_t top[kWarps][kMaxTopK];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    uint32_t* B = buf[warp];
-    uint32_t* TOP = top[warp];
-    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t i = blockIdx.x * kWarps + warp; i < Q.n; i += gridDim.x * kWarps)
+        match_query(Q, T, i, tables, topK, ratioNum, ratioDen, O, buf[warp], top[warp], lane);
+}
 
-    for (uint32_t i = blockIdx.x * kWarps + warp; i < Q.n; i += gridDim.x * kWarps) {
-        const uint2 qk = Q.keys[i];
-        const uint4 qc = Q.codes[i];
-        uint32_t cnt = 0, nTop = 0, total = 0;
-
-        // Extract the topK smallest keys of buffer + running top into TOP (lane r keeps round r's).
-        auto select = [&]() {
-            uint32_t prev = 0, have = 0, mine = 0xFFFFFFFFu;
-            const uint32_t want = min(topK, cnt + nTop);
-            for (uint32_t r = 0; r < want; ++r) {
-                uint32_t mn = 0xFFFFFFFFu;
-                for (uint32_t x = lane; x < cnt; x += 32) {
-                    const uint32_t v = B[x];
-                    if ((have == 0 || v > prev) && v < mn) mn = v;
-                }
-                if (lane < nTop) {
-                    const uint32_t v = TOP[lane];
-                    if ((have == 0 || v > prev) && v < mn) mn = v;
-                }
-                mn = __reduce_min_sync(0xffffffffu, mn);
-                prev = mn;
-                have = 1;
-                if (lane == r) mine = mn;
-            }
-            __syncwarp();
-            if (lane < want) TOP[lane] = mine;
-            __syncwarp();
-            nTop = want;
-            cnt = 0;
-        };
-
-        for (uint32_t s = 0; s < tables; ++s) {
-            const uint32_t bk = s < 4 ? (qk.x >> (8 * s)) & 0xFFu : (qk.y >> (8 * (s - 4))) & 0xFFu;
-            const uint32_t lo = bk ? T.ends[s * 256 + bk - 1] : 0u, hi = T.ends[s * 256 + bk];
-            const uint32_t* list = T.buckets + size_t(s) * T.n;
-            for (uint32_t x0 = lo; x0 < hi; x0 += 32) {
-                const uint32_t x = x0 + lane;
-                bool keep = false;
-                uint32_t key = 0;
-                if (x < hi) {
-                    const uint32_t j = list[x];
-                    const uint2 tk = T.keys[j];
-                    const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
-                    keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
-                    if (keep) {
-                        const uint4 tc = T.codes[j];
-                        const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
-                                           __popc(tc.w ^ qc.w);
-                        key = (h << 24) | j;
-                    }
-                }
-                const uint32_t m = __ballot_sync(0xffffffffu, keep);
-                if (cnt + __popc(m) > kBuf) select();
-                if (keep) B[cnt + __popc(m & lt)] = key;
-                cnt += __popc(m);
-                total += __popc(m);
-                __syncwarp();
-            }
+// Many pairs in one launch: global query g belongs to the last pair p with begin[p] <= g.
+struct PairDev {
+    Img q, t;
+    Out o;
+};
+__global__ void __launch_bounds__(32 * kWarps) ranked_batch_kernel(const PairDev* __restrict__ pairs,
+                                                                   const uint32_t* __restrict__ begin, uint32_t nPairs,
+                                                                   uint32_t total, uint32_t tables, uint32_t topK,
+                                                                   uint32_t ratioNum, uint32_t ratioDen) {
+    __shared__ uint32_t buf[kWarps][kBuf];
+    __shared__ uint32_t top[kWarps][kMaxTopK];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (uint32_t g = blockIdx.x * kWarps + warp; g < total; g += gridDim.x * kWarps) {
+        uint32_t lo = 0, hi = nPairs - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (begin[mid] <= g) lo = mid; else hi = mid - 1;
         }
-        select();
-        // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
-        const uint32_t qw = reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128)[lane];
-        const uint32_t nq = Q.sqr[i];
-        uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
-        for (uint32_t r = 0; r < nTop; ++r) {
-            const uint32_t j = TOP[r] & 0xFFFFFFu;
-            const uint32_t tw = reinterpret_cast<const uint32_t*>(T.desc + size_t(j) * 128)[lane];
-            uint32_t dot = __dp4a(qw, tw, 0u);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-            const uint32_t d = nq + T.sqr[j] - 2u * dot;
-            if (d < bd || (d == bd && j < bj)) {
-                sd = bd;
-                bd = d;
-                bj = j;
-            } else if (d < sd) {
-                sd = d;
-            }
-        }
-        if (lane == 0) {
-            best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
-            second[i] = sd;
-            uint32_t f = 0;
-            if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
-            flags[i] = f;
-            if (nbCand) nbCand[i] = total;
-        }
-        __syncwarp();
+        const PairDev& P = pairs[lo];
+        match_query(P.q, P.t, g - begin[lo], tables, topK, ratioNum, ratioDen, P.o, buf[warp], top[warp], lane);
     }
 }
 
@@ -174,9 +205,95 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
-    chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen,
-                                                             reinterpret_cast<unsigned long long*>(best), secondDist,
-                                                             flags, nbCandidates);
+    const chr::Out O{reinterpret_cast<unsigned long long*>(best), secondDist, flags, nbCandidates};
+    chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    if (prof) profile_end(stream, tok);
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+struct rsfm_ranked_batch {
+    chr::PairDev* dPairs = nullptr;
+    uint32_t* dBegin = nullptr;
+    uint32_t nPairs = 0, total = 0, tables = 0, topK = 0, ratioNum = 0, ratioDen = 1;
+};
+
+extern "C" int rsfm_ranked_batch_destroy(rsfm_ranked_batch* b) {
+    if (!b) return RSFM_OK;
+    if (b->dPairs) cudaFree(b->dPairs);
+    if (b->dBegin) cudaFree(b->dBegin);
+    delete b;
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t nbPairs, uint32_t nbTables,
+                                        uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
+                                        rsfm_ranked_batch** out) {
+    if (!out || !pairs || nbPairs == 0 || nbTables == 0 || nbTables > 8 || topK == 0 ||
+        topK > uint32_t(chr::kMaxTopK))
+        return RSFM_ERR_INVALID_ARG;
+    std::vector<chr::PairDev> host(nbPairs);
+    std::vector<uint32_t> begin(nbPairs + 1, 0);
+    uint64_t total = 0;
+    auto mk = [](const rsfm_ranked_image* m) {
+        chr::Img I;
+        I.desc = static_cast<const uint8_t*>(m->desc);
+        I.keys = reinterpret_cast<const uint2*>(m->keys);
+        I.codes = reinterpret_cast<const uint4*>(m->codes);
+        I.ends = m->bucketEnds;
+        I.buckets = m->buckets;
+        I.sqr = m->sqrNormDesc;
+        I.n = m->nbDesc;
+        return I;
+    };
+    for (uint32_t p = 0; p < nbPairs; ++p) {
+        const rsfm_ranked_pair& in = pairs[p];
+        if (!in.query || !in.train) return RSFM_ERR_INVALID_ARG;
+        const rsfm_ranked_image *q = in.query, *t = in.train;
+        if (t->nbDesc >= (1u << 24)) return RSFM_ERR_CAPACITY;  // index shares a word with the distance
+        if (q->nbDesc && (!q->desc || !q->keys || !q->codes || !q->sqrNormDesc || !in.best || !in.secondDist ||
+                          !in.flags))
+            return RSFM_ERR_INVALID_ARG;
+        if (q->nbDesc && t->nbDesc && (!t->desc || !t->keys || !t->codes || !t->bucketEnds || !t->buckets ||
+                                       !t->sqrNormDesc))
+            return RSFM_ERR_INVALID_ARG;
+        host[p].q = mk(q);
+        host[p].t = mk(t);
+        host[p].o = chr::Out{reinterpret_cast<unsigned long long*>(in.best), in.secondDist, in.flags, in.nbCandidates};
+        begin[p] = uint32_t(total);
+        total += q->nbDesc;
+        if (total >= (1ull << 32)) return RSFM_ERR_CAPACITY;
+    }
+    begin[nbPairs] = uint32_t(total);
+    auto* b = new rsfm_ranked_batch();
+    if (cudaMalloc(reinterpret_cast<void**>(&b->dPairs), sizeof(chr::PairDev) * nbPairs) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&b->dBegin), sizeof(uint32_t) * (nbPairs + 1)) != cudaSuccess ||
+        cudaMemcpy(b->dPairs, host.data(), sizeof(chr::PairDev) * nbPairs, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->dBegin, begin.data(), sizeof(uint32_t) * (nbPairs + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        rsfm_ranked_batch_destroy(b);
+        return RSFM_ERR_CUDA;
+    }
+    b->nPairs = nbPairs;
+    b->total = uint32_t(total);
+    b->tables = nbTables;
+    b->topK = topK;
+    b->ratioNum = ratioNum;
+    b->ratioDen = ratioDen;
+    *out = b;
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t stream) {
+    launch_count_reset();
+    if (!b) return RSFM_ERR_INVALID_ARG;
+    if (b->total == 0) return RSFM_OK;
+    const uint32_t grid = std::min<uint32_t>((b->total + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
+    void* tok = nullptr;
+    const bool prof = profile_begin(stream, &tok);
+    chr::ranked_batch_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total,
+                                                                   b->tables, b->topK, b->ratioNum, b->ratioDen);
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);
     launch_count_add(1);
