@@ -330,6 +330,11 @@ def run_ours(args):
     threads = os.cpu_count() or 1
     rows, (cpu_val, cpu_dt) = _cpu_sample(q, t, threads, 10.0)
 
+    extras = {}
+    if not args.no_extras:
+        extras["batched"] = run_batched(dev, stream)
+        extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
+
     line = {
         "metric": METRIC,
         "value": value,
@@ -353,9 +358,114 @@ def run_ours(args):
         "clocks": clocks,
         "int8_tops_effective": nops / (ms_per_step * 1e-3) / 1e12,
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def _events_ms(fn, reps, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_batched(dev, stream, seed=2):
+    """Config 2: 512 uneven pairs (sizes U[2000,16000], overlap U[0.1,0.7], noise U[4,12]) as one
+    autotuned graph plan vs. one rsfm_bf_match_ext call per pair. Inputs (about 1.2 GB) exceed L2."""
+    import torch
+    import rapidsfm_b200 as R
+    from rapidsfm_b200 import synth
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    tasks, pairs = [], 0
+    for _ in range(512):
+        na, nb = int(rng.integers(2000, 16001)), int(rng.integers(2000, 16001))
+        q, t, _ = synth.make_pair_torch(na, nb, float(rng.uniform(0.1, 0.7)), float(rng.uniform(4, 12)), g, dev)
+        tasks.append(R.BFTask(q, t))
+        pairs += na * nb
+    t0 = time.perf_counter()
+    opts, _ = R.autotune_plan(tasks, reps=2)
+    tune_s = time.perf_counter() - t0
+    plan = R.BFPlan(tasks, options=opts)
+    plan_ms = _events_ms(lambda: plan.launch(stream), 5, stream)
+    per_ms = _events_ms(lambda: [R.bf_match_ext([t], stream=stream) for t in tasks], 2, stream)
+    plan.close()
+    return {"workload": "512 pairs, N,M ~ U[2000,16000]", "desc_pairs": pairs,
+            "plan_ms": plan_ms, "plan_desc_pairs_per_s": pairs / (plan_ms * 1e-3),
+            "per_pair_ms": per_ms, "per_pair_desc_pairs_per_s": pairs / (per_ms * 1e-3),
+            "speedup_vs_per_pair": per_ms / plan_ms,
+            "options": {"rowTiles": opts.rowTiles, "colBlocks": opts.colBlocks,
+                        "epilogueGroups": opts.epilogueGroups, "schedule": opts.schedule},
+            "autotune_s": tune_s, "int8_tops": 256.0 * pairs / (plan_ms * 1e-3) / 1e12}
+
+
+def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
+    """Configs 3 and 4: n_pairs pairs of n descriptors (40% overlap, noise 8); ranked cascade
+    matching (T tables x 8 bits, 128-bit Hamming ranking, top-10 exact re-rank, ratio 0.8) with
+    random projections vs. the learned hash, all pairs in one launch each. Recall = share of the
+    brute-force matches passing ratio test and cross-check that the hash matcher finds."""
+    import torch
+    import rapidsfm_b200 as R
+    from rapidsfm_b200 import cashash as ch
+    from rapidsfm_b200 import learned_hash as lh
+    from rapidsfm_b200 import synth
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    imgs = [synth.make_pair_torch(n, n, 0.4, 8.0, g, dev)[:2] for _ in range(n_pairs)]
+    tasks = [R.BFTask(q, t) for q, t in imgs]
+    plan = R.BFPlan(tasks)
+    bf_ms = _events_ms(lambda: plan.launch(stream), 2, stream)
+    plan.close()
+    truth = [((t.flagsA & 3) == 3, t.bestA & 0xFFFFFFFF) for t in tasks]
+    pairs = n_pairs * n * n
+    out = {"workload": f"{n_pairs} pairs x {n} descriptors, 40% overlap, noise 8", "desc_pairs": pairs,
+           "brute_force_plan_ms": bf_ms}
+    hashers = {"plain": ch.CasHash(ch.gaussian_weights(1))}
+    wpath = lh.default_params_path()
+    if os.path.exists(wpath):
+        hashers["learned"] = lh.LearnedHash(np.load(wpath))
+    for name, h in hashers.items():
+        if name == "plain":
+            for q, t in imgs:
+                h.fit(q)
+                h.fit(t)
+        t0 = time.perf_counter()
+        ranked = []
+        for q, t in imgs:
+            kq, cq = h.hash(q, stream=stream)[:2]
+            kt, ct = h.hash(t, stream=stream)[:2]
+            ranked.append((ch.RankedImage(q, kq, cq, stream=stream), ch.RankedImage(t, kt, ct, stream=stream)))
+        torch.cuda.synchronize()
+        hash_s = time.perf_counter() - t0
+        rows = {}
+        for tables in (2, 3, 4, 6):
+            batch = ch.RankedBatch(ranked, tables, 10)
+            ms = _events_ms(lambda: batch.launch(stream), 3, stream)
+            hit = torch.zeros((), dtype=torch.int64, device=dev)
+            tot = torch.zeros((), dtype=torch.int64, device=dev)
+            for (ok, gt), (best, _, _, _) in zip(truth, batch.results):
+                hit += (((best & 0xFFFFFFFF) == gt) & ok).sum()
+                tot += ok.sum()
+            rows[str(tables)] = {"match_ms": ms, "recall": int(hit) / max(1, int(tot)),
+                                 "desc_pairs_per_s": pairs / (ms * 1e-3)}
+            batch.close()
+        ok98 = [int(k) for k, v in rows.items() if v["recall"] >= 0.98]
+        out[name] = {"tables": rows, "hash_and_buckets_host_s": hash_s,
+                     "fewest_tables_at_98pct_recall": min(ok98) if ok98 else None}
+    if "learned" in out:
+        p6 = out["plain"]["tables"]["6"]
+        ok = [v for v in out["learned"]["tables"].values() if v["recall"] >= p6["recall"]]
+        out["learned_speedup_at_plain_recall"] = (p6["match_ms"] / min(v["match_ms"] for v in ok)) if ok else None
+    return out
 
 
 def main():
@@ -364,7 +474,12 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=0, help="descriptors per side (smaller profiling cases)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and cascade-hash sections")
+    ap.add_argument("--cascade-pairs", type=int, default=1000)
     args = ap.parse_args()
+    if args.size:
+        globals().update(N_QUERY=args.size, N_TRAIN=args.size, WORKLOAD=f"bf_pair_{args.size}x{args.size}")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -147,3 +147,58 @@ def mine_correspondences(pairs, ratio_num=64, ratio_den=100):
         ti = (t.bestA[ok.bool()] & 0xFFFFFFFF).to(torch.int32)
         out.append((qi, ti))
     return out
+
+
+def default_params_path():
+    """Trained parameter block shipped with the package (written by `python -m
+    rapidsfm_b200.learned_hash --out <path>`)."""
+    import os
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "learned_hash_params.npy")
+
+
+def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3, margin=48.0, seed=0,
+                           device="cuda", log=None):
+    """Trains the learned hash on correspondences the brute-force matcher produces (ratio test and
+    cross-check passed) on `n_pairs` seeded synthetic pairs (40% overlap, noise 8); negatives are
+    random train descriptors of the same pair. Returns the f32 parameter block."""
+    from . import synth
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 12345)
+    qs, ts, A, P = [], [], [], []
+    for k in range(n_pairs):
+        q, t, _ = synth.make_pair_torch(n, n, 0.4, 8.0, g, device)
+        (qi, ti), = mine_correspondences([(q, t)])
+        qs.append(q)
+        ts.append(t)
+        A.append(qi + k * n)
+        P.append(ti + k * n)
+    Q, T = torch.cat(qs), torch.cat(ts)
+    A, P = torch.cat(A), torch.cat(P)
+    params = center_output_bias(init_params(seed), lambda p: LearnedHash(p, device=device), Q[:20000])
+    tr = Trainer(params, batch, lr=lr, margin=margin)
+    for s in range(steps):
+        sel = torch.randint(0, len(A), (batch,), device=device, generator=g)
+        ip = P[sel].int()
+        inn = ((ip // n) * n + torch.randint(0, n, (batch,), device=device, generator=g)).int()
+        tr.step(Q, A[sel].int(), T, ip, T, inn)
+        if log and (s % 1000 == 0 or s == steps - 1):
+            log(f"step {s} loss {tr.loss.item():.4f}")
+    out = tr.params()
+    tr.close()
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import os
+    ap = argparse.ArgumentParser(description="train the learned hash on brute-force correspondences")
+    ap.add_argument("--out", default=default_params_path())
+    ap.add_argument("--pairs", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--margin", type=float, default=48.0)
+    a = ap.parse_args()
+    p = train_from_brute_force(a.pairs, steps=a.steps, batch=a.batch, margin=a.margin, log=print)
+    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    np.save(a.out, p)
+    print("saved", a.out)
