@@ -217,7 +217,14 @@ typedef struct rsfm_ranked_image {
     const uint32_t* buckets;
     const uint32_t* sqrNormDesc;
     uint32_t nbDesc;
+    const uint32_t* records;  /* optional (32-byte aligned): rsfm_ranked_pack_records output */
 } rsfm_ranked_image;
+
+/* Packs keys, codes and squared norms into one 32-byte record per descriptor (8 x uint32:
+ * key bytes 0-7, code words 0-3, squared norm, 0), so a candidate costs one memory sector in
+ * ranked matching instead of two (no reference counterpart). records: nbDesc x 32 bytes. */
+int rsfm_ranked_pack_records(const uint8_t* keys, const uint32_t* codes, const uint32_t* sqrNormDesc,
+                             uint32_t nbDesc, uint32_t* records, cudaStream_t stream);
 
 /* Ranked cascade-hash matching (no reference counterpart): for every query descriptor, the
  * candidates are the train descriptors sharing one of the first nbTables bucket keys; they are

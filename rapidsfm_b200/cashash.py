@@ -51,6 +51,10 @@ class RankedImage:
                    "rsfm_cashash_compute_bucket_bound")
         _lib.check(lib.rsfm_cashash_build_buckets(_p(keys), n, _p(lower), _p(self.buckets), s),
                    "rsfm_cashash_build_buckets")
+        # one 32-byte record per descriptor (keys, code, norm): one sector per candidate when matching
+        self.records = torch.empty((max(n, 1), 8), dtype=torch.int32, device=dev)
+        _lib.check(lib.rsfm_ranked_pack_records(_p(keys), _p(codes), _p(self.sqr), n, _p(self.records), s),
+                   "rsfm_ranked_pack_records")
         self.n = n
 
     def max_bucket_size(self):
@@ -58,7 +62,8 @@ class RankedImage:
 
     def as_ctype(self):
         return _lib.RankedImage(self.desc.data_ptr(), self.keys.data_ptr(), self.codes.data_ptr(),
-                                self.upper.data_ptr(), self.buckets.data_ptr(), self.sqr.data_ptr(), self.n)
+                                self.upper.data_ptr(), self.buckets.data_ptr(), self.sqr.data_ptr(), self.n,
+                                self.records.data_ptr())
 
 
 def match_ranked(query, train, tables=6, top_k=10, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08,

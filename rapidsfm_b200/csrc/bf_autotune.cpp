@@ -117,11 +117,11 @@ extern "C" int rsfm_bf_plan_autotune(const rsfm_sift_bf_task* tasks, size_t nbTa
             win = o;
         }
     };
-    // Stage 1: unit shape with two epilogue warpgroups, largest pairs first.
+    // Stage 1: unit shape with four epilogue warpgroups, largest pairs first.
     for (uint32_t rt : {8u, 4u, 2u})
         for (uint32_t cb : {8u, 4u, 2u, 1u}) {
             if (st != RSFM_OK) break;
-            trial(rsfm_bf_plan_options{rt, cb, 2u, 1u, 1u});
+            trial(rsfm_bf_plan_options{rt, cb, 4u, 1u, 1u});
         }
     // Stage 2: warpgroups and schedule around the best shape.
     const rsfm_bf_plan_options shape = win;

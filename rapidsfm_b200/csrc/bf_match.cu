@@ -158,8 +158,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
     constexpr int kCPW = Cfg<kWG>::kCPW;
     constexpr int kBStages = Cfg<kWG>::kBStages;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem<kWG>& S =
-        *reinterpret_cast<Smem<kWG>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    Smem<kWG>& S = smem_aligned_1024<Smem<kWG>>(smem_raw);
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
 
@@ -582,11 +581,11 @@ static void choose_shape(const std::vector<std::pair<uint32_t, uint32_t>>& sizes
     colBlocks = 1;
 }
 
-// Epilogue warpgroups (2 or 4); RSFM_BF_EPILOGUE_GROUPS overrides the default for tuning runs.
+// Epilogue warpgroups (4 by default, or 2); RSFM_BF_EPILOGUE_GROUPS overrides it for tuning runs.
 static int epilogue_groups() {
     static int g = [] {
         const char* e = getenv("RSFM_BF_EPILOGUE_GROUPS");
-        return (e && atoi(e) == 4) ? 4 : 2;
+        return (e && atoi(e) == 2) ? 2 : 4;
     }();
     return g;
 }

@@ -97,7 +97,7 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
             const int32_t* __restrict__ bias, int channels, uint32_t n, uint8_t* __restrict__ keys,
             uint32_t* __restrict__ remap, uint32_t* __restrict__ histogram, uint32_t* err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    HashSmem& S = *reinterpret_cast<HashSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    HashSmem& S = smem_aligned_1024<HashSmem>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t tiles = (n + 127) / 128;
     for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) (&S.hist[0][0])[x] = 0;

@@ -100,7 +100,7 @@ __global__ void init_kernel(const __grid_constant__ Params P, uint32_t nTrain, u
 __global__ void __launch_bounds__(kThreads) match_kernel(const __grid_constant__ Params P, uint32_t nTrain,
                                                          const uint32_t* __restrict__ qSizes) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    Smem& S = smem_aligned_1024<Smem>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     if (tid == 0) {
         mbar_init(&S.mma, 1);

@@ -27,8 +27,20 @@ struct Img {
     const uint32_t* ends;  // [8][256] inclusive upper bounds
     const uint32_t* buckets;  // [8][n]: bucket (s, b) at buckets[s*n + lower(s,b)]
     const uint32_t* sqr;
+    const uint4* rec;      // optional packed records, 2 x uint4 per descriptor (see pack_kernel)
     uint32_t n;
 };
+
+// Packed candidate record (one 32-byte sector): {key.x, key.y, code.x, code.y}, {code.z, code.w, sqr, 0}.
+__global__ void pack_kernel(const uint2* __restrict__ keys, const uint4* __restrict__ codes,
+                            const uint32_t* __restrict__ sqr, uint32_t n, uint4* __restrict__ rec) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint2 k = keys[i];
+        const uint4 c = codes[i];
+        rec[2 * size_t(i)] = make_uint4(k.x, k.y, c.x, c.y);
+        rec[2 * size_t(i) + 1] = make_uint4(c.z, c.w, sqr[i], 0u);
+    }
+}
 
 // Bytes equal in a and b -> bit set per byte (4 bits for 4 bytes of each word).
 __device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
@@ -81,33 +93,64 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
         cnt = 0;
     };
 
-    for (uint32_t s = 0; s < tables; ++s) {
-        const uint32_t bk = s < 4 ? (qk.x >> (8 * s)) & 0xFFu : (qk.y >> (8 * (s - 4))) & 0xFFu;
-        const uint32_t lo = bk ? T.ends[s * 256 + bk - 1] : 0u, hi = T.ends[s * 256 + bk];
-        const uint32_t* list = T.buckets + size_t(s) * T.n;
-        for (uint32_t x0 = lo; x0 < hi; x0 += 32) {
-            const uint32_t x = x0 + lane;
-            bool keep = false;
-            uint32_t key = 0;
-            if (x < hi) {
-                const uint32_t j = list[x];
-                const uint2 tk = T.keys[j];
-                const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
-                keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
-                if (keep) {
-                    const uint4 tc = T.codes[j];
-                    const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
-                                       __popc(tc.w ^ qc.w);
-                    key = (h << 24) | j;
+    // Bucket ranges of all tables at once (lane s holds table s), then one flattened pass over
+    // the concatenated member lists: lane l takes candidate base + l wherever it falls.
+    uint32_t myLo = 0, mySize = 0;
+    if (lane < tables) {
+        const uint32_t bk = lane < 4 ? (qk.x >> (8 * lane)) & 0xFFu : (qk.y >> (8 * (lane - 4))) & 0xFFu;
+        myLo = bk ? T.ends[lane * 256 + bk - 1] : 0u;
+        mySize = T.ends[lane * 256 + bk] - myLo;
+    }
+    uint32_t incl = mySize;  // inclusive prefix of list sizes over the tables
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= uint32_t(o)) incl += v;
+    }
+    uint32_t endS[8], loS[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        endS[t] = __shfl_sync(0xffffffffu, incl, t);
+        loS[t] = __shfl_sync(0xffffffffu, myLo, t);
+    }
+    const uint32_t all = endS[tables - 1];
+    for (uint32_t x0 = 0; x0 < all; x0 += 32) {
+        const uint32_t x = x0 + lane;
+        bool keep = false;
+        uint32_t key = 0;
+        if (x < all) {
+            uint32_t s = 0, begin = 0;
+#pragma unroll
+            for (int t = 0; t < 7; ++t)
+                if (uint32_t(t) + 1 < tables && x >= endS[t]) {
+                    s = t + 1;
+                    begin = endS[t];
                 }
+            const uint32_t j = T.buckets[size_t(s) * T.n + loS[s] + (x - begin)];
+            uint2 tk;
+            uint4 tc;
+            if (T.rec) {
+                const uint4 r0 = T.rec[2 * size_t(j)], r1 = T.rec[2 * size_t(j) + 1];
+                tk = make_uint2(r0.x, r0.y);
+                tc = make_uint4(r0.z, r0.w, r1.x, r1.y);
+            } else {
+                tk = T.keys[j];
+                tc = T.codes[j];
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            if (cnt + __popc(m) > kBuf) select();
-            if (keep) B[cnt + __popc(m & lt)] = key;
-            cnt += __popc(m);
-            total += __popc(m);
-            __syncwarp();
+            const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
+            keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
+            if (keep) {
+                const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
+                                   __popc(tc.w ^ qc.w);
+                key = (h << 24) | j;
+            }
         }
+        const uint32_t m = __ballot_sync(0xffffffffu, keep);
+        if (cnt + __popc(m) > kBuf) select();
+        if (keep) B[cnt + __popc(m & lt)] = key;
+        cnt += __popc(m);
+        total += __popc(m);
+        __syncwarp();
     }
     select();
     // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
@@ -120,7 +163,7 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
         uint32_t dot = __dp4a(qw, tw, 0u);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-        const uint32_t d = nq + T.sqr[j] - 2u * dot;
+        const uint32_t d = nq + (T.rec ? T.rec[2 * size_t(j) + 1].z : T.sqr[j]) - 2u * dot;
         if (d < bd || (d == bd && j < bj)) {
             sd = bd;
             bd = d;
@@ -195,6 +238,7 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
         I.ends = m->bucketEnds;
         I.buckets = m->buckets;
         I.sqr = m->sqrNormDesc;
+        I.rec = reinterpret_cast<const uint4*>(m->records);
         I.n = m->nbDesc;
         return I;
     };
@@ -244,6 +288,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
         I.ends = m->bucketEnds;
         I.buckets = m->buckets;
         I.sqr = m->sqrNormDesc;
+        I.rec = reinterpret_cast<const uint4*>(m->records);
         I.n = m->nbDesc;
         return I;
     };
@@ -296,6 +341,22 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
                                                                    b->tables, b->topK, b->ratioNum, b->ratioDen);
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_ranked_pack_records(const uint8_t* keys, const uint32_t* codes, const uint32_t* sqrNormDesc,
+                                        uint32_t nbDesc, uint32_t* records, cudaStream_t stream) {
+    launch_count_reset();
+    if (nbDesc == 0) return RSFM_OK;
+    if (!keys || !codes || !sqrNormDesc || !records || (reinterpret_cast<uintptr_t>(keys) & 7u) ||
+        (reinterpret_cast<uintptr_t>(codes) & 15u) || (reinterpret_cast<uintptr_t>(records) & 31u))
+        return RSFM_ERR_INVALID_ARG;
+    const uint32_t grid = std::min<uint32_t>((nbDesc + 255) / 256, uint32_t(8 * sm_count()));
+    chr::pack_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const uint2*>(keys),
+                                               reinterpret_cast<const uint4*>(codes), sqrNormDesc, nbDesc,
+                                               reinterpret_cast<uint4*>(records));
+    RSFM_CUDA_TRY(cudaGetLastError());
     launch_count_add(1);
     return RSFM_OK;
 }

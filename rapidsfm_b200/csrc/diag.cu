@@ -45,7 +45,7 @@ using namespace sm100;
 // MMA-only loop: 128x256x32 u8 UMMAs from static shared-memory tiles into two TMEM buffers.
 __global__ void __launch_bounds__(128, 1) int8_peak_kernel(int iters, uint32_t* err, int32_t* sink) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* smem = &smem_aligned_1024<uint8_t>(smem_raw);
     __shared__ uint64_t bar;
     __shared__ uint32_t tbase;
     for (int i = threadIdx.x; i < (16384 + 32768) / 4; i += blockDim.x)

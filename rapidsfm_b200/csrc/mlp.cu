@@ -55,7 +55,7 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
              const float* __restrict__ b2, const uint8_t* __restrict__ desc, uint32_t n, float* __restrict__ out,
              uint8_t* __restrict__ keys, uint32_t* __restrict__ codes, uint32_t* err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    InfSmem& S = *reinterpret_cast<InfSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    InfSmem& S = smem_aligned_1024<InfSmem>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     // weights into swizzled K panels (16-byte chunks)
     for (uint32_t x = tid; x < 256 * 16; x += kInfThreads) {

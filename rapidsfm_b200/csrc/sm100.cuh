@@ -26,6 +26,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// Dynamic shared memory rounded up to a 1024-byte boundary. The pointer arithmetic stays on the
+// __shared__ array (no integer round trip), so the compiler keeps the shared address space and
+// emits shared-memory loads and stores instead of generic ones.
+template <typename T>
+__device__ __forceinline__ T& smem_aligned_1024(uint8_t* raw) {
+    const uint32_t pad = (1024u - (smem_u32(raw) & 1023u)) & 1023u;
+    return *reinterpret_cast<T*>(raw + pad);
+}
+
 // ---------------------------------------------------------------- mbarrier
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));

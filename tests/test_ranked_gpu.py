@@ -27,16 +27,25 @@ def _prep(oracle, desc, w, bias):
             "sqr": oracle.sqr_norm(desc)}
 
 
-def _ranked_image(rsfm, img, keep):
+def _ranked_image(rsfm, img, keep, records=False):
     t = {k: _dev(v.view(np.int32) if v.dtype == np.uint32 else v) for k, v in img.items()}
     keep.append(t)
+    rec = 0
+    if records:
+        r = torch.empty((max(len(img["desc"]), 1), 8), dtype=torch.int32, device="cuda")
+        keep.append(r)
+        rsfm._lib.check(rsfm._lib.load().rsfm_ranked_pack_records(
+            ctypes.c_void_p(t["keys"].data_ptr()), ctypes.c_void_p(t["codes"].data_ptr()),
+            ctypes.c_void_p(t["sqr"].data_ptr()), len(img["desc"]), ctypes.c_void_p(r.data_ptr()), None), "pack")
+        rec = r.data_ptr()
     return rsfm._lib.RankedImage(t["desc"].data_ptr(), t["keys"].data_ptr(), t["codes"].data_ptr(),
                                  t["upper"].data_ptr(), t["buckets"].data_ptr(), t["sqr"].data_ptr(),
-                                 len(img["desc"]))
+                                 len(img["desc"]), rec)
 
 
+@pytest.mark.parametrize("records", [False, True])
 @pytest.mark.parametrize("n,tables,topk", [(8192, 6, 10), (3000, 6, 10), (1000, 8, 32), (500, 1, 1)])
-def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk):
+def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, records):
     q, t, _ = synth.make_pair(n, n, 0.4, 8.0, seed=n + tables)
     w = _gauss_weights(7)
     acc = oracle.cashash_accumulate(np.concatenate([q, t]))
@@ -44,7 +53,7 @@ def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk):
     bias = oracle.cashash_bias(w, base, acc, 2 * n)
     Q, T = _prep(oracle, q, w, bias), _prep(oracle, t, w, bias)
     keep = []
-    qi, ti = _ranked_image(rsfm, Q, keep), _ranked_image(rsfm, T, keep)
+    qi, ti = _ranked_image(rsfm, Q, keep, records), _ranked_image(rsfm, T, keep, records)
     best = torch.empty(n, dtype=torch.int64, device="cuda")
     sec = torch.empty(n, dtype=torch.int32, device="cuda")
     flg = torch.empty(n, dtype=torch.int32, device="cuda")
