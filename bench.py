@@ -318,7 +318,11 @@ def run_ours(args):
         "peak": peak,
         "unit": "TOP/s",
         "frac": achieved / peak,
-        "traffic": None,
+        # DRAM bytes per launch from an ncu capture of the 16384^2 case (dram__bytes_read.sum +
+        # dram__bytes_write.sum = 4.71 MB), scaled linearly: DRAM traffic is the inputs and outputs,
+        # since the B blocks each row block re-streams hit L2.
+        "traffic": 4.71e6 * (N_QUERY / 16384.0),
+        "traffic_note": "ncu at 16384^2, scaled by n/16384",
         "kernel": "bf_match_kernel",
         "kernel_ms": kernel_ms,
         "peak_source": "measured live: int8 tcgen05 MMA-only probe (rsfm_int8_mma_peak), dense",
