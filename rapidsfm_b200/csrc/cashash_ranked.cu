@@ -17,7 +17,7 @@ namespace rsfm_b200 {
 namespace chr {
 
 constexpr int kWarps = 8;
-constexpr int kBuf = 1024;   // candidate keys per warp buffer
+constexpr int kBuf = 512;    // candidate keys per warp buffer (more are merged in rounds)
 constexpr int kMaxTopK = 32;
 
 struct Img {
@@ -107,18 +107,18 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
         const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= uint32_t(o)) incl += v;
     }
-    uint32_t endS[8], loS[8];
+    uint32_t endS[8];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-        endS[t] = __shfl_sync(0xffffffffu, incl, t);
-        loS[t] = __shfl_sync(0xffffffffu, myLo, t);
-    }
-    const uint32_t all = endS[tables - 1];
-    for (uint32_t x0 = 0; x0 < all; x0 += 32) {
-        const uint32_t x = x0 + lane;
-        bool keep = false;
-        uint32_t key = 0;
-        if (x < all) {
+    for (int t = 0; t < 8; ++t) endS[t] = __shfl_sync(0xffffffffu, incl, t);
+    const uint32_t all = __shfl_sync(0xffffffffu, incl, tables - 1);
+    // Four candidates per lane per round: their list entries, then their records, are loaded
+    // together so the memory latency is paid once per round instead of once per candidate.
+    constexpr int kU = 4;
+    for (uint32_t x0 = 0; x0 < all; x0 += 32 * kU) {
+        uint32_t jj[kU], ss[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + 32u * u + lane;
             uint32_t s = 0, begin = 0;
 #pragma unroll
             for (int t = 0; t < 7; ++t)
@@ -126,50 +126,86 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
                     s = t + 1;
                     begin = endS[t];
                 }
-            const uint32_t j = T.buckets[size_t(s) * T.n + loS[s] + (x - begin)];
-            uint2 tk;
-            uint4 tc;
-            if (T.rec) {
+            ss[u] = s;
+            const uint32_t lo = __shfl_sync(0xffffffffu, myLo, s);  // lane s holds table s's range
+            jj[u] = x < all ? T.buckets[size_t(s) * T.n + lo + (x - begin)] : 0xFFFFFFFFu;
+        }
+        uint2 tk[kU];
+        uint4 tc[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t j = jj[u];
+            if (j == 0xFFFFFFFFu) {
+                tk[u] = make_uint2(0, 0);
+                tc[u] = make_uint4(0, 0, 0, 0);
+            } else if (T.rec) {
                 const uint4 r0 = T.rec[2 * size_t(j)], r1 = T.rec[2 * size_t(j) + 1];
-                tk = make_uint2(r0.x, r0.y);
-                tc = make_uint4(r0.z, r0.w, r1.x, r1.y);
+                tk[u] = make_uint2(r0.x, r0.y);
+                tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
             } else {
-                tk = T.keys[j];
-                tc = T.codes[j];
-            }
-            const uint32_t eqm = eq_bytes(tk.x, qk.x) | (eq_bytes(tk.y, qk.y) << 4);
-            keep = (eqm & ((1u << s) - 1u)) == 0;  // first table where j collides
-            if (keep) {
-                const uint32_t h = __popc(tc.x ^ qc.x) + __popc(tc.y ^ qc.y) + __popc(tc.z ^ qc.z) +
-                                   __popc(tc.w ^ qc.w);
-                key = (h << 24) | j;
+                tk[u] = T.keys[j];
+                tc[u] = T.codes[j];
             }
         }
-        const uint32_t m = __ballot_sync(0xffffffffu, keep);
-        if (cnt + __popc(m) > kBuf) select();
-        if (keep) B[cnt + __popc(m & lt)] = key;
-        cnt += __popc(m);
-        total += __popc(m);
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t j = jj[u];
+            bool keep = false;
+            uint32_t key = 0;
+            if (j != 0xFFFFFFFFu) {
+                const uint32_t eqm = eq_bytes(tk[u].x, qk.x) | (eq_bytes(tk[u].y, qk.y) << 4);
+                keep = (eqm & ((1u << ss[u]) - 1u)) == 0;  // first table where j collides
+                if (keep) {
+                    const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
+                                       __popc(tc[u].w ^ qc.w);
+                    key = (h << 24) | j;
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (cnt + __popc(m) > kBuf) select();
+            if (keep) B[cnt + __popc(m & lt)] = key;
+            cnt += __popc(m);
+            total += __popc(m);
+            __syncwarp();
+        }
     }
     select();
     // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
     const uint32_t qw = reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128)[lane];
     const uint32_t nq = Q.sqr[i];
     uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
-    for (uint32_t r = 0; r < nTop; ++r) {
-        const uint32_t j = TOP[r] & 0xFFFFFFu;
-        const uint32_t tw = reinterpret_cast<const uint32_t*>(T.desc + size_t(j) * 128)[lane];
-        uint32_t dot = __dp4a(qw, tw, 0u);
+    // Candidates in groups of 8: all their loads first, then the dot products.
+    for (uint32_t r0 = 0; r0 < nTop; r0 += 8) {
+        uint32_t jr[8], tw[8], ns[8];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-        const uint32_t d = nq + (T.rec ? T.rec[2 * size_t(j) + 1].z : T.sqr[j]) - 2u * dot;
-        if (d < bd || (d == bd && j < bj)) {
-            sd = bd;
-            bd = d;
-            bj = j;
-        } else if (d < sd) {
-            sd = d;
+        for (int k = 0; k < 8; ++k) {
+            jr[k] = r0 + k < nTop ? (TOP[r0 + k] & 0xFFFFFFu) : 0xFFFFFFFFu;
+            tw[k] = 0;
+            ns[k] = 0;
+            if (jr[k] != 0xFFFFFFFFu) {
+                tw[k] = reinterpret_cast<const uint32_t*>(T.desc + size_t(jr[k]) * 128)[lane];
+                ns[k] = T.rec ? T.rec[2 * size_t(jr[k]) + 1].z : T.sqr[jr[k]];
+            }
+        }
+        uint32_t dot[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) dot[k] = __dp4a(qw, tw[k], 0u);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) dot[k] += __shfl_xor_sync(0xffffffffu, dot[k], o);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t j = jr[k];
+            if (j == 0xFFFFFFFFu) continue;
+            const uint32_t d = nq + ns[k] - 2u * dot[k];
+            if (d < bd || (d == bd && j < bj)) {
+                sd = bd;
+                bd = d;
+                bj = j;
+            } else if (d < sd) {
+                sd = d;
+            }
         }
     }
     if (lane == 0) {
@@ -183,7 +219,7 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * kWarps) ranked_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
+__global__ void __launch_bounds__(32 * kWarps, 4) ranked_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
                                                              uint32_t ratioNum, uint32_t ratioDen, Out O) {
     __shared__ uint32_t buf[kWarps][kBuf];
     __shared__ uint32_t top[kWarps][kMaxTopK];
@@ -197,7 +233,7 @@ struct PairDev {
     Img q, t;
     Out o;
 };
-__global__ void __launch_bounds__(32 * kWarps) ranked_batch_kernel(const PairDev* __restrict__ pairs,
+__global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const PairDev* __restrict__ pairs,
                                                                    const uint32_t* __restrict__ begin, uint32_t nPairs,
                                                                    uint32_t total, uint32_t tables, uint32_t topK,
                                                                    uint32_t ratioNum, uint32_t ratioDen) {
