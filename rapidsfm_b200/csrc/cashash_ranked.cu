@@ -61,30 +61,92 @@ struct Out {
 // One query descriptor i of image Q against image T, by one warp; B / TOP are the warp's buffers.
 __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t i, uint32_t tables, uint32_t topK,
                                             uint32_t ratioNum, uint32_t ratioDen, const Out& O, uint32_t* B,
-                                            uint32_t* TOP, uint32_t lane) {
+                                            uint32_t* TOP, uint32_t* H, uint32_t* C, uint32_t lane) {
     const uint32_t lt = (1u << lane) - 1u;
     const uint2 qk = Q.keys[i];
     const uint4 qc = Q.codes[i];
     uint32_t cnt = 0, nTop = 0, total = 0;
 
-    // Extract the topK smallest keys of buffer + running top into TOP (lane r keeps round r's).
+    // Extract the topK smallest keys of buffer + running top into TOP (ascending). Keys are
+    // distinct (the index is in the low 24 bits). Fast path: a per-warp histogram of the Hamming
+    // distances gives the threshold h* of the topK-th key; if at most 32 keys have distance <= h*
+    // they are sorted across the lanes (bitonic) and the first topK kept. Otherwise topK rounds of
+    // a warp minimum over all keys.
     auto select = [&]() {
-        uint32_t prev = 0, have = 0, mine = 0xFFFFFFFFu;
         const uint32_t want = min(topK, cnt + nTop);
-        for (uint32_t r = 0; r < want; ++r) {
-            uint32_t mn = 0xFFFFFFFFu;
-            for (uint32_t x = lane; x < cnt; x += 32) {
-                const uint32_t v = B[x];
-                if ((have == 0 || v > prev) && v < mn) mn = v;
+        for (uint32_t b = lane; b < 160; b += 32) H[b] = 0;
+        __syncwarp();
+        for (uint32_t x = lane; x < cnt; x += 32) atomicAdd(&H[B[x] >> 24], 1u);
+        if (lane < nTop) atomicAdd(&H[TOP[lane] >> 24], 1u);
+        __syncwarp();
+        uint32_t c5[5], local = 0;
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+            c5[b] = H[5 * lane + b];
+            local += c5[b];
+        }
+        uint32_t incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= uint32_t(o)) incl += v;
+        }
+        uint32_t hs = 0xFFFFFFFFu, run = incl - local;
+        if (run < want && want <= incl) {
+#pragma unroll
+            for (int b = 0; b < 5; ++b) {
+                run += c5[b];
+                if (run >= want && hs == 0xFFFFFFFFu) hs = 5 * lane + b;
             }
-            if (lane < nTop) {
-                const uint32_t v = TOP[lane];
-                if ((have == 0 || v > prev) && v < mn) mn = v;
+        }
+        hs = __reduce_min_sync(0xffffffffu, hs);
+        // keys with distance <= hs, compacted into C (at most 32 kept)
+        uint32_t m = 0;
+        for (uint32_t x0 = 0; x0 < cnt; x0 += 32) {
+            const uint32_t x = x0 + lane;
+            const uint32_t v = x < cnt ? B[x] : 0xFFFFFFFFu;
+            const bool k = x < cnt && (v >> 24) <= hs;
+            const uint32_t bm = __ballot_sync(0xffffffffu, k);
+            if (k && m + __popc(bm & lt) < 32) C[m + __popc(bm & lt)] = v;
+            m += __popc(bm);
+        }
+        {
+            const bool k = lane < nTop && (TOP[lane] >> 24) <= hs;
+            const uint32_t v = lane < nTop ? TOP[lane] : 0xFFFFFFFFu;
+            const uint32_t bm = __ballot_sync(0xffffffffu, k);
+            if (k && m + __popc(bm & lt) < 32) C[m + __popc(bm & lt)] = v;
+            m += __popc(bm);
+        }
+        __syncwarp();
+        uint32_t mine = 0xFFFFFFFFu;
+        if (m <= 32) {
+            uint32_t v = lane < m ? C[lane] : 0xFFFFFFFFu;
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint32_t w = __shfl_xor_sync(0xffffffffu, v, j);
+                    const bool up = (lane & uint32_t(k)) == 0, lower = (lane & uint32_t(j)) == 0;
+                    v = (lower == up) ? min(v, w) : max(v, w);
+                }
+            mine = v;
+        } else {
+            uint32_t prev = 0, have = 0;
+            for (uint32_t r = 0; r < want; ++r) {
+                uint32_t mn = 0xFFFFFFFFu;
+                for (uint32_t x = lane; x < cnt; x += 32) {
+                    const uint32_t v = B[x];
+                    if ((have == 0 || v > prev) && v < mn) mn = v;
+                }
+                if (lane < nTop) {
+                    const uint32_t v = TOP[lane];
+                    if ((have == 0 || v > prev) && v < mn) mn = v;
+                }
+                mn = __reduce_min_sync(0xffffffffu, mn);
+                prev = mn;
+                have = 1;
+                if (lane == r) mine = mn;
             }
-            mn = __reduce_min_sync(0xffffffffu, mn);
-            prev = mn;
-            have = 1;
-            if (lane == r) mine = mn;
         }
         __syncwarp();
         if (lane < want) TOP[lane] = mine;
@@ -107,9 +169,6 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
         const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= uint32_t(o)) incl += v;
     }
-    uint32_t endS[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) endS[t] = __shfl_sync(0xffffffffu, incl, t);
     const uint32_t all = __shfl_sync(0xffffffffu, incl, tables - 1);
     // Four candidates per lane per round: their list entries, then their records, are loaded
     // together so the memory latency is paid once per round instead of once per candidate.
@@ -119,15 +178,16 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const uint32_t x = x0 + 32u * u + lane;
-            uint32_t s = 0, begin = 0;
-#pragma unroll
-            for (int t = 0; t < 7; ++t)
-                if (uint32_t(t) + 1 < tables && x >= endS[t]) {
-                    s = t + 1;
-                    begin = endS[t];
-                }
-            ss[u] = s;
+            // table of candidate x: number of tables whose lists end at or before x (binary search
+            // over the inclusive ends held by lanes 0..7; ends past the last table equal `all`)
+            uint32_t t = 0;
+            if (__shfl_sync(0xffffffffu, incl, 3) <= x) t = 4;
+            if (__shfl_sync(0xffffffffu, incl, t + 1) <= x) t += 2;
+            if (__shfl_sync(0xffffffffu, incl, t) <= x) t += 1;
+            const uint32_t s = min(t, tables - 1);
+            const uint32_t begin = __shfl_sync(0xffffffffu, incl - mySize, s);
             const uint32_t lo = __shfl_sync(0xffffffffu, myLo, s);  // lane s holds table s's range
+            ss[u] = s;
             jj[u] = x < all ? T.buckets[size_t(s) * T.n + lo + (x - begin)] : 0xFFFFFFFFu;
         }
         uint2 tk[kU];
@@ -223,9 +283,11 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_kernel(Img Q, Img T, ui
                                                              uint32_t ratioNum, uint32_t ratioDen, Out O) {
     __shared__ uint32_t buf[kWarps][kBuf];
     __shared__ uint32_t top[kWarps][kMaxTopK];
+    __shared__ uint32_t hist[kWarps][160];
+    __shared__ uint32_t comp[kWarps][32];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     for (uint32_t i = blockIdx.x * kWarps + warp; i < Q.n; i += gridDim.x * kWarps)
-        match_query(Q, T, i, tables, topK, ratioNum, ratioDen, O, buf[warp], top[warp], lane);
+        match_query(Q, T, i, tables, topK, ratioNum, ratioDen, O, buf[warp], top[warp], hist[warp], comp[warp], lane);
 }
 
 // Many pairs in one launch: global query g belongs to the last pair p with begin[p] <= g.
@@ -239,6 +301,8 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
                                                                    uint32_t ratioNum, uint32_t ratioDen) {
     __shared__ uint32_t buf[kWarps][kBuf];
     __shared__ uint32_t top[kWarps][kMaxTopK];
+    __shared__ uint32_t hist[kWarps][160];
+    __shared__ uint32_t comp[kWarps][32];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     for (uint32_t g = blockIdx.x * kWarps + warp; g < total; g += gridDim.x * kWarps) {
         uint32_t lo = 0, hi = nPairs - 1;
@@ -247,7 +311,8 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
             if (begin[mid] <= g) lo = mid; else hi = mid - 1;
         }
         const PairDev& P = pairs[lo];
-        match_query(P.q, P.t, g - begin[lo], tables, topK, ratioNum, ratioDen, P.o, buf[warp], top[warp], lane);
+        match_query(P.q, P.t, g - begin[lo], tables, topK, ratioNum, ratioDen, P.o, buf[warp], top[warp], hist[warp],
+                    comp[warp], lane);
     }
 }
 
