@@ -282,6 +282,11 @@ typedef struct rsfm_mlp_trainer rsfm_mlp_trainer;
 int rsfm_mlp_trainer_create(const float* initParamsHost, uint32_t batch, float lr, float margin,
                             rsfm_mlp_trainer** trainer);
 int rsfm_mlp_trainer_model(const rsfm_mlp_trainer* trainer, rsfm_mlp* model);
+/* Loss of later steps: kind 0 = the triplet hinge above (default); kind 1 = a bucket-key loss on
+ * channels 0..47 (6 tables of 8 bits; per table A(u,v) = prod_k max((1 + z_u z_v) / 2, 1e-4), the
+ * soft probability that the keys agree; loss -log(A(a,p) + 1e-6) + lambda * A(a,n)) plus the hinge
+ * over channels 48..127 only. */
+int rsfm_mlp_trainer_set_loss(rsfm_mlp_trainer* trainer, int kind, float lambda);
 int rsfm_mlp_trainer_step(rsfm_mlp_trainer* trainer, const void* a, const uint32_t* ia, const void* p,
                           const uint32_t* ip, const void* n, const uint32_t* in, float* lossDevice,
                           cudaStream_t stream);

@@ -48,6 +48,8 @@ def load():
         "orc_cashash_match_ranked": (None, [_P, _P, _P, u32, _P, _P, _P, u32, i32, i32, u32, u32, _P, _P, _P, _P]),
         "orc_mlp_forward": (None, [_P, _P, _P, _P, _P, u32, _P, _P]),
         "orc_mlp_triplet_grad": (ctypes.c_double, [_P, _P, _P, _P, _P, _P, _P, u32, ctypes.c_float, _P, _P, _P, _P]),
+        "orc_mlp_loss_grad": (ctypes.c_double, [_P, _P, _P, _P, _P, _P, _P, u32, ctypes.c_float, ctypes.c_int,
+                                                ctypes.c_float, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -224,14 +226,17 @@ def mlp_forward(params, desc):
     return out, codes
 
 
-def mlp_triplet_grad(params, a, p, n, margin):
-    """Loss and gradient block (same layout as params) of one triplet batch, in double precision."""
+def mlp_triplet_grad(params, a, p, n, margin, kind=0, lam=0.0):
+    """Loss and gradient block (same layout as params) of one triplet batch, in double precision.
+    kind 0: triplet hinge on all channels; kind 1: bucket-key loss on channels 0..47 (weight lam on
+    negatives) plus the hinge on channels 48..127."""
     w1, b1, w2, b2 = mlp_split(np.asarray(params, dtype=np.float32))
     w1, w2 = bf16_round(w1), bf16_round(w2)
     a, p, n = (np.ascontiguousarray(x, dtype=np.uint8) for x in (a, p, n))
     g = [np.zeros(k, dtype=np.float64) for k in MLP_SIZES]
-    loss = load().orc_mlp_triplet_grad(_c(w1), _c(np.ascontiguousarray(b1)), _c(w2), _c(np.ascontiguousarray(b2)),
-                                       _c(a), _c(p), _c(n), len(a), margin, _c(g[0]), _c(g[1]), _c(g[2]), _c(g[3]))
+    loss = load().orc_mlp_loss_grad(_c(w1), _c(np.ascontiguousarray(b1)), _c(w2), _c(np.ascontiguousarray(b2)),
+                                    _c(a), _c(p), _c(n), len(a), margin, kind, lam, _c(g[0]), _c(g[1]), _c(g[2]),
+                                    _c(g[3]))
     return loss, np.concatenate(g)
 
 

@@ -9,6 +9,7 @@
 // Training loss on triplets (anchor a, positive p, negative n), z = tanh(o):
 //   D(u,v) = sum_c (z_u,c - z_v,c)^2 / 4,   L = mean_b max(0, margin + D(a,p) - D(a,n))
 // Gradients flow through the bf16 rounding of h as through the identity.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -50,9 +51,14 @@ void orc_mlp_forward(const float* w1, const float* b1, const float* w2, const fl
 }
 
 // Loss and gradients (dW1 [256*128], db1 [256], dW2 [128*256], db2 [128]) of one triplet batch.
-double orc_mlp_triplet_grad(const float* w1, const float* b1, const float* w2, const float* b2, const uint8_t* a,
-                            const uint8_t* p, const uint8_t* ng, uint32_t batch, float margin, double* dw1,
-                            double* db1, double* dw2, double* db2) {
+//   kind 0: triplet hinge on all 128 channels (above).
+//   kind 1: bucket-key loss on channels 0..47 (6 tables of 8 bits) plus the triplet hinge on the
+//           code channels 48..127. Per table s and pair (u, v): q_k = max((1 + z_u,k z_v,k) / 2, 1e-4),
+//           A_s(u, v) = prod_{k in s} q_k (soft probability that the 8-bit keys agree);
+//           loss += -log(A_s(a, p) + 1e-6) + lambda * A_s(a, n).
+double orc_mlp_loss_grad(const float* w1, const float* b1, const float* w2, const float* b2, const uint8_t* a,
+                         const uint8_t* p, const uint8_t* ng, uint32_t batch, float margin, int kind, float lambda,
+                         double* dw1, double* db1, double* dw2, double* db2) {
     std::memset(dw1, 0, sizeof(double) * 256 * 128);
     std::memset(db1, 0, sizeof(double) * 256);
     std::memset(dw2, 0, sizeof(double) * 128 * 256);
@@ -74,8 +80,9 @@ double orc_mlp_triplet_grad(const float* w1, const float* b1, const float* w2, c
                 z[r * 128 + c] = std::tanh(s);
             }
         }
+        const int c0 = kind == 1 ? 48 : 0;  // first channel of the hinge term
         double dap = 0, dan = 0;
-        for (int c = 0; c < 128; ++c) {
+        for (int c = c0; c < 128; ++c) {
             const double u = z[c] - z[128 + c], v = z[c] - z[256 + c];
             dap += u * u / 4;
             dan += v * v / 4;
@@ -84,11 +91,31 @@ double orc_mlp_triplet_grad(const float* w1, const float* b1, const float* w2, c
         std::fill(dz.begin(), dz.end(), 0.0);
         if (l > 0) {
             loss += l;
-            for (int c = 0; c < 128; ++c) {
+            for (int c = c0; c < 128; ++c) {
                 const double u = z[c] - z[128 + c], v = z[c] - z[256 + c];
                 dz[c] = (u - v) / 2 / batch;
                 dz[128 + c] = -u / 2 / batch;
                 dz[256 + c] = v / 2 / batch;
+            }
+        }
+        if (kind == 1) {
+            for (int t = 0; t < 6; ++t) {
+                double aap = 1, aan = 1;
+                for (int k = 8 * t; k < 8 * t + 8; ++k) {
+                    aap *= std::max((1 + z[k] * z[128 + k]) / 2, 1e-4);
+                    aan *= std::max((1 + z[k] * z[256 + k]) / 2, 1e-4);
+                }
+                loss += -std::log(aap + 1e-6) + lambda * aan;
+                for (int k = 8 * t; k < 8 * t + 8; ++k) {
+                    const double qap = std::max((1 + z[k] * z[128 + k]) / 2, 1e-4);
+                    const double qan = std::max((1 + z[k] * z[256 + k]) / 2, 1e-4);
+                    // d q / d z_u = z_v / 2 where q is not clamped
+                    const double cap = (1 + z[k] * z[128 + k]) / 2 > 1e-4 ? -(aap / (aap + 1e-6)) / qap * 0.5 : 0.0;
+                    const double can = (1 + z[k] * z[256 + k]) / 2 > 1e-4 ? lambda * aan / qan * 0.5 : 0.0;
+                    dz[k] += (cap * z[128 + k] + can * z[256 + k]) / batch;
+                    dz[128 + k] += cap * z[k] / batch;
+                    dz[256 + k] += can * z[k] / batch;
+                }
             }
         }
         for (int r = 0; r < 3; ++r) {
@@ -107,6 +134,12 @@ double orc_mlp_triplet_grad(const float* w1, const float* b1, const float* w2, c
         }
     }
     return loss / batch;
+}
+
+double orc_mlp_triplet_grad(const float* w1, const float* b1, const float* w2, const float* b2, const uint8_t* a,
+                            const uint8_t* p, const uint8_t* ng, uint32_t batch, float margin, double* dw1,
+                            double* db1, double* dw2, double* db2) {
+    return orc_mlp_loss_grad(w1, b1, w2, b2, a, p, ng, batch, margin, 0, 0.f, dw1, db1, dw2, db2);
 }
 
 }  // extern "C"

@@ -144,6 +144,7 @@ SIGNATURES = {
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_mlp_trainer_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_float,
                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "rsfm_mlp_trainer_set_loss": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]),
     "rsfm_mlp_trainer_model": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MLP)]),
     "rsfm_mlp_trainer_step": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_void_p,
                                                                                         ctypes.c_void_p]),

@@ -260,16 +260,22 @@ __global__ void bias_relu_kernel(float* __restrict__ hpre, const float* __restri
     }
 }
 
-// z = tanh(o + b2); triplet loss and dO = dL/do for rows [a | p | n] (B each).
+// z = tanh(o + b2); loss and dO = dL/do for rows [a | p | n] (B each), one block of 128 threads
+// (= channels) per triplet.
+//   kind 0: hinge  max(0, margin + D(a,p) - D(a,n)),  D(u,v) = sum_c (z_u,c - z_v,c)^2 / 4.
+//   kind 1: the same hinge over channels 48..127 only, plus, per 8-bit bucket table t < 6
+//           (channels 8t..8t+7), -log(A_t(a,p) + 1e-6) + lambda * A_t(a,n) with
+//           A_t(u,v) = prod_k max((1 + z_u,k z_v,k) / 2, 1e-4).
 __global__ void triplet_kernel(const float* __restrict__ o, const float* __restrict__ b2, float* __restrict__ dO,
-                               uint32_t B, float margin, float* __restrict__ lossSum) {
-    const uint32_t b = blockIdx.x;  // one block (128 threads = channels) per triplet
+                               uint32_t B, float margin, int kind, float lambda, float* __restrict__ lossSum) {
+    const uint32_t b = blockIdx.x;
     const uint32_t c = threadIdx.x;
     __shared__ float red[2][4];
     const float za = tanhf(o[size_t(b) * 128 + c] + b2[c]);
     const float zp = tanhf(o[size_t(B + b) * 128 + c] + b2[c]);
     const float zn = tanhf(o[size_t(2 * B + b) * 128 + c] + b2[c]);
-    const float u = za - zp, v = za - zn;
+    const bool keyCh = kind == 1 && c < 48;
+    const float u = keyCh ? 0.f : za - zp, v = keyCh ? 0.f : za - zn;
     float dap = u * u * 0.25f, dan = v * v * 0.25f;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -284,9 +290,30 @@ __global__ void triplet_kernel(const float* __restrict__ o, const float* __restr
     const float l = margin + (red[0][0] + red[0][1] + red[0][2] + red[0][3]) - (red[1][0] + red[1][1] + red[1][2] + red[1][3]);
     const bool active = l > 0.f;
     const float inv = 1.f / float(B);
-    dO[size_t(b) * 128 + c] = active ? (u - v) * 0.5f * inv * (1.f - za * za) : 0.f;
-    dO[size_t(B + b) * 128 + c] = active ? -u * 0.5f * inv * (1.f - zp * zp) : 0.f;
-    dO[size_t(2 * B + b) * 128 + c] = active ? v * 0.5f * inv * (1.f - zn * zn) : 0.f;
+    float ga = active ? (u - v) * 0.5f : 0.f, gp = active ? -u * 0.5f : 0.f, gn = active ? v * 0.5f : 0.f;
+    float lossKey = 0.f;
+    if (kind == 1 && c < 64) {  // whole warps 0 and 1 take part in the table products
+        const float rap = 0.5f * (1.f + za * zp), ran = 0.5f * (1.f + za * zn);
+        const float qap = fmaxf(rap, 1e-4f), qan = fmaxf(ran, 1e-4f);
+        float aap = keyCh ? qap : 1.f, aan = keyCh ? qan : 1.f;
+#pragma unroll
+        for (int s = 1; s < 8; s <<= 1) {  // product over the 8 lanes of a table
+            aap *= __shfl_xor_sync(0xffffffffu, aap, s);
+            aan *= __shfl_xor_sync(0xffffffffu, aan, s);
+        }
+        if (keyCh) {
+            const float cap = rap > 1e-4f ? -(aap / (aap + 1e-6f)) / qap * 0.5f : 0.f;
+            const float can = ran > 1e-4f ? lambda * aan / qan * 0.5f : 0.f;
+            ga += cap * zp + can * zn;
+            gp += cap * za;
+            gn += can * za;
+            if ((c & 7u) == 0) lossKey = -logf(aap + 1e-6f) + lambda * aan;
+        }
+    }
+    dO[size_t(b) * 128 + c] = ga * inv * (1.f - za * za);
+    dO[size_t(B + b) * 128 + c] = gp * inv * (1.f - zp * zp);
+    dO[size_t(2 * B + b) * 128 + c] = gn * inv * (1.f - zn * zn);
+    if (lossKey != 0.f) atomicAdd(lossSum, lossKey * inv);
     if (c == 0 && active) atomicAdd(lossSum, l * inv);
 }
 
@@ -363,6 +390,8 @@ using namespace rsfm_b200;
 struct rsfm_mlp_trainer {
     uint32_t batch = 0;
     float margin = 16.f, lr = 1e-3f;
+    int kind = 0;        // loss: 0 = triplet hinge, 1 = bucket-key loss + hinge on the code channels
+    float lambda = 0.f;  // weight of the negatives' key agreement (kind 1)
     uint32_t step = 0;
     rsfm_mlp model{};
     // fp32 masters, Adam moments, gradients
@@ -444,6 +473,13 @@ extern "C" int rsfm_mlp_trainer_create(const float* initParams, uint32_t batch, 
     return RSFM_OK;
 }
 
+extern "C" int rsfm_mlp_trainer_set_loss(rsfm_mlp_trainer* t, int kind, float lambda) {
+    if (!t || (kind != 0 && kind != 1) || !(lambda >= 0.f)) return RSFM_ERR_INVALID_ARG;
+    t->kind = kind;
+    t->lambda = lambda;
+    return RSFM_OK;
+}
+
 extern "C" int rsfm_mlp_trainer_model(const rsfm_mlp_trainer* t, rsfm_mlp* model) {
     if (!t || !model) return RSFM_ERR_INVALID_ARG;
     *model = t->model;
@@ -468,7 +504,7 @@ static int trainer_grads(rsfm_mlp_trainer* t, const void* a, const uint32_t* ia,
     // o = h W2^T
     st = gemm(s, R, 128, 256, t->h, kBF16, 256, 1, t->model.w2, kBF16, 1, 256, t->o, 128, 1, 1.f, 1);
     if (st) return st;
-    triplet_kernel<<<B, 128, 0, s>>>(t->o, t->model.b2, t->dO, B, t->margin, t->loss);
+    triplet_kernel<<<B, 128, 0, s>>>(t->o, t->model.b2, t->dO, B, t->margin, t->kind, t->lambda, t->loss);
     // dW2 = dO^T h ; db2 = sum dO
     float* gW1 = t->g;
     float* gB1 = t->g + kNW1;

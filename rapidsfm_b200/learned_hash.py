@@ -73,7 +73,7 @@ class LearnedHash:
 class Trainer:
     """GPU triplet trainer (rsfm_mlp_trainer_*): fp32 masters + Adam, bf16 copies for inference."""
 
-    def __init__(self, params, batch, lr=1e-3, margin=0.5):
+    def __init__(self, params, batch, lr=1e-3, margin=0.5, loss="triplet", lam=16.0):
         lib = _lib.load()
         p = np.ascontiguousarray(params, dtype=np.float32)
         if p.size != NPARAMS:
@@ -82,6 +82,10 @@ class Trainer:
         self._h = ctypes.c_void_p(0)
         _lib.check(lib.rsfm_mlp_trainer_create(p.ctypes.data, batch, lr, margin, ctypes.byref(self._h)),
                    "rsfm_mlp_trainer_create")
+        if loss not in ("triplet", "bucket"):
+            raise ValueError("loss must be 'triplet' or 'bucket'")
+        _lib.check(lib.rsfm_mlp_trainer_set_loss(self._h, 1 if loss == "bucket" else 0, lam),
+                   "rsfm_mlp_trainer_set_loss")
         self.loss = torch.zeros(1, dtype=torch.float32, device="cuda")
 
     @staticmethod
@@ -157,7 +161,7 @@ def default_params_path():
 
 
 def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3, margin=48.0, seed=0,
-                           device="cuda", log=None):
+                           device="cuda", log=None, loss="triplet", lam=16.0):
     """Trains the learned hash on correspondences the brute-force matcher produces (ratio test and
     cross-check passed) on `n_pairs` seeded synthetic pairs (40% overlap, noise 8); negatives are
     random train descriptors of the same pair. Returns the f32 parameter block."""
@@ -175,7 +179,7 @@ def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3
     Q, T = torch.cat(qs), torch.cat(ts)
     A, P = torch.cat(A), torch.cat(P)
     params = center_output_bias(init_params(seed), lambda p: LearnedHash(p, device=device), Q[:20000])
-    tr = Trainer(params, batch, lr=lr, margin=margin)
+    tr = Trainer(params, batch, lr=lr, margin=margin, loss=loss, lam=lam)
     for s in range(steps):
         sel = torch.randint(0, len(A), (batch,), device=device, generator=g)
         ip = P[sel].int()
@@ -197,8 +201,11 @@ if __name__ == "__main__":
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--margin", type=float, default=48.0)
+    ap.add_argument("--loss", default="triplet", choices=["triplet", "bucket"])
+    ap.add_argument("--lam", type=float, default=16.0)
     a = ap.parse_args()
-    p = train_from_brute_force(a.pairs, steps=a.steps, batch=a.batch, margin=a.margin, log=print)
+    p = train_from_brute_force(a.pairs, steps=a.steps, batch=a.batch, margin=a.margin, log=print, loss=a.loss,
+                               lam=a.lam)
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     np.save(a.out, p)
     print("saved", a.out)

@@ -49,7 +49,8 @@ def test_hash_matches_oracle(rsfm, oracle, n):
     np.testing.assert_array_equal(keys.cpu().numpy(), codes.cpu().numpy().view(np.uint8)[:, :8])
 
 
-def test_trainer_gradients_match_oracle(rsfm, oracle):
+@pytest.mark.parametrize("loss,lam", [("triplet", 0.0), ("bucket", 4.0)])
+def test_trainer_gradients_match_oracle(rsfm, oracle, loss, lam):
     from rapidsfm_b200 import learned_hash as lh
     B = 96
     q, t, truth = synth.make_pair(2000, 2000, 0.6, 8.0, seed=5)
@@ -60,11 +61,11 @@ def test_trainer_gradients_match_oracle(rsfm, oracle):
     inn = rng.integers(0, len(t), B).astype(np.int32)
     p = _params(7)
     margin = 8.0
-    tr = lh.Trainer(p, B, lr=1e-3, margin=margin)
+    tr = lh.Trainer(p, B, lr=1e-3, margin=margin, loss=loss, lam=lam)
     dq, dt = _dev(q), _dev(t)
-    loss, g = tr.gradients(dq, _dev(ia), dt, _dev(ip), dt, _dev(inn))
-    eloss, eg = oracle.mlp_triplet_grad(p, q[ia], t[ip], t[inn], margin)
-    assert abs(loss - eloss) <= 1e-3 * (1 + abs(eloss))
+    got_loss, g = tr.gradients(dq, _dev(ia), dt, _dev(ip), dt, _dev(inn))
+    eloss, eg = oracle.mlp_triplet_grad(p, q[ia], t[ip], t[inn], margin, kind=1 if loss == "bucket" else 0, lam=lam)
+    assert abs(got_loss - eloss) <= 1e-3 * (1 + abs(eloss))
     for got, want in zip(lh.split(g), lh.split(eg)):
         rel = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-12)
         assert rel <= 5e-3, rel
