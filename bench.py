@@ -15,6 +15,7 @@ its kernel tests (test/bruteForceMatchKernelTest.cpp:140-164), restated in oracl
 the host cores (all threads) on a bounded row sample of the same workload.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -114,6 +115,18 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def max_over_ranks(value, device="cpu"):
+    """Largest value over all ranks of the default process group (the job's step time is its
+    slowest rank's); the value itself when running alone."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_baseline(q, t, rows, threads, min_seconds=0.0):
@@ -252,9 +265,7 @@ def run_ours(args):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     if ws > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(tt.item())
+        total_ms = max_over_ranks(total_ms, dev)
         torch.distributed.barrier()
     clocks = sampler.stop() if sampler else None
     ms_per_step = total_ms / args.steps
@@ -289,9 +300,7 @@ def run_ours(args):
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_step = statistics.mean(e2e_ms)
     if ws > 1:
-        tt = torch.tensor([e2e_step], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_step = float(tt.item())
+        e2e_step = max_over_ranks(e2e_step, dev)
     e2e_value = ws * N_QUERY * N_TRAIN / (e2e_step * 1e-3)
 
     if rank != 0:
@@ -335,9 +344,10 @@ def run_ours(args):
     rows, (cpu_val, cpu_dt) = _cpu_sample(q, t, threads, 10.0)
 
     extras = {}
-    if not args.no_extras:
+    if not args.no_extras and ws == 1:  # single-GPU sections; scaling runs time the pair only
         extras["batched"] = run_batched(dev, stream)
         extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
+        extras["hash"] = run_hash(dev, stream)
 
     line = {
         "metric": METRIC,
@@ -470,6 +480,65 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
         ok = [v for v in out["learned"]["tables"].values() if v["recall"] >= p6["recall"]]
         out["learned_speedup_at_plain_recall"] = (p6["match_ms"] / min(v["match_ms"] for v in ok)) if ok else None
     return out
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return {}
+
+
+def run_hash(dev, stream, n=1 << 24):
+    """Hashing throughput on n descriptors (2 GiB, far above L2): cascade hash (192 channels,
+    fused histogram; algorithmic bytes n*(128+8+16)), descriptor accumulation (n*128 bytes) and the
+    learned hash (131072 bf16 FLOP per descriptor), against the measured HBM and bf16 peaks."""
+    import torch
+    from rapidsfm_b200 import cashash as ch
+    from rapidsfm_b200 import learned_hash as lh
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    desc = torch.randint(0, 256, (n, 128), dtype=torch.uint8, device=dev, generator=g)
+    cas = ch.CasHash(ch.gaussian_weights(4))
+    cas.fit(desc[: 1 << 20])
+    keys = torch.empty((n, 8), dtype=torch.uint8, device=dev)
+    codes = torch.empty((n, 4), dtype=torch.int32, device=dev)
+    hist = torch.empty((8, 256), dtype=torch.int32, device=dev)
+    lib = R_lib()
+    p = ch._p
+
+    def hash_call():
+        lib.rsfm_cashash_compute_hash(p(cas.w), p(cas.bias), 192, p(desc), n, p(keys), p(codes), p(hist),
+                                      ctypes.c_void_p(stream.cuda_stream))
+
+    def acc_call():
+        lib.rsfm_cashash_accumulate_desc(p(cas.acc), 1, p(desc), n, ctypes.c_void_p(stream.cuda_stream))
+
+    peaks = _peaks()
+    hbm = peaks.get("hbm_gbs")
+    bf16 = peaks.get("bf16_tflops")
+    out = {"n_desc": n}
+    ms = _events_ms(hash_call, 5, stream)
+    gbs = n * (128 + 8 + 16) / (ms * 1e-3) / 1e9
+    out["cashash_hash"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None}
+    ms = _events_ms(acc_call, 5, stream)
+    gbs = n * 128 / (ms * 1e-3) / 1e9
+    out["cashash_accumulate"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None}
+    wpath = lh.default_params_path()
+    if os.path.exists(wpath):
+        h = lh.LearnedHash(np.load(wpath))
+        ms = _events_ms(lambda: h.hash(desc, keys=keys, codes=codes, stream=stream), 5, stream)
+        tf = n * 131072.0 / (ms * 1e-3) / 1e12
+        gbs = n * (128 + 8 + 16) / (ms * 1e-3) / 1e9
+        out["learned_hash"] = {"ms": ms, "TFLOP/s": tf, "frac_of_measured_bf16": tf / bf16 if bf16 else None,
+                               "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None}
+    return out
+
+
+def R_lib():
+    from rapidsfm_b200 import _lib
+    return _lib.load()
 
 
 def main():

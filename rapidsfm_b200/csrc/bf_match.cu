@@ -228,12 +228,13 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         // ------------------------------------------------------------ UMMA issuer
         if (elect_one()) {
             const uint32_t idesc = idesc_u8u8_s32(128, 128);
+            const uint64_t aDesc0 = umma_desc_k_sw128(smem_u32(S.a[0]));
             uint32_t aUse = 0, stage = 0, bPhase = 0, acc = 0;
             for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x) {
                 const Unit U = decode_unit(P, u);
                 for (uint32_t b = 0; b < U.cb; ++b) {
                     mbar_wait(&S.bFull[stage], bPhase, err, kDevTimeoutTmaFull);
-                    const uint32_t bAddr = smem_u32(S.b[stage]);
+                    const uint64_t bDesc = umma_desc_k_sw128(smem_u32(S.b[stage]));
                     for (uint32_t p = 0; p < U.pt; ++p) {
                         if (b == 0) {
                             mbar_wait(&S.aFull[p], (aUse >> p) & 1u, err, kDevTimeoutTmaFull);
@@ -242,11 +243,12 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                         const uint32_t buf = acc % kAccBufs;
                         mbar_wait(&S.accEmpty[buf], ((acc / kAccBufs) & 1u) ^ 1u, err, kDevTimeoutAccEmpty);
                         tc_fence_after();
-                        const uint32_t aAddr = smem_u32(S.a[p]);
+                        // K step k = +32 bytes = +2 in the descriptor's start-address field (the
+                        // tiles sit below 256 KB, so the 14-bit field cannot carry).
+                        const uint64_t aDesc = aDesc0 + uint64_t(p) * (kTileBytes >> 4);
                         const uint32_t d = tmem + buf * 128u;
 #pragma unroll
-                        for (uint32_t k = 0; k < 4; ++k)
-                            umma_i8(d, umma_desc_k_sw128(aAddr + 32u * k), umma_desc_k_sw128(bAddr + 32u * k), idesc, k);
+                        for (uint32_t k = 0; k < 4; ++k) umma_i8(d, aDesc + 2u * k, bDesc + 2u * k, idesc, k);
                         umma_commit(&S.accFull[buf]);
                         if (b + 1 == U.cb) umma_commit(&S.aEmpty[p]);
                         ++acc;

@@ -1,8 +1,9 @@
 // Thin inline-PTX layer for the sm_100a features the matcher kernels use:
 // mbarriers, TMA tensor loads, tcgen05 (TMEM allocation, int8 UMMA, TMEM loads/stores).
 //
-// Every wait on an mbarrier is bounded: after kSpinLimit polls it records an error code in
-// the caller-supplied flag word and returns false, so a kernel can give up instead of hanging.
+// Every wait on an mbarrier is bounded: after kWaitLimitNs of wall time (or kSpinLimit polls) it
+// records an error code in the caller-supplied flag word and returns false, so a kernel can give
+// up instead of hanging.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -10,8 +11,10 @@
 namespace rsfm_b200 {
 namespace sm100 {
 
-// A poll costs ~100 ns with the nanosleep back-off below; 2^24 polls is well over a second.
+// A poll suspends for up to 1 us in hardware (try_wait suspend-time hint); the wall-time limit
+// ends a wait first.
 constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
 enum DeviceError : uint32_t {
     kDevOk = 0,
@@ -68,12 +71,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // Bounded wait for the phase with the given parity to complete. On timeout, records `code` in
 // *err (first error wins) and returns false.
+// try_wait with a suspend-time hint: the thread sleeps in hardware (up to `ns`) until the phase
+// completes, instead of spinning through instruction issue.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for the phase with the given parity to complete: gives up after kWaitLimitNs of
+// wall time (or kSpinLimit polls), records `code` in *err (first error wins) and returns false.
+// Returns early without waiting when another wait has already recorded an error.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err, uint32_t code) {
     if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
     for (uint32_t i = 0; i < kSpinLimit; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (i > 512) __nanosleep(32);
-        if ((i & 1023u) == 0 && *reinterpret_cast<volatile uint32_t*>(err) != 0u) return false;
+        if (mbar_try_wait_hint(bar, parity, 1000u)) return true;
+        if ((i & 63u) == 63u) {
+            if (*reinterpret_cast<volatile uint32_t*>(err) != 0u) return false;
+            if (global_ns() - t0 > kWaitLimitNs) break;
+        }
     }
     atomicCAS(err, 0u, code);
     return false;
