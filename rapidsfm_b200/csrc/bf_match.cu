@@ -121,10 +121,12 @@ struct Smem {
     unsigned long long colmin[2][128];   // [block parity][column]: merge of the 4 lane quarters
     // Row state of the current unit, per unit row r = 128 p + 32 q + lane:
     int32_t rowc[kUnitRows];             // column-key addend ((7-p) << 5 | (31-lane)) - |a|^2 * 256
-    int32_t hint[kUnitRows];             // -(global best distance at unit start) * 256
-    int32_t l1k[kWG][kUnitRows];         // per warpgroup: best row key, second row key
+    // Per warpgroup: tk = trigger threshold in row-key space (set from the global best at unit
+    // start, tie-inclusive; after the warpgroup's own best d1 it is -(d1 - 1) * 256 + c, i.e.
+    // strictly better); l2k = second key; l1j = column of the own best (0xFFFF: none yet).
+    int32_t tk[kWG][kUnitRows];
     int32_t l2k[kWG][kUnitRows];
-    uint16_t l1j[kWG][kUnitRows];        // column of the best key, relative to the unit's first column
+    uint16_t l1j[kWG][kUnitRows];
     uint64_t aFull[kMaxRowTiles], aEmpty[kMaxRowTiles];
     uint64_t bFull[Cfg<kWG>::kBStages], bEmpty[Cfg<kWG>::kBStages];
     uint64_t accFull[kAccBufs], accEmpty[kAccBufs];
@@ -272,12 +274,12 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         // no repacking. Within one thread and tile c is constant and c + (31 - k) < 287, so row
         // keys of one chunk order by (d, k); u = rk - c = -d * 256 + (31 - k) decodes both.
         //
-        // Row state lives in shared memory, per warpgroup and unit row: l1k = best row key,
-        // l1j = its column, l2k = max over the other keys that can matter for the second-best.
-        // A chunk does extra work only if its maximum beats this warpgroup's best AND can still
-        // tie or beat the global best known at unit start (hint); every other chunk contributes
-        // its maximum to l2k only. This is exact: a chunk that cannot hold the best holds at most
-        // one value that matters, its maximum.
+        // Row state lives in shared memory, per warpgroup and unit row: tk = trigger threshold,
+        // l1j = column of the own best, l2k = max over the other keys that can matter for the
+        // second-best. A chunk does extra work only if its maximum reaches tk: it beats this
+        // warpgroup's best AND can still tie or beat the global best known at unit start; every
+        // other chunk contributes its maximum to l2k only. This is exact: a chunk that cannot
+        // hold the best holds at most one value that matters, its maximum.
         const uint32_t e = warp - 2u;                    // epilogue warp
         const uint32_t wg = e >> 2;                      // warpgroup: columns [32 kCPW wg, +32 kCPW)
         const uint32_t q = warp & 3u;                    // TMEM lane quarter
@@ -314,10 +316,10 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 const uint32_t i = U.r0 + r;
                 const bool valid = p < U.pt && i < T.nA;
                 S.rowc[r] = valid ? int32_t(c - (na[it] << 8)) : int32_t(0x80000000u | c);
-                S.hint[r] = int32_t(0u - (min(h1[it], kMaxDist) << 8));
+                const int32_t t0 = valid ? int32_t((0u - (min(h1[it], kMaxDist) << 8)) + c) : INT32_MAX;
 #pragma unroll
                 for (int w = 0; w < kWG; ++w) {
-                    S.l1k[w][r] = INT32_MIN;
+                    S.tk[w][r] = t0;
                     S.l2k[w][r] = INT32_MIN;
                     S.l1j[w][r] = 0xFFFFu;
                 }
@@ -339,14 +341,9 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 for (uint32_t p = 0; p < U.pt; ++p) {
                     const uint32_t r = 128u * p + t128;
                     const int32_t rowcP = S.rowc[r];
-                    const uint32_t c = uint32_t(rowcP) & 255u;
-                    int32_t l1kP = S.l1k[wg][r], l2kP = S.l2k[wg][r];
-                    uint32_t l1jP = S.l1j[wg][r];
                     // Trigger threshold: strictly better than this warpgroup's best (its columns
                     // come in increasing order), and no worse than the global best.
-                    const int32_t own = l1kP == INT32_MIN ? INT32_MIN
-                                                          : int32_t((uint32_t(l1kP) - ((uint32_t(l1kP) - c) & 255u)) + 256u);
-                    int32_t tkP = (U.r0 + r < T.nA) ? max(own, int32_t(uint32_t(S.hint[r]) + c)) : INT32_MAX;
+                    int32_t tkP = S.tk[wg][r], l2kP = S.l2k[wg][r];
                     const uint32_t buf = acc % kAccBufs;
                     mbar_wait(&S.accFull[buf], (acc / kAccBufs) & 1u, err, kDevTimeoutAccFull);
                     tc_fence_after();
@@ -401,10 +398,13 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(rmax) - 1u - x[32 * cc + k]);
                             const int32_t s2 = int32_t(uint32_t(rmax) - 1u - mn);
                             if (rmax >= tkP) {
-                                l2kP = max(max(l2kP, l1kP), s2);
-                                l1kP = rmax;
-                                l1jP = (j0 - U.c0) + 31u - ((uint32_t(rmax) - c) & 255u);
-                                tkP = max(tkP, int32_t((uint32_t(rmax) - ((uint32_t(rmax) - c) & 255u)) + 256u));
+                                const uint32_t c = uint32_t(rowcP) & 255u;
+                                // the previous own best (key of distance d1: tk - 256) becomes a second
+                                if (S.l1j[wg][r] != 0xFFFFu) l2kP = max(l2kP, int32_t(uint32_t(tkP) - 256u));
+                                l2kP = max(l2kP, s2);
+                                S.l1j[wg][r] = uint16_t((j0 - U.c0) + 31u - ((uint32_t(rmax) - c) & 255u));
+                                tkP = int32_t((uint32_t(rmax) - ((uint32_t(rmax) - c) & 255u)) + 256u);
+                                S.tk[wg][r] = tkP;
                             } else {
                                 l2kP = max(l2kP, rmax);
                             }
@@ -412,9 +412,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             l2kP = max(l2kP, rmax);
                         }
                     }
-                    S.l1k[wg][r] = l1kP;
                     S.l2k[wg][r] = l2kP;
-                    S.l1j[wg][r] = uint16_t(l1jP);
                 }
                 // ---- column flush: best key per column over this warp's 32 lanes, then over the
                 // four lane quarters in shared memory, then one global atomic per column.
@@ -461,9 +459,9 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 uint32_t sec = ~0u;
 #pragma unroll
                 for (int w = 0; w < kWG; ++w) {
-                    const int32_t k1 = S.l1k[w][r], k2 = S.l2k[w][r];
-                    if (k1 != INT32_MIN) {
-                        const uint32_t d1 = 0u - uint32_t(int32_t(uint32_t(k1) - c) >> 8);
+                    const int32_t k2 = S.l2k[w][r];
+                    if (S.l1j[w][r] != 0xFFFFu) {  // tk = -(d1 - 1) * 256 + c
+                        const uint32_t d1 = 1u - uint32_t(int32_t(uint32_t(S.tk[w][r]) - c) >> 8);
                         const unsigned long long key =
                             (static_cast<unsigned long long>(d1) << 32) | (U.c0 + uint32_t(S.l1j[w][r]));
                         if (key < bst) {

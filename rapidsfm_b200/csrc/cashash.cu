@@ -77,13 +77,14 @@ __global__ void bias_kernel(int32_t* __restrict__ bias, const int8_t* __restrict
 // place (x >> 1 fits int8), one thread issues s8 x s8 UMMAs (M=128, N=channels, K=128) against
 // the weights (s8, loaded once per CTA), each thread reads its descriptor's channel sums from
 // its TMEM lane and packs the sign bits.
-constexpr int kHashThreads = 128;
+constexpr int kHashThreads = 256;  // two threads per TMEM lane: each takes half of the channel groups
+constexpr int kHashStages = 4;  // descriptor tiles in flight per CTA (two CTAs per SM)
 struct HashSmem {
-    uint8_t desc[2][128 * 128];
+    uint8_t desc[kHashStages][128 * 128];
     uint8_t w[192 * 128];
     int32_t bias[192];
     uint32_t hist[8][256];
-    uint64_t full[2];
+    uint64_t full[kHashStages];
     uint64_t mma;
     uint32_t tmem;
 };
@@ -103,8 +104,7 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
     for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) (&S.hist[0][0])[x] = 0;
     for (int c = tid; c < channels; c += kHashThreads) S.bias[c] = bias[c];
     if (tid == 0) {
-        mbar_init(&S.full[0], 1);
-        mbar_init(&S.full[1], 1);
+        for (int b = 0; b < kHashStages; ++b) mbar_init(&S.full[b], 1);
         mbar_init(&S.mma, 1);
         fence_mbar_init();
     }
@@ -121,31 +121,36 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
     if (tid == 0) {
         mbar_arrive_expect_tx(&S.mma, uint32_t(channels) * 128u);
         for (int r = 0; r < channels; r += 64) tma_load_2d(S.w + r * 128, &tmW, &S.mma, 0, r);
-        if (blockIdx.x < tiles) {
-            mbar_arrive_expect_tx(&S.full[0], 128u * 128u);
-            tma_load_2d(S.desc[0], &tmDesc, &S.full[0], 0, int32_t(blockIdx.x * 128u));
+        for (uint32_t k = 0; k + 1 < uint32_t(kHashStages); ++k) {
+            const uint32_t t = blockIdx.x + k * gridDim.x;
+            if (t < tiles) {
+                mbar_arrive_expect_tx(&S.full[k], 128u * 128u);
+                tma_load_2d(S.desc[k], &tmDesc, &S.full[k], 0, int32_t(t * 128u));
+            }
         }
     }
     mbar_wait(&S.mma, 0, err_, kDevTimeoutTmaFull);
     uint32_t it = 0, mmaPhase = 1;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-        const uint32_t buf = it & 1u;
-        // prefetch the next tile into the other buffer (its previous MMA has completed)
-        if (tid == 0 && tile + gridDim.x < tiles) {
-            mbar_arrive_expect_tx(&S.full[buf ^ 1u], 128u * 128u);
-            tma_load_2d(S.desc[buf ^ 1u], &tmDesc, &S.full[buf ^ 1u], 0, int32_t((tile + gridDim.x) * 128u));
+        const uint32_t buf = it % kHashStages;
+        // prefetch kHashStages-1 tiles ahead into the buffer the previous iteration has finished with
+        const uint32_t ahead = tile + (kHashStages - 1) * gridDim.x;
+        if (tid == 0 && ahead < tiles) {
+            const uint32_t nb = (it + kHashStages - 1) % kHashStages;
+            mbar_arrive_expect_tx(&S.full[nb], 128u * 128u);
+            tma_load_2d(S.desc[nb], &tmDesc, &S.full[nb], 0, int32_t(ahead * 128u));
         }
-        mbar_wait(&S.full[buf], (it >> 1) & 1u, err_, kDevTimeoutTmaFull);
+        mbar_wait(&S.full[buf], (it / kHashStages) & 1u, err_, kDevTimeoutTmaFull);
         // halve every byte in place: (x & 0xFE) >> 1
         uint4* d4 = reinterpret_cast<uint4*>(S.desc[buf]);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            uint4 v = d4[tid + 128 * k];
+        for (int k = 0; k < 1024 / kHashThreads; ++k) {
+            uint4 v = d4[tid + kHashThreads * k];
             v.x = (v.x & 0xFEFEFEFEu) >> 1;
             v.y = (v.y & 0xFEFEFEFEu) >> 1;
             v.z = (v.z & 0xFEFEFEFEu) >> 1;
             v.w = (v.w & 0xFEFEFEFEu) >> 1;
-            d4[tid + 128 * k] = v;
+            d4[tid + kHashThreads * k] = v;
         }
         fence_proxy_async_smem();
         __syncthreads();
@@ -162,24 +167,27 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
         mbar_wait(&S.mma, mmaPhase, err_, kDevTimeoutAccFull);
         mmaPhase ^= 1u;
         tc_fence_after();
-        const uint32_t i = tile * 128u + tid;  // descriptor of this thread's TMEM lane
-        uint32_t words[6];
-        for (int cw = 0; cw < channels / 32; ++cw) {
+        // Warp w reads TMEM lanes 32 (w % 4).. (its descriptors) and the 32-channel groups
+        // cw = half, half + 2, ... (half = w / 4): keys are groups 0-1, the remap code groups 2-5.
+        const uint32_t q = warp & 3u, half = warp >> 2;
+        const uint32_t i = tile * 128u + 32u * q + lane;
+        for (int cw = int(half); cw < channels / 32; cw += 2) {
             uint32_t v[32];
-            tmem_ld32(tmem + ((32u * warp) << 16) + 32u * cw, v);
+            tmem_ld32(tmem + ((32u * q) << 16) + 32u * cw, v);
             tmem_wait_ld();
             uint32_t bits = 0;
 #pragma unroll
             for (int k = 0; k < 32; ++k) bits |= (int32_t(v[k]) + S.bias[32 * cw + k] >= 0 ? 1u : 0u) << k;
-            words[cw] = bits;
-        }
-        if (i < n) {
-            *reinterpret_cast<uint2*>(keys + size_t(i) * 8) = make_uint2(words[0], words[1]);
-            if (remap && channels == 192)
-                *reinterpret_cast<uint4*>(remap + size_t(i) * 4) = make_uint4(words[2], words[3], words[4], words[5]);
-            if (histogram) {
+            if (i < n) {
+                if (cw < 2) {
+                    reinterpret_cast<uint32_t*>(keys + size_t(i) * 8)[cw] = bits;
+                    if (histogram) {
 #pragma unroll
-                for (int s = 0; s < 8; ++s) atomicAdd(&S.hist[s][(words[s >> 2] >> (8 * (s & 3))) & 0xFFu], 1u);
+                        for (int b = 0; b < 4; ++b) atomicAdd(&S.hist[4 * cw + b][(bits >> (8 * b)) & 0xFFu], 1u);
+                    }
+                } else if (remap) {
+                    remap[size_t(i) * 4 + (cw - 2)] = bits;
+                }
             }
         }
         tc_fence_before();
