@@ -347,7 +347,7 @@ def run_ours(args):
     if not args.no_extras and ws == 1:  # single-GPU sections; scaling runs time the pair only
         extras["batched"] = run_batched(dev, stream)
         extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
-        extras["hash"] = run_hash(dev, stream)
+        extras["hash"] = run_hash(dev, stream, n=1 << args.hash_log2)
 
     line = {
         "metric": METRIC,
@@ -550,7 +550,15 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="descriptors per side (smaller profiling cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and cascade-hash sections")
     ap.add_argument("--cascade-pairs", type=int, default=1000)
+    ap.add_argument("--only-hash", action="store_true", help="run the hashing-throughput section alone (profiling)")
+    ap.add_argument("--hash-log2", type=int, default=24, help="log2 of the descriptors in the hashing section")
     args = ap.parse_args()
+    if args.only_hash:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"hash": run_hash(dev, torch.cuda.current_stream(dev), n=1 << args.hash_log2)}), flush=True)
+        return
     if args.size:
         globals().update(N_QUERY=args.size, N_TRAIN=args.size, WORKLOAD=f"bf_pair_{args.size}x{args.size}")
     if args.impl == "reference":

@@ -175,9 +175,19 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
             uint32_t v[32];
             tmem_ld32(tmem + ((32u * q) << 16) + 32u * cw, v);
             tmem_wait_ld();
-            uint32_t bits = 0;
+            // sign bits of (sum + bias), shifted in from the top channel down: one funnel shift per
+            // channel; bit k = [sum_k + bias_k >= 0] after the final inversion
+            uint32_t neg = 0;
+            const int4* b4 = reinterpret_cast<const int4*>(&S.bias[32 * cw]);
 #pragma unroll
-            for (int k = 0; k < 32; ++k) bits |= (int32_t(v[k]) + S.bias[32 * cw + k] >= 0 ? 1u : 0u) << k;
+            for (int k4 = 7; k4 >= 0; --k4) {
+                const int4 bb = b4[k4];
+                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 3]) + bb.w), neg, 1);
+                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 2]) + bb.z), neg, 1);
+                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 1]) + bb.y), neg, 1);
+                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 0]) + bb.x), neg, 1);
+            }
+            const uint32_t bits = ~neg;
             if (i < n) {
                 if (cw < 2) {
                     reinterpret_cast<uint32_t*>(keys + size_t(i) * 8)[cw] = bits;

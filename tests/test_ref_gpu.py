@@ -100,3 +100,36 @@ def test_host_filters_match_reference(ref, rsfm):
     got = rsfm.remove_match_conflicts(fwd, nt)
     np.testing.assert_array_equal(got["idxQuery"], exp["q"])
     np.testing.assert_array_equal(got["idxTrain"], exp["t"])
+
+
+def test_faster_than_reference_kernels(ref, rsfm):
+    """The same-box bar: RapidSFM's own mma.sync matcher (built for sm_100a) against ours on a
+    16384 x 16384 SIFT-like pair, both through their launchers with the norms precomputed; CUDA
+    events on the default stream, 5 launches each after a warm-up. Results must agree."""
+    from rapidsfm_b200._lib import SiftBFTask
+    q, t, _ = synth.make_pair(16384, 16384, 0.5, 10.0, seed=12)
+    dA, dB = torch.from_numpy(q).cuda(), torch.from_numpy(t).cuda()
+    sA, sB = rsfm.precomp_sift_sqr_norm(dA), rsfm.precomp_sift_sqr_norm(dB)
+    outs = {}
+    times = {}
+    lib = rsfm._lib.load()
+    for name, fn in (("reference", ref.ref_bf_match_imma), ("rsfm_b200", lib.rsfm_bf_match)):
+        fwd = torch.empty(len(q), dtype=torch.int64, device="cuda")
+        bwd = torch.empty(len(t), dtype=torch.int64, device="cuda")
+        task = SiftBFTask(len(q), len(t), dA.data_ptr(), dB.data_ptr(), fwd.data_ptr(), bwd.data_ptr(),
+                          sA.data_ptr(), sB.data_ptr())
+        assert fn(ctypes.byref(task), 1, None) == 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            assert fn(ctypes.byref(task), 1, None) == 0
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / 5
+        outs[name] = (fwd.clone(), bwd.clone())
+    print({k: f"{v * 1e3:.0f} us" for k, v in times.items()},
+          f"speedup {times['reference'] / times['rsfm_b200']:.2f}x")
+    assert torch.equal(outs["reference"][0], outs["rsfm_b200"][0])
+    assert torch.equal(outs["reference"][1], outs["rsfm_b200"][1])
+    assert times["rsfm_b200"] < times["reference"]
