@@ -820,7 +820,12 @@ extern "C" int rsfm_bf_match(const rsfm_sift_bf_task* tasks, size_t nbTasks, cud
     size_t total = 0;
     for (size_t t = 0; t < nbTasks; ++t) total += tasks[t].nbDescA;
     uint32_t* scratch = nullptr;
-    if (total > 0) RSFM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), total * 4, stream));
+    if (total > 0) {
+        cudaMemPool_t pool = nullptr;
+        const int ps = scratch_pool(&pool);
+        if (ps != RSFM_OK) return ps;
+        RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), total * 4, pool, stream));
+    }
     std::vector<uint32_t*> second(nbTasks);
     size_t off = 0;
     for (size_t t = 0; t < nbTasks; ++t) {

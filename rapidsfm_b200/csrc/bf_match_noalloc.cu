@@ -1,9 +1,9 @@
 // Allocation-free variant of rsfm_bf_match (no reference counterpart).
 //
 // rsfm_bf_match needs one 32-bit second-best distance per query row while it runs (the row
-// thresholds of the fused top-2 epilogue), and takes that scratch from cudaMallocAsync. This entry
-// point takes it instead from a fixed file-scope device array, so a call allocates no device
-// memory at all: for callers that must not allocate (a scheduler thread that runs under a fixed
+// thresholds of the fused top-2 epilogue), and takes that scratch from a stream-ordered pool
+// allocation. This entry point takes it instead from a fixed file-scope device array, so a call
+// allocates no device memory at all: for callers that must not allocate (a scheduler thread that runs under a fixed
 // memory budget, or code that may not touch the allocator while other work is in flight).
 //
 // Limits and contract:

@@ -425,7 +425,10 @@ extern "C" int rsfm_cashash_build_buckets(const uint8_t* bucketIndices, uint32_t
     if (nbDesc == 0) return RSFM_OK;
     const uint32_t chunks = (nbDesc + ch::kChunk - 1) / ch::kChunk;
     uint32_t* scratch = nullptr;
-    RSFM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), size_t(chunks) * 2048 * 4, stream));
+    cudaMemPool_t pool = nullptr;
+    const int ps = scratch_pool(&pool);
+    if (ps != RSFM_OK) return ps;
+    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), size_t(chunks) * 2048 * 4, pool, stream));
     ch::chunk_hist_kernel<<<chunks, 256, 0, stream>>>(scratch, reinterpret_cast<const uint2*>(bucketIndices), nbDesc);
     ch::chunk_offsets_kernel<<<8, 256, 0, stream>>>(scratch, idxAllocator, chunks);
     ch::fill_kernel<<<chunks, 256, 0, stream>>>(bucketIndices, nbDesc, scratch, buckets);

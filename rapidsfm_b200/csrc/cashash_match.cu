@@ -291,7 +291,10 @@ static int find_best_match_impl(const rsfm_cashash_image* queries, const uint32_
     const bool bidir = results[0].train != nullptr;
     uint32_t* counter = nullptr;
     uint32_t* qSizes = nullptr;
-    RSFM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&counter), 4 + 4 * chm::kMaxTasks, stream));
+    cudaMemPool_t pool = nullptr;
+    const int ps = scratch_pool(&pool);
+    if (ps != RSFM_OK) return ps;
+    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&counter), 4 + 4 * chm::kMaxTasks, pool, stream));
     qSizes = counter + 1;
     static bool attr = false;
     const size_t smem = sizeof(chm::Smem) + 1024;

@@ -66,6 +66,31 @@ int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows) {
     return r == CUDA_SUCCESS ? RSFM_OK : RSFM_ERR_INVALID_ARG;
 }
 
+// Stream-ordered scratch comes from a pool of this library (one per device) that keeps its memory
+// between calls: the device's default pool returns freed memory to the system at every
+// synchronisation (release threshold 0), and mapping it again costs tens of microseconds a call.
+int scratch_pool(cudaMemPool_t* out) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    RSFM_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return RSFM_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        RSFM_CUDA_TRY(cudaMemPoolCreate(&p, &props));
+        uint64_t keep = ~0ull;
+        RSFM_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[dev] = p;
+    }
+    *out = pools[dev];
+    return RSFM_OK;
+}
+
 int sm_count() {
     int dev = 0, n = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;

@@ -36,6 +36,8 @@ int encode_desc_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint32_t
 int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows);
 
 int sm_count();
+// Stream-ordered scratch pool of this library on the current device (keeps its memory).
+int scratch_pool(cudaMemPool_t* pool);
 
 // Dominant-kernel event bracketing (see rsfm_profile_enable). profile_begin returns false when
 // profiling is off; otherwise the caller launches the kernel and then calls profile_end.
