@@ -42,13 +42,12 @@ __global__ void pack_kernel(const uint2* __restrict__ keys, const uint4* __restr
     }
 }
 
-// Bytes equal in a and b -> bit set per byte (4 bits for 4 bytes of each word).
-__device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
-    const uint32_t x = a ^ b;
-    uint32_t m = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) m |= ((x >> (8 * k)) & 0xFFu) == 0 ? (1u << k) : 0u;
-    return m;
+// True when any of the first s key bytes of t equals q's (bytes 0-3 in .x, 4-7 in .y): the
+// candidate was already found in an earlier table. __vcmpeq4 sets 0xFF per equal byte.
+__device__ __forceinline__ bool collides_before(uint2 t, uint2 q, uint32_t s) {
+    const uint32_t lo = s >= 4 ? 0xFFFFFFFFu : (1u << (8 * s)) - 1u;
+    const uint32_t hi = s <= 4 ? 0u : (1u << (8 * (s - 4))) - 1u;
+    return ((__vcmpeq4(t.x, q.x) & lo) | (__vcmpeq4(t.y, q.y) & hi)) != 0u;
 }
 
 struct Out {
@@ -213,8 +212,7 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
             bool keep = false;
             uint32_t key = 0;
             if (j != 0xFFFFFFFFu) {
-                const uint32_t eqm = eq_bytes(tk[u].x, qk.x) | (eq_bytes(tk[u].y, qk.y) << 4);
-                keep = (eqm & ((1u << ss[u]) - 1u)) == 0;  // first table where j collides
+                keep = !collides_before(tk[u], qk, ss[u]);  // first table where j collides
                 if (keep) {
                     const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
                                        __popc(tc[u].w ^ qc.w);
