@@ -62,8 +62,8 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
                                             uint32_t ratioNum, uint32_t ratioDen, const Out& O, uint32_t* B,
                                             uint32_t* TOP, uint32_t* H, uint32_t* C, uint32_t lane) {
     const uint32_t lt = (1u << lane) - 1u;
-    const uint2 qk = Q.keys[i];
-    const uint4 qc = Q.codes[i];
+    const uint2 qk = __ldg(&Q.keys[i]);
+    const uint4 qc = __ldg(&Q.codes[i]);
     uint32_t cnt = 0, nTop = 0, total = 0;
 
     // Extract the topK smallest keys of buffer + running top into TOP (ascending). Keys are
@@ -159,8 +159,8 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
     uint32_t myLo = 0, mySize = 0;
     if (lane < tables) {
         const uint32_t bk = lane < 4 ? (qk.x >> (8 * lane)) & 0xFFu : (qk.y >> (8 * (lane - 4))) & 0xFFu;
-        myLo = bk ? T.ends[lane * 256 + bk - 1] : 0u;
-        mySize = T.ends[lane * 256 + bk] - myLo;
+        myLo = bk ? __ldg(&T.ends[lane * 256 + bk - 1]) : 0u;
+        mySize = __ldg(&T.ends[lane * 256 + bk]) - myLo;
     }
     uint32_t incl = mySize;  // inclusive prefix of list sizes over the tables
 #pragma unroll
@@ -187,7 +187,7 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
             const uint32_t begin = __shfl_sync(0xffffffffu, incl - mySize, s);
             const uint32_t lo = __shfl_sync(0xffffffffu, myLo, s);  // lane s holds table s's range
             ss[u] = s;
-            jj[u] = x < all ? T.buckets[size_t(s) * T.n + lo + (x - begin)] : 0xFFFFFFFFu;
+            jj[u] = x < all ? __ldg(&T.buckets[size_t(s) * T.n + lo + (x - begin)]) : 0xFFFFFFFFu;
         }
         uint2 tk[kU];
         uint4 tc[kU];
@@ -198,12 +198,12 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
                 tk[u] = make_uint2(0, 0);
                 tc[u] = make_uint4(0, 0, 0, 0);
             } else if (T.rec) {
-                const uint4 r0 = T.rec[2 * size_t(j)], r1 = T.rec[2 * size_t(j) + 1];
+                const uint4 r0 = __ldg(&T.rec[2 * size_t(j)]), r1 = __ldg(&T.rec[2 * size_t(j) + 1]);
                 tk[u] = make_uint2(r0.x, r0.y);
                 tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
             } else {
-                tk[u] = T.keys[j];
-                tc[u] = T.codes[j];
+                tk[u] = __ldg(&T.keys[j]);
+                tc[u] = __ldg(&T.codes[j]);
             }
         }
 #pragma unroll
@@ -229,8 +229,8 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
     }
     select();
     // Exact L2 on the ranked candidates: lane l handles bytes [4l, 4l+4).
-    const uint32_t qw = reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128)[lane];
-    const uint32_t nq = Q.sqr[i];
+    const uint32_t qw = __ldg(reinterpret_cast<const uint32_t*>(Q.desc + size_t(i) * 128) + lane);
+    const uint32_t nq = __ldg(&Q.sqr[i]);
     uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
     // Candidates in groups of 8: all their loads first, then the dot products.
     for (uint32_t r0 = 0; r0 < nTop; r0 += 8) {
@@ -241,22 +241,37 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
             tw[k] = 0;
             ns[k] = 0;
             if (jr[k] != 0xFFFFFFFFu) {
-                tw[k] = reinterpret_cast<const uint32_t*>(T.desc + size_t(jr[k]) * 128)[lane];
-                ns[k] = T.rec ? T.rec[2 * size_t(jr[k]) + 1].z : T.sqr[jr[k]];
+                tw[k] = __ldg(reinterpret_cast<const uint32_t*>(T.desc + size_t(jr[k]) * 128) + lane);
+                ns[k] = T.rec ? __ldg(&T.rec[2 * size_t(jr[k]) + 1].z) : __ldg(&T.sqr[jr[k]]);
             }
         }
         uint32_t dot[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) dot[k] = __dp4a(qw, tw[k], 0u);
+        // Sum over the 32 lanes of all 8 partial dots at once: three halving levels (lane bits 4, 3,
+        // 2 choose which candidates a lane keeps), then two plain levels; afterwards lane l holds the
+        // dot of candidate ((l >> 2) & 7) bit-reversed over bits 4..2, read back by one shuffle each.
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+        for (int lvl = 0; lvl < 3; ++lvl) {
+            const int half = 4 >> lvl, o = 16 >> lvl;
+            const bool up = (lane & uint32_t(o)) != 0u;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) dot[k] += __shfl_xor_sync(0xffffffffu, dot[k], o);
+            for (int k = 0; k < half; ++k) {
+                const uint32_t lo = dot[k], hi = dot[k + half];
+                dot[k] = (up ? hi : lo) + __shfl_xor_sync(0xffffffffu, up ? lo : hi, o);
+            }
+        }
+        dot[0] += __shfl_xor_sync(0xffffffffu, dot[0], 2);
+        dot[0] += __shfl_xor_sync(0xffffffffu, dot[0], 1);
+        uint32_t dots[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)  // candidate k sits in lanes with bit4 = k>>2, bit3 = (k>>1)&1, bit2 = k&1
+            dots[k] = __shfl_sync(0xffffffffu, dot[0], (((k >> 2) & 1) << 4) | (((k >> 1) & 1) << 3) | ((k & 1) << 2));
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const uint32_t j = jr[k];
             if (j == 0xFFFFFFFFu) continue;
-            const uint32_t d = nq + ns[k] - 2u * dot[k];
+            const uint32_t d = nq + ns[k] - 2u * dots[k];
             if (d < bd || (d == bd && j < bj)) {
                 sd = bd;
                 bd = d;
