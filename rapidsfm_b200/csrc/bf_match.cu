@@ -354,8 +354,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                                   *reinterpret_cast<uint32_t(*)[32]>(&x[32 * cc]));
                     tmem_wait_ld();
                     // The accumulator is in registers now: hand the TMEM buffer back to the MMA.
-                    tc_fence_before();
-                    __syncwarp();
+                    tc_fence_before();  // (tcgen05.ld and its wait are warp-collective: the warp is converged)
                     if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
                     ++acc;
 #pragma unroll
