@@ -531,6 +531,19 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
         ok98 = [int(k) for k, v in rows.items() if v["recall"] >= 0.98]
         out[name] = {"tables": rows, "hash_and_buckets_host_s": hash_s,
                      "fewest_tables_at_98pct_recall": min(ok98) if ok98 else None}
+        if name == "plain":
+            # reference mode (cashash::findBestMatch): all 8 schemes, exact L2 over every descriptor
+            # pair sharing a bucket, per-scheme bucket lists; one call per pair
+            fbm = lambda: [ch.find_best_match([qi], ti, stream=stream) for qi, ti in ranked]
+            ms = _events_ms(fbm, 2, stream)
+            res = fbm()
+            hit = torch.zeros((), dtype=torch.int64, device=dev)
+            tot = torch.zeros((), dtype=torch.int64, device=dev)
+            for (ok, gt), ((bq, _),) in zip(truth, res):
+                hit += (((bq & 0xFFFFFFFF) == gt) & ok).sum()
+                tot += ok.sum()
+            out["find_best_match_8_schemes"] = {"ms": ms, "recall": int(hit) / max(1, int(tot)),
+                                                "desc_pairs_per_s": pairs / (ms * 1e-3)}
     if "learned" in out:
         p6 = out["plain"]["tables"]["6"]
         ok = [v for v in out["learned"]["tables"].values() if v["recall"] >= p6["recall"]]

@@ -222,3 +222,30 @@ class CascadeMatcher:
                 out[k] = (t.bestA, t.secondA, t.flagsA & 1)
         self.fallback_pairs = brute
         return out
+
+
+def find_best_match(queries, train, per_scheme_lists=True, max_bucket_sizes=None, stream=None):
+    """cashash::findBestMatch (cascadeHash.h:106-107) over RankedImages: every (query, train)
+    descriptor pair sharing a bucket in any of the 8 schemes is scored by exact L2; returns per query
+    image (best int64 [nq] for its descriptors, best int64 [nt] for the train descriptors). With
+    per_scheme_lists=False the bucket lists are read exactly as the reference reads them (without
+    the per-scheme offset, rsfm_cashash_find_best_match); the default reads each scheme's own lists."""
+    lib = _lib.load()
+    n = len(queries)
+    outs = [(torch.empty(q.n, dtype=torch.int64, device=q.desc.device),
+             torch.empty(train.n, dtype=torch.int64, device=q.desc.device)) for q in queries]
+    def ci(img):
+        return _lib.CasHashImage(img.desc.data_ptr(), img.upper.data_ptr(), img.buckets.data_ptr(), img.sqr.data_ptr())
+    qi = (_lib.CasHashImage * n)(*[ci(q) for q in queries])
+    ti = ci(train)
+    rr = (_lib.CasHashResult * n)(*[_lib.CasHashResult(a.data_ptr(), b.data_ptr()) for a, b in outs])
+    qs = (ctypes.c_uint32 * n)(*[q.n for q in queries])
+    if per_scheme_lists:
+        _lib.check(lib.rsfm_cashash_find_best_match_ex(qi, qs, ctypes.byref(ti), train.n, rr, n, 1,
+                                                       _stream_ptr(stream)), "rsfm_cashash_find_best_match_ex")
+    else:
+        mq = (ctypes.c_uint32 * n)(*(max_bucket_sizes or [q.max_bucket_size() for q in queries]))
+        _lib.check(lib.rsfm_cashash_find_best_match(qi, qs, ctypes.byref(ti), train.n, rr, n, mq,
+                                                    train.max_bucket_size(), _stream_ptr(stream)),
+                   "rsfm_cashash_find_best_match")
+    return outs

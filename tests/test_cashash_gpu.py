@@ -236,3 +236,33 @@ def test_find_best_match(rsfm, oracle, ref, n, nq):
                                                 train["host_buckets"], per_scheme=True)
         np.testing.assert_array_equal(got_ps[t][0], eq)
         np.testing.assert_array_equal(got_ps[t][1], et)
+
+
+def test_find_best_match_timing_vs_reference(rsfm, oracle, ref):
+    """Same-box bar for findBestMatch: the reference's kernel and ours on 8 query images of 4096
+    uniform descriptors against one train image (uniform random keys, the reference test's
+    distribution), reference bucket indexing; results must agree. Times are printed."""
+    if ref is None:
+        pytest.skip("reference kernels not built")
+    rng = np.random.default_rng(5)
+    imgs = []
+    for _ in range(9):
+        desc = rng.integers(0, 256, size=(4096, 128), dtype=np.int64).astype(np.uint8)
+        keys = rng.integers(0, 256, size=(4096, 8), dtype=np.int64).astype(np.uint8)
+        imgs.append(_image(oracle, desc, keys))
+    queries, train = imgs[:8], imgs[8]
+    times = {}
+    outs = {}
+    for api in ("ref", "ours"):
+        _run_fbm(rsfm, queries, train, api=api, ref=ref)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            outs[api] = _run_fbm(rsfm, queries, train, api=api, ref=ref)
+        e1.record()
+        torch.cuda.synchronize()
+        times[api] = e0.elapsed_time(e1) / 3
+    print({k: f"{v * 1e3:.0f} us (incl. host copies)" for k, v in times.items()})
+    for (a, b), (c, d) in zip(outs["ref"], outs["ours"]):
+        np.testing.assert_array_equal(a, c)
+        np.testing.assert_array_equal(b, d)
