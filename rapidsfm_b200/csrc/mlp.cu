@@ -40,13 +40,19 @@ __device__ __forceinline__ void umma_f16(uint32_t d, uint64_t a, uint64_t b, uin
 }
 
 // ---------------------------------------------------------------- inference
+// Persistent, one CTA per SM, 256 threads. Per 128-descriptor tile: X (u8 -> bf16, x/64 exact)
+// into smem; layer 1 = 8 UMMAs (M=128, N=256, K=16) into TMEM columns 0-255; bias + ReLU -> bf16
+// H back to smem; layer 2 = 16 UMMAs (N=128) into columns 256-383; sign bits out. Two tiles are in
+// flight: the next tile's X conversion overlaps this tile's layer 2, and this tile's layer-2
+// epilogue overlaps the next tile's layer 1.
 constexpr int kInfThreads = 256;
 struct InfSmem {
     uint8_t w1[2][256 * 128];  // K panels of W1 (256 rows = outputs, 64 inputs per panel)
     uint8_t w2[4][128 * 128];  // K panels of W2 (128 rows, 64 hidden per panel)
-    uint8_t xh[4][128 * 128];  // X (panels 0-1) during layer 1, then H (panels 0-3)
+    uint8_t h[4][128 * 128];   // H: 4 K panels of 64 hidden units
+    uint8_t x[2][128 * 128];   // X: 2 K panels of 64 input dimensions
     float b1[256], b2[128];
-    uint64_t mma;
+    uint64_t mma1, mma2;
     uint32_t tmem;
 };
 
@@ -71,7 +77,8 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
     for (uint32_t x = tid; x < 256; x += kInfThreads) S.b1[x] = b1[x];
     for (uint32_t x = tid; x < 128; x += kInfThreads) S.b2[x] = b2[x];
     if (tid == 0) {
-        mbar_init(&S.mma, 1);
+        mbar_init(&S.mma1, 1);
+        mbar_init(&S.mma2, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
@@ -85,43 +92,65 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
     const uint32_t q = warp & 3u, half = warp >> 2;
     const uint32_t laneBase = (32u * q) << 16;
     const uint32_t row = 32u * q + lane;
-    uint32_t phase = 0;
-    for (uint32_t tile = blockIdx.x; tile * 128u < n; tile += gridDim.x) {
-        // ---- X: thread t converts half t%2 of row t/2 (64 bytes -> 64 bf16 = one panel row)
-        {
-            const uint32_t r = tid >> 1, h = tid & 1u, i = tile * 128u + r;
-            uint4 raw[4] = {};
-            if (i < n) {
-                const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 64 * h);
+
+    // thread t converts half t%2 of row t/2 (64 bytes -> 64 bf16 = one panel row)
+    auto convert_x = [&](uint32_t tile) {
+        const uint32_t r = tid >> 1, hh = tid & 1u, i = tile * 128u + r;
+        uint4 raw[4] = {};
+        if (i < n) {
+            const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 64 * hh);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) raw[k] = src[k];
-            }
-            const uint8_t* b = reinterpret_cast<const uint8_t*>(raw);
+            for (int k = 0; k < 4; ++k) raw[k] = src[k];
+        }
+        const uint8_t* b = reinterpret_cast<const uint8_t*>(raw);
 #pragma unroll
-            for (uint32_t c = 0; c < 8; ++c) {
-                uint4 o;
-                o.x = pack_bf16x2(b[8 * c + 0] * (1.f / 64), b[8 * c + 1] * (1.f / 64));
-                o.y = pack_bf16x2(b[8 * c + 2] * (1.f / 64), b[8 * c + 3] * (1.f / 64));
-                o.z = pack_bf16x2(b[8 * c + 4] * (1.f / 64), b[8 * c + 5] * (1.f / 64));
-                o.w = pack_bf16x2(b[8 * c + 6] * (1.f / 64), b[8 * c + 7] * (1.f / 64));
-                *reinterpret_cast<uint4*>(S.xh[h] + sw128(r, c)) = o;
-            }
+        for (uint32_t c = 0; c < 8; ++c) {
+            uint4 o;
+            o.x = pack_bf16x2(b[8 * c + 0] * (1.f / 64), b[8 * c + 1] * (1.f / 64));
+            o.y = pack_bf16x2(b[8 * c + 2] * (1.f / 64), b[8 * c + 3] * (1.f / 64));
+            o.z = pack_bf16x2(b[8 * c + 4] * (1.f / 64), b[8 * c + 5] * (1.f / 64));
+            o.w = pack_bf16x2(b[8 * c + 6] * (1.f / 64), b[8 * c + 7] * (1.f / 64));
+            *reinterpret_cast<uint4*>(S.x[hh] + sw128(r, c)) = o;
         }
         fence_proxy_async_smem();
-        __syncthreads();
+    };
+    auto issue_layer1 = [&]() {
         if (tid == 0) {
             tc_fence_after();
 #pragma unroll
             for (uint32_t s = 0; s < 8; ++s) {
-                const uint32_t pa = smem_u32(S.xh[s >> 2]) + 32u * (s & 3u);
+                const uint32_t pa = smem_u32(S.x[s >> 2]) + 32u * (s & 3u);
                 const uint32_t pb = smem_u32(S.w1[s >> 2]) + 32u * (s & 3u);
                 umma_f16(tmem, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 256), s);
             }
-            umma_commit(&S.mma);
+            umma_commit(&S.mma1);
         }
+    };
+    auto issue_layer2 = [&]() {
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (uint32_t s = 0; s < 16; ++s) {
+                const uint32_t pa = smem_u32(S.h[s >> 2]) + 32u * (s & 3u);
+                const uint32_t pb = smem_u32(S.w2[s >> 2]) + 32u * (s & 3u);
+                umma_f16(tmem + 256u, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 128), s);
+            }
+            umma_commit(&S.mma2);
+        }
+    };
+
+    uint32_t ph1 = 0, ph2 = 0;
+    if (blockIdx.x * 128u < n) {
+        convert_x(blockIdx.x);
+        __syncthreads();
+        issue_layer1();
+    }
+    for (uint32_t tile = blockIdx.x; tile * 128u < n; tile += gridDim.x) {
+        const uint32_t next = tile + gridDim.x;
+        const bool hasNext = next * 128u < n;
         __syncwarp();
-        mbar_wait(&S.mma, phase, err, kDevTimeoutAccFull);
-        phase ^= 1u;
+        mbar_wait(&S.mma1, ph1, err, kDevTimeoutAccFull);
+        ph1 ^= 1u;
         tc_fence_after();
         // ---- layer-1 epilogue: warp (q, half) handles rows 32q.. and hidden [128 half, +128)
 #pragma unroll 1
@@ -141,25 +170,20 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
                 o.z = pack_bf16x2(f[4], f[5]);
                 o.w = pack_bf16x2(f[6], f[7]);
                 const uint32_t k0 = col + 8 * c8;  // hidden index of the chunk
-                *reinterpret_cast<uint4*>(S.xh[k0 >> 6] + sw128(row, (k0 >> 3) & 7u)) = o;
+                *reinterpret_cast<uint4*>(S.h[k0 >> 6] + sw128(row, (k0 >> 3) & 7u)) = o;
             }
         }
         tc_fence_before();
         fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll
-            for (uint32_t s = 0; s < 16; ++s) {
-                const uint32_t pa = smem_u32(S.xh[s >> 2]) + 32u * (s & 3u);
-                const uint32_t pb = smem_u32(S.w2[s >> 2]) + 32u * (s & 3u);
-                umma_f16(tmem + 256u, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 128), s);
-            }
-            umma_commit(&S.mma);
-        }
+        __syncthreads();  // H complete; TMEM columns 0-255 read; X free (layer 1 done)
+        issue_layer2();
+        if (hasNext) convert_x(next);
+        tc_fence_before();
+        __syncthreads();  // next X complete
+        if (hasNext) issue_layer1();  // TMEM columns 0-255 are free: their reads finished above
         __syncwarp();
-        mbar_wait(&S.mma, phase, err, kDevTimeoutAccFull);
-        phase ^= 1u;
+        mbar_wait(&S.mma2, ph2, err, kDevTimeoutAccFull);
+        ph2 ^= 1u;
         tc_fence_after();
         // ---- layer-2 epilogue: outputs [64 half, +64) -> 64 sign bits
         const uint32_t i = tile * 128u + row;
@@ -184,7 +208,7 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
             if (half == 0 && keys) *reinterpret_cast<uint2*>(keys + size_t(i) * 8) = make_uint2(bits[0], bits[1]);
         }
         tc_fence_before();
-        __syncthreads();
+        __syncthreads();  // TMEM columns 256-383 read; H may be overwritten (layer 2 done)
     }
     tc_fence_before();
     __syncthreads();
