@@ -69,6 +69,27 @@ int rsfm_precomp_sift_sqr_norm(uint32_t* sqrNorm, const void* desc, uint32_t nbD
  * reference: lexicographic minimum of (distance, index) in both directions. */
 int rsfm_bf_match(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream);
 
+/* Replaces launchBruteForceMatchIDP (bruteForceMatch.h:118, bruteForceMatch.cu:614-620), the
+ * matcher for callers without precomputed squared norms: sqrNormDescA/B are not read (may be
+ * NULL). Same results as rsfm_bf_match (the reference's dp4a kernel computes the same exact
+ * distances and tie rule); the norms are computed into stream-ordered scratch. */
+int rsfm_bf_match_idp(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream);
+
+/* 4-bit SIFT (the reference's useSift4b mode). A 4-bit descriptor is 64 bytes, 16-byte aligned,
+ * in the reference's packing: per 16 source bytes s[0..15], output byte 4i + k (i = 0, 1;
+ * k = 0..3) = (s[8i + k] >> 4) | (s[8i + 4 + k] & 0xF0).
+ * Replaces launchSiftDesc8bTo4b (bruteForceMatch.h:132, bruteForceMatchIMMA.cu:637-667). */
+int rsfm_sift_desc_8b_to_4b(void* dst4b, const void* src8b, uint32_t nbDesc, cudaStream_t stream);
+/* Replaces launchPreCompSift4bSqrNorm (bruteForceMatch.h:133, bruteForceMatchIMMA.cu:671-741):
+ * sqrNorm[i] = sum of squares of the 128 nibbles of desc4b[i]. */
+int rsfm_precomp_sift4b_sqr_norm(uint32_t* sqrNorm, const void* desc4b, uint32_t nbDesc, cudaStream_t stream);
+/* Replaces launchBruteForceMatchIMMA(const Sift4bBruteForceMatchTask*, size_t, cudaStream_t)
+ * (bruteForceMatch.h:134, bruteForceMatchIMMA.cu:617-624): tasks as rsfm_sift_bf_task with
+ * descA/descB pointing to 4-bit descriptors and norms from rsfm_precomp_sift4b_sqr_norm. L2
+ * distance over the 128 4-bit values, lexicographic (distance, index) minimum both directions.
+ * Each distinct image is widened to bytes in stream-ordered scratch (128 B per descriptor). */
+int rsfm_bf_match_4b(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream);
+
 /* Allocation-free rsfm_bf_match (no counterpart in the reference): same results, but the per-row
  * second-best scratch is a fixed 4 MiB device array instead of stream-ordered allocations, so no
  * call allocates device memory. At most 1 Mi query rows (sum of nbDescA) per call, else

@@ -18,7 +18,7 @@ NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
   --expt-relaxed-constexpr -Xcompiler -fPIC -shared \
   -I"$HERE/ref_shim" -I"$REF" \
   -o "$OUT/librsfm_ref.so.tmp" \
-  "$REF/bruteForceMatchIMMA.cu" "$REF/bruteForceMatch.cpp" \
+  "$REF/bruteForceMatchIMMA.cu" "$REF/bruteForceMatch.cu" "$REF/bruteForceMatch.cpp" \
   "$REF/casHash/accumulateDesc.cu" "$REF/casHash/computeHash.cu" \
   "$REF/casHash/buildBuckets.cu" "$REF/casHash/findBestMatch.cu" \
   "$HERE/ref_wrapper.cu"

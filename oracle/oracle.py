@@ -81,6 +81,31 @@ def bf_match(a, b, threads=0):
     return fwd, bwd, sec
 
 
+def desc_8b_to_4b(desc):
+    """The reference's 4-bit packing (bruteForceMatchIMMA.cu:637-660, kernelSiftDesc8bTo4b): per
+    16-byte group, output word i = ((word 2i & 0xF0F0F0F0) >> 4) | (word 2i+1 & 0xF0F0F0F0)."""
+    w = np.ascontiguousarray(desc, dtype=np.uint8).reshape(-1, 8, 4, 4).view(np.uint32)[..., 0]
+    w = w.reshape(-1, 8, 4)  # [n, group, word]
+    out = np.empty(w.shape[:2] + (2,), dtype=np.uint32)
+    for i in range(2):
+        out[..., i] = ((w[..., 2 * i] & 0xF0F0F0F0) >> 4) | (w[..., 2 * i + 1] & 0xF0F0F0F0)
+    return out.view(np.uint8).reshape(len(desc), 64)
+
+
+def desc_4b_values(desc4b):
+    """The 128 4-bit values of packed descriptors, as bytes [n, 128] in source dimension order:
+    low nibbles of packed word i of a group are dimensions 8i..8i+3, high nibbles 8i+4..8i+7."""
+    b = np.ascontiguousarray(desc4b, dtype=np.uint8).reshape(-1, 8, 2, 4)  # [n, group, word, byte]
+    lo, hi = b & 0x0F, b >> 4
+    return np.stack([lo, hi], axis=3).reshape(len(desc4b), 128)
+
+
+def sqr_norm_4b(desc4b):
+    """bruteForceMatchIMMA.cu:671-700 (kernelPreCompSift4bSqrNorm): sum of squared nibbles."""
+    v = desc_4b_values(desc4b).astype(np.uint32)
+    return (v * v).sum(axis=1).astype(np.uint32)
+
+
 def match_flags(fwd, second, bwd, ratio_num=64, ratio_den=100):
     out = np.empty(len(fwd), dtype=np.uint32)
     fwd = np.ascontiguousarray(fwd, dtype=np.uint32)
@@ -259,6 +284,10 @@ def load_ref():
     sig = {
         "ref_precomp_sqr_norm": (i32, [_P, _P, u32, _P]),
         "ref_bf_match_imma": (i32, [_P, ctypes.c_size_t, _P]),
+        "ref_bf_match_idp": (i32, [_P, ctypes.c_size_t, _P]),
+        "ref_desc_8b_to_4b": (i32, [_P, _P, u32, _P]),
+        "ref_precomp_sqr_norm_4b": (i32, [_P, _P, u32, _P]),
+        "ref_bf_match_imma_4b": (i32, [_P, ctypes.c_size_t, _P]),
         "ref_cross_check": (ctypes.c_size_t, [_P, u32, _P, u32, _P]),
         "ref_remove_match_conflicts": (ctypes.c_size_t, [_P, u32, u32, _P]),
         "ref_cashash_accumulate": (i32, [_P, _P, u32, i32, _P]),

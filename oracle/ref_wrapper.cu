@@ -25,6 +25,35 @@ int ref_bf_match_imma(const void* tasks, size_t n, cudaStream_t s) {
     return 0;
 }
 
+int ref_bf_match_idp(const void* tasks, size_t n, cudaStream_t s) {
+    try {
+        launchBruteForceMatchIDP(static_cast<const SiftBruteForceMatchTask*>(tasks), n, s);
+    } catch (...) { return 1; }
+    return 0;
+}
+
+int ref_desc_8b_to_4b(void* dst, const void* src, uint32_t n, cudaStream_t s) {
+    try {
+        launchSiftDesc8bTo4b(static_cast<Sift4bDescTraits::Descriptor*>(dst),
+                             static_cast<const SiftDescTraits::Descriptor*>(src), n, s);
+    } catch (...) { return 1; }
+    return 0;
+}
+
+int ref_precomp_sqr_norm_4b(uint32_t* sqrNorm, const void* desc, uint32_t n, cudaStream_t s) {
+    try {
+        launchPreCompSift4bSqrNorm(sqrNorm, static_cast<const Sift4bDescTraits::Descriptor*>(desc), n, s);
+    } catch (...) { return 1; }
+    return 0;
+}
+
+int ref_bf_match_imma_4b(const void* tasks, size_t n, cudaStream_t s) {
+    try {
+        launchBruteForceMatchIMMA(static_cast<const Sift4bBruteForceMatchTask*>(tasks), n, s);
+    } catch (...) { return 1; }
+    return 0;
+}
+
 size_t ref_cross_check(const void* fwd, uint32_t nq, const void* bwd, uint32_t nt, ValidMatch* out) {
     auto v = crossCheckMatches(static_cast<const SiftBruteForceMatchTask::BestMatch*>(fwd), nq,
                                static_cast<const SiftBruteForceMatchTask::BestMatch*>(bwd), nt);

@@ -10,11 +10,15 @@ from .matcher import (  # noqa: F401
     BruteForceMatcher,
     autotune_plan,
     bf_match,
+    bf_match_4b,
     bf_match_ext,
+    bf_match_idp,
     cross_check_matches,
     device_error,
     last_launch_count,
+    precomp_sift4b_sqr_norm,
     precomp_sift_sqr_norm,
     remove_match_conflicts,
+    sift_desc_8b_to_4b,
     unpack_best,
 )

@@ -17,6 +17,7 @@ SOURCES = [
     "common.cu",
     "bf_match.cu",
     "bf_match_noalloc.cu",
+    "bf_variants.cu",
     "bf_autotune.cpp",
     "host_filters.cpp",
     "diag.cu",

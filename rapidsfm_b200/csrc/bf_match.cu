@@ -533,9 +533,9 @@ __global__ void bf_flags_kernel(const __grid_constant__ FlagParams P) {
 // ---------------------------------------------------------------- squared norms
 // One warp per 4 descriptors: 8 lanes x 16 bytes per descriptor (coalesced 128-bit loads).
 __global__ void sqr_norm_kernel(uint32_t* __restrict__ out, const uint4* __restrict__ desc, uint32_t n) {
-    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t i = gid >> 3;
-    const uint32_t part = gid & 7u;
+    const uint64_t gid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t i = gid >> 3;
+    const uint32_t part = uint32_t(gid) & 7u;
     uint32_t acc = 0;
     if (i < n) {
         const uint4 v = __ldg(&desc[size_t(i) * 8 + part]);

@@ -3,6 +3,10 @@
 Reference interfaces mirrored (paths relative to the RapidSFM source tree):
   launchPreCompSiftSqrNorm    bruteForceMatch.h:135        -> precomp_sift_sqr_norm
   launchBruteForceMatchIMMA   bruteForceMatch.h:136        -> bf_match
+  launchBruteForceMatchIDP    bruteForceMatch.h:118        -> bf_match_idp
+  launchSiftDesc8bTo4b        bruteForceMatch.h:132        -> sift_desc_8b_to_4b
+  launchPreCompSift4bSqrNorm  bruteForceMatch.h:133        -> precomp_sift4b_sqr_norm
+  launchBruteForceMatchIMMA (Sift4bBruteForceMatchTask)     bruteForceMatch.h:134 -> bf_match_4b
   crossCheckMatches           bruteForceMatch.h:126        -> cross_check_matches
   removeMatchConflicts        bruteForceMatch.h:128        -> remove_match_conflicts
   BruteForceMatcher           bruteForceMatcher.h:28-102   -> BruteForceMatcher
@@ -32,9 +36,9 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
 
 
-def _check_desc(d):
-    if d.dtype != torch.uint8 or d.dim() != 2 or d.shape[1] != 128 or not d.is_cuda or not d.is_contiguous():
-        raise ValueError("descriptors must be a contiguous CUDA uint8 tensor of shape [n, 128]")
+def _check_desc(d, width=128):
+    if d.dtype != torch.uint8 or d.dim() != 2 or d.shape[1] != width or not d.is_cuda or not d.is_contiguous():
+        raise ValueError(f"descriptors must be a contiguous CUDA uint8 tensor of shape [n, {width}]")
 
 
 def precomp_sift_sqr_norm(desc, out=None, stream=None):
@@ -49,15 +53,48 @@ def precomp_sift_sqr_norm(desc, out=None, stream=None):
     return out
 
 
-class BFTask:
-    """One query/train pair: descA (queries) vs descB (train)."""
+def sift_desc_8b_to_4b(desc, out=None, stream=None):
+    """8-bit descriptors [n, 128] -> the reference's packed 4-bit form [n, 64] (high nibbles)."""
+    _check_desc(desc)
+    lib = _lib.load()
+    n = desc.shape[0]
+    if out is None:
+        out = torch.empty((n, 64), dtype=torch.uint8, device=desc.device)
+    _lib.check(lib.rsfm_sift_desc_8b_to_4b(_ptr(out), _ptr(desc), n, _stream_ptr(stream)), "rsfm_sift_desc_8b_to_4b")
+    return out
 
-    def __init__(self, descA, descB, sqrA=None, sqrB=None, stream=None):
-        _check_desc(descA)
-        _check_desc(descB)
+
+def precomp_sift4b_sqr_norm(desc4b, out=None, stream=None):
+    """Squared norm of each packed 4-bit descriptor [n, 64] (sum over its 128 nibbles)."""
+    _check_desc(desc4b, 64)
+    lib = _lib.load()
+    n = desc4b.shape[0]
+    if out is None:
+        out = torch.empty(n, dtype=torch.int32, device=desc4b.device)
+    _lib.check(lib.rsfm_precomp_sift4b_sqr_norm(_ptr(out), _ptr(desc4b), n, _stream_ptr(stream)),
+               "rsfm_precomp_sift4b_sqr_norm")
+    return out
+
+
+class BFTask:
+    """One query/train pair: descA (queries) vs descB (train).
+
+    bits=4: descriptors are packed 4-bit [n, 64] (norms from precomp_sift4b_sqr_norm).
+    norms=False: no squared norms (for bf_match_idp, which does not read them).
+    """
+
+    def __init__(self, descA, descB, sqrA=None, sqrB=None, stream=None, bits=8, norms=True):
+        width = 64 if bits == 4 else 128
+        _check_desc(descA, width)
+        _check_desc(descB, width)
         self.descA, self.descB = descA, descB
-        self.sqrA = sqrA if sqrA is not None else precomp_sift_sqr_norm(descA, stream=stream)
-        self.sqrB = sqrB if sqrB is not None else precomp_sift_sqr_norm(descB, stream=stream)
+        pre = precomp_sift4b_sqr_norm if bits == 4 else precomp_sift_sqr_norm
+        if not norms:
+            sqrA = sqrB = None
+        else:
+            sqrA = sqrA if sqrA is not None else pre(descA, stream=stream)
+            sqrB = sqrB if sqrB is not None else pre(descB, stream=stream)
+        self.sqrA, self.sqrB = sqrA, sqrB
         dev = descA.device
         self.bestA = torch.empty(descA.shape[0], dtype=torch.int64, device=dev)
         self.bestB = torch.empty(descB.shape[0], dtype=torch.int64, device=dev)
@@ -67,7 +104,8 @@ class BFTask:
     def as_ctype(self):
         return _lib.SiftBFTask(self.descA.shape[0], self.descB.shape[0], self.descA.data_ptr(),
                                self.descB.data_ptr(), self.bestA.data_ptr(), self.bestB.data_ptr(),
-                               self.sqrA.data_ptr(), self.sqrB.data_ptr())
+                               self.sqrA.data_ptr() if self.sqrA is not None else 0,
+                               self.sqrB.data_ptr() if self.sqrB is not None else 0)
 
 
 def bf_match(tasks, stream=None):
@@ -75,6 +113,22 @@ def bf_match(tasks, stream=None):
     lib = _lib.load()
     arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
     _lib.check(lib.rsfm_bf_match(arr, len(tasks), _stream_ptr(stream)), "rsfm_bf_match")
+    return tasks
+
+
+def bf_match_idp(tasks, stream=None):
+    """launchBruteForceMatchIDP: same results as bf_match; the tasks' norms are not read."""
+    lib = _lib.load()
+    arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+    _lib.check(lib.rsfm_bf_match_idp(arr, len(tasks), _stream_ptr(stream)), "rsfm_bf_match_idp")
+    return tasks
+
+
+def bf_match_4b(tasks, stream=None):
+    """launchBruteForceMatchIMMA on 4-bit tasks (BFTask(..., bits=4))."""
+    lib = _lib.load()
+    arr = (_lib.SiftBFTask * len(tasks))(*[t.as_ctype() for t in tasks])
+    _lib.check(lib.rsfm_bf_match_4b(arr, len(tasks), _stream_ptr(stream)), "rsfm_bf_match_4b")
     return tasks
 
 
@@ -208,25 +262,38 @@ class BruteForceMatcher:
     (bruteForceMatcher.cpp:426-442).
     """
 
-    def __init__(self, device="cuda"):
+    def __init__(self, device="cuda", use_sift4b=False, use_sqr_norm_precomp=True):
         self.device = torch.device(device)
         self._images = {}
         self.stream = torch.cuda.Stream(device=self.device)
+        # bruteForceMatcher.cpp:113-119: 4-bit mode implies the norm precompute; without it the
+        # dp4a matcher (IDP) runs.
+        self.use_sift4b = use_sift4b
+        self.use_sqr_norm_precomp = use_sqr_norm_precomp or use_sift4b
 
     def register_image(self, handle, desc):
         _check_desc(desc)
         with torch.cuda.stream(self.stream):
-            self._images[handle] = (desc, precomp_sift_sqr_norm(desc, stream=self.stream))
+            if self.use_sift4b:
+                d4 = sift_desc_8b_to_4b(desc, stream=self.stream)
+                self._images[handle] = (d4, precomp_sift4b_sqr_norm(d4, stream=self.stream))
+            elif self.use_sqr_norm_precomp:
+                self._images[handle] = (desc, precomp_sift_sqr_norm(desc, stream=self.stream))
+            else:
+                self._images[handle] = (desc, None)
 
     def _tasks(self, queries, train):
         dt, st = self._images[train]
-        return [BFTask(self._images[q][0], dt, self._images[q][1], st) for q in queries]
+        bits = 4 if self.use_sift4b else 8
+        return [BFTask(self._images[q][0], dt, self._images[q][1], st, bits=bits,
+                       norms=self.use_sqr_norm_precomp) for q in queries]
 
     def match(self, queries, train):
         if not queries:
             return []
+        run = bf_match_4b if self.use_sift4b else bf_match if self.use_sqr_norm_precomp else bf_match_idp
         with torch.cuda.stream(self.stream):
-            tasks = bf_match(self._tasks(queries, train), stream=self.stream)
+            tasks = run(self._tasks(queries, train), stream=self.stream)
         self.stream.synchronize()
         return [(np.stack(unpack_best(t.bestA), 1), np.stack(unpack_best(t.bestB), 1)) for t in tasks]
 

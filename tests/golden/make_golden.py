@@ -4,7 +4,9 @@ Runs on a machine with an sm_100 GPU and the reference kernels built by oracle/b
 (oracle/_ref/librsfm_ref.so). Inputs are seeded; every fixture stores its inputs and the
 reference kernels' outputs, so the CPU tests can pin the oracle without a GPU:
 
-    python tests/golden/make_golden.py [output_dir]
+    python tests/golden/make_golden.py [output_dir] [fixture ...]
+
+With fixture names (e.g. bf4b_sift bf_idp_sift) only those are written.
 """
 import ctypes
 import os
@@ -44,6 +46,38 @@ def ref_bf(ref, a, b):
             sA.cpu().numpy().view(np.uint32))
 
 
+def ref_bf4b(ref, a, b):
+    """The reference's 4-bit path: pack both sets, 4-bit norms, 4-bit matcher."""
+    dA, dB = dev(a), dev(b)
+    pA = torch.empty((len(a), 64), dtype=torch.uint8, device="cuda")
+    pB = torch.empty((len(b), 64), dtype=torch.uint8, device="cuda")
+    assert ref.ref_desc_8b_to_4b(P(pA.data_ptr()), P(dA.data_ptr()), len(a), None) == 0
+    assert ref.ref_desc_8b_to_4b(P(pB.data_ptr()), P(dB.data_ptr()), len(b), None) == 0
+    sA = torch.empty(len(a), dtype=torch.int32, device="cuda")
+    sB = torch.empty(len(b), dtype=torch.int32, device="cuda")
+    assert ref.ref_precomp_sqr_norm_4b(P(sA.data_ptr()), P(pA.data_ptr()), len(a), None) == 0
+    assert ref.ref_precomp_sqr_norm_4b(P(sB.data_ptr()), P(pB.data_ptr()), len(b), None) == 0
+    fwd = torch.empty(len(a), dtype=torch.int64, device="cuda")
+    bwd = torch.empty(len(b), dtype=torch.int64, device="cuda")
+    t = SiftBFTask(len(a), len(b), pA.data_ptr(), pB.data_ptr(), fwd.data_ptr(), bwd.data_ptr(), sA.data_ptr(),
+                   sB.data_ptr())
+    assert ref.ref_bf_match_imma_4b(ctypes.byref(t), 1, None) == 0
+    torch.cuda.synchronize()
+    u32 = lambda x: x.cpu().numpy().view(np.uint32)  # noqa: E731
+    return (pA.cpu().numpy(), pB.cpu().numpy(), u32(sA), u32(sB), u32(fwd).reshape(-1, 2), u32(bwd).reshape(-1, 2))
+
+
+def ref_bf_idp(ref, a, b):
+    """The reference's dp4a matcher (no squared norms)."""
+    dA, dB = dev(a), dev(b)
+    fwd = torch.empty(len(a), dtype=torch.int64, device="cuda")
+    bwd = torch.empty(len(b), dtype=torch.int64, device="cuda")
+    t = SiftBFTask(len(a), len(b), dA.data_ptr(), dB.data_ptr(), fwd.data_ptr(), bwd.data_ptr(), 0, 0)
+    assert ref.ref_bf_match_idp(ctypes.byref(t), 1, None) == 0
+    torch.cuda.synchronize()
+    return (fwd.cpu().numpy().view(np.uint32).reshape(-1, 2), bwd.cpu().numpy().view(np.uint32).reshape(-1, 2))
+
+
 def ref_hash(ref, w, b, desc):
     n, c = len(desc), len(w)
     dw, db, dd = dev(w), dev(b), dev(desc)
@@ -56,8 +90,25 @@ def ref_hash(ref, w, b, desc):
     return keys.cpu().numpy(), remap.cpu().numpy().view(np.uint32), hist.cpu().numpy().view(np.uint32)
 
 
-def main(out):
+def variants(ref, out, only):
+    """4-bit path and dp4a matcher fixtures."""
+    a, b = synth.make_pair(300, 340, 0.6, 8.0, seed=109)[:2]
+    if not only or "bf4b_sift" in only:
+        a4, b4, s4a, s4b, fwd, bwd = ref_bf4b(ref, a, b)
+        np.savez_compressed(os.path.join(out, "bf4b_sift.npz"), a=a, b=b, a4=a4, b4=b4, sqr4_a=s4a, sqr4_b=s4b,
+                            fwd=fwd, bwd=bwd)
+    if not only or "bf_idp_sift" in only:
+        fwd, bwd = ref_bf_idp(ref, a, b)
+        np.savez_compressed(os.path.join(out, "bf_idp_sift.npz"), a=a, b=b, fwd=fwd, bwd=bwd)
+
+
+def main(out, only=()):
     ref = orc.load_ref()
+    if only:
+        variants(ref, out, only)
+        print("golden fixtures written to", out)
+        return
+    variants(ref, out, only)
     # brute force: uniform bytes (the reference test's input kind), SIFT-like, heavy ties
     cases = {
         "bf_uniform": (synth.uniform_bytes(300, 101), synth.uniform_bytes(320, 102)),
@@ -83,4 +134,4 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE, tuple(sys.argv[2:]))

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-BF = sorted(glob.glob(os.path.join(HERE, "bf_*.npz")))
+BF = sorted(p for p in glob.glob(os.path.join(HERE, "bf_*.npz")) if "sqr_a" in np.load(p).files)
 
 
 @pytest.mark.parametrize("path", BF, ids=[os.path.basename(p) for p in BF])
@@ -17,6 +17,33 @@ def test_oracle_matches_reference_bruteforce(oracle, path):
     np.testing.assert_array_equal(fwd, z["fwd"])
     np.testing.assert_array_equal(bwd, z["bwd"])
     np.testing.assert_array_equal(oracle.sqr_norm(z["a"]), z["sqr_a"])
+
+
+def _fixture(name):
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    return np.load(path)
+
+
+def test_oracle_matches_reference_4bit(oracle):
+    # launchSiftDesc8bTo4b, launchPreCompSift4bSqrNorm and the 4-bit matcher of the reference
+    z = _fixture("bf4b_sift.npz")
+    np.testing.assert_array_equal(oracle.desc_8b_to_4b(z["a"]), z["a4"])
+    np.testing.assert_array_equal(oracle.desc_8b_to_4b(z["b"]), z["b4"])
+    np.testing.assert_array_equal(oracle.sqr_norm_4b(z["a4"]), z["sqr4_a"])
+    np.testing.assert_array_equal(oracle.sqr_norm_4b(z["b4"]), z["sqr4_b"])
+    fwd, bwd, _ = oracle.bf_match(oracle.desc_4b_values(z["a4"]), oracle.desc_4b_values(z["b4"]))
+    np.testing.assert_array_equal(fwd, z["fwd"])
+    np.testing.assert_array_equal(bwd, z["bwd"])
+
+
+def test_oracle_matches_reference_idp(oracle):
+    # launchBruteForceMatchIDP (dp4a, no squared norms) gives the exact matcher's results
+    z = _fixture("bf_idp_sift.npz")
+    fwd, bwd, _ = oracle.bf_match(z["a"], z["b"])
+    np.testing.assert_array_equal(fwd, z["fwd"])
+    np.testing.assert_array_equal(bwd, z["bwd"])
 
 
 def test_oracle_matches_reference_hash(oracle):

@@ -133,3 +133,57 @@ def test_faster_than_reference_kernels(ref, rsfm):
     assert torch.equal(outs["reference"][0], outs["rsfm_b200"][0])
     assert torch.equal(outs["reference"][1], outs["rsfm_b200"][1])
     assert times["rsfm_b200"] < times["reference"]
+
+
+def _time(fn, reps=5):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+@pytest.mark.parametrize("n", [897, 8192])
+def test_4bit_and_idp_match_reference_kernels(ref, rsfm, n):
+    """The reference's 4-bit path (pack, 4-bit norms, u4 matcher) and its dp4a matcher against
+    ours on the same SIFT-like pair: identical packed bytes, norms and results; times printed."""
+    from rapidsfm_b200._lib import SiftBFTask
+    P = ctypes.c_void_p
+    q, t, _ = synth.make_pair(n, n + 37, 0.5, 10.0, seed=n)
+    dA, dB = torch.from_numpy(q).cuda(), torch.from_numpy(t).cuda()
+    lib = rsfm._lib.load()
+    packed = {}
+    for name, pack, norm in (("reference", ref.ref_desc_8b_to_4b, ref.ref_precomp_sqr_norm_4b),
+                             ("rsfm_b200", lib.rsfm_sift_desc_8b_to_4b, lib.rsfm_precomp_sift4b_sqr_norm)):
+        pA = torch.empty((len(q), 64), dtype=torch.uint8, device="cuda")
+        pB = torch.empty((len(t), 64), dtype=torch.uint8, device="cuda")
+        sA = torch.empty(len(q), dtype=torch.int32, device="cuda")
+        sB = torch.empty(len(t), dtype=torch.int32, device="cuda")
+        for src, dst, sq in ((dA, pA, sA), (dB, pB, sB)):
+            assert pack(P(dst.data_ptr()), P(src.data_ptr()), len(src), None) == 0
+            assert norm(P(sq.data_ptr()), P(dst.data_ptr()), len(dst), None) == 0
+        packed[name] = (pA, pB, sA, sB)
+    for a, b in zip(packed["reference"], packed["rsfm_b200"]):
+        assert torch.equal(a, b)
+    pA, pB, sA, sB = packed["reference"]
+    times, outs = {}, {}
+    runs = (("ref_4b", ref.ref_bf_match_imma_4b, pA, pB, sA, sB), ("b200_4b", lib.rsfm_bf_match_4b, pA, pB, sA, sB),
+            ("ref_idp", ref.ref_bf_match_idp, dA, dB, None, None), ("b200_idp", lib.rsfm_bf_match_idp, dA, dB, None, None))
+    for name, fn, a, b, na, nb in runs:
+        fwd = torch.empty(len(a), dtype=torch.int64, device="cuda")
+        bwd = torch.empty(len(b), dtype=torch.int64, device="cuda")
+        task = SiftBFTask(len(a), len(b), a.data_ptr(), b.data_ptr(), fwd.data_ptr(), bwd.data_ptr(),
+                          na.data_ptr() if na is not None else 0, nb.data_ptr() if nb is not None else 0)
+        times[name] = _time(lambda: fn(ctypes.byref(task), 1, None))
+        assert fn(ctypes.byref(task), 1, None) == 0
+        torch.cuda.synchronize()
+        outs[name] = (fwd.clone(), bwd.clone())
+    print({k: f"{v * 1e3:.0f} us" for k, v in times.items()})
+    for x, y in (("ref_4b", "b200_4b"), ("ref_idp", "b200_idp")):
+        assert torch.equal(outs[x][0], outs[y][0])
+        assert torch.equal(outs[x][1], outs[y][1])
+    assert rsfm.device_error() == 0
