@@ -398,6 +398,7 @@ def run_ours(args):
 
     extras = {}
     if not args.no_extras and ws == 1:  # single-GPU sections; scaling runs time the pair only
+        extras["filtered"] = run_filtered(dev, stream, q, t)
         extras["batched"] = run_batched(dev, stream)
         extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
         extras["hash"] = run_hash(dev, stream, n=1 << args.hash_log2)
@@ -445,6 +446,73 @@ def _events_ms(fn, reps, stream):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def run_filtered(dev, stream, q, t, reps=10):
+    """matchAndFilter, cross-check mode, one pair through the public API, wall clock per pair with
+    the H2D of both descriptor sets: filters on the GPU (the count, then only the surviving
+    ValidMatch records cross to the host) vs the reference's flow (both BestMatch arrays to the
+    host, then the host crossCheckMatches, bruteForceMatcher.cpp:355-369, 426-442)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import rapidsfm_b200 as R
+
+    lib = R._lib.load()
+    nq, nt = len(q), len(t)
+    hq, ht = torch.from_numpy(q).pin_memory(), torch.from_numpy(t).pin_memory()
+    dq, dt_ = torch.empty_like(hq, device=dev), torch.empty_like(ht, device=dev)
+    task = R.BFTask(dq, dt_)
+    cap = min(nq, nt)
+    out = torch.empty((cap, 3), dtype=torch.int32, device=dev)
+    cnt = torch.empty(1, dtype=torch.int32, device=dev)
+    hout = torch.empty((cap, 3), dtype=torch.int32).pin_memory()
+    hcnt = torch.empty(1, dtype=torch.int32).pin_memory()
+    hf = torch.empty(nq, dtype=torch.int64).pin_memory()
+    hb = torch.empty(nt, dtype=torch.int64).pin_memory()
+    hvm = np.empty((cap, 3), dtype=np.uint32)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def match():
+        dq.copy_(hq, non_blocking=True)
+        dt_.copy_(ht, non_blocking=True)
+        R.precomp_sift_sqr_norm(dq, out=task.sqrA, stream=stream)
+        R.precomp_sift_sqr_norm(dt_, out=task.sqrB, stream=stream)
+        R.bf_match([task], stream=stream)
+
+    def on_device():
+        match()
+        R._lib.check(lib.rsfm_cross_check_matches_device(task.bestA.data_ptr(), nq, task.bestB.data_ptr(), nt,
+                                                         out.data_ptr(), cnt.data_ptr(), sp), "filter")
+        hcnt.copy_(cnt, non_blocking=True)
+        stream.synchronize()
+        n = int(hcnt[0])
+        hout[:n].copy_(out[:n], non_blocking=True)
+        stream.synchronize()
+        return n, 4 + 12 * n
+
+    def on_host():
+        match()
+        hf.copy_(task.bestA, non_blocking=True)
+        hb.copy_(task.bestB, non_blocking=True)
+        stream.synchronize()
+        n = lib.rsfm_cross_check_matches(hf.data_ptr(), nq, hb.data_ptr(), nt, hvm.ctypes.data)
+        return n, 8 * (nq + nt)
+
+    res = {}
+    for name, fn in (("device_filter", on_device), ("host_filter", on_host)):
+        for _ in range(3):
+            fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            n, d2h = fn()
+        ms = (time.perf_counter() - t0) * 1e3 / reps
+        res[name] = {"ms_per_pair": ms, "matches": int(n), "d2h_bytes": int(d2h)}
+    assert res["device_filter"]["matches"] == res["host_filter"]["matches"]
+    res["pair"] = f"{nq}x{nt}"
+    return res
 
 
 def run_batched(dev, stream, seed=2):

@@ -145,6 +145,17 @@ size_t rsfm_cross_check_matches(const rsfm_best_match* matches, uint32_t nbQuery
 size_t rsfm_remove_match_conflicts(const rsfm_best_match* matches, uint32_t nbQueryDesc, uint32_t nbTrainDesc,
                                    rsfm_valid_match* out);
 
+/* Device-side crossCheckMatches / removeMatchConflicts (same semantics and output order as the
+ * two host functions above; no reference counterpart on the GPU — the reference copies both
+ * BestMatch arrays to the host, bruteForceMatcher.cpp:355-369). matches/matchesBwd/out/count are
+ * device memory; `out` must hold min(nbQueryDesc, nbTrainDesc) records; *count receives the
+ * number written. Only `count` and the first *count records need to cross to the host. */
+int rsfm_cross_check_matches_device(const rsfm_best_match* matches, uint32_t nbQueryDesc,
+                                    const rsfm_best_match* matchesBwd, uint32_t nbTrainDesc, rsfm_valid_match* out,
+                                    uint32_t* count, cudaStream_t stream);
+int rsfm_remove_match_conflicts_device(const rsfm_best_match* matches, uint32_t nbQueryDesc, uint32_t nbTrainDesc,
+                                       rsfm_valid_match* out, uint32_t* count, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- cascade hash
  * Descriptors are nbDesc x 128 uint8, 16-byte aligned. Weights are nbChannels x 128 int8 rows
  * (the reference's KArray<int32_t, 32> per channel), 16-byte aligned; 64 channels give the 8

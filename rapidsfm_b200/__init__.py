@@ -15,10 +15,12 @@ from .matcher import (  # noqa: F401
     bf_match_idp,
     cross_check_matches,
     device_error,
+    filter_matches_device,
     last_launch_count,
     precomp_sift4b_sqr_norm,
     precomp_sift_sqr_norm,
     remove_match_conflicts,
     sift_desc_8b_to_4b,
     unpack_best,
+    valid_matches_to_host,
 )

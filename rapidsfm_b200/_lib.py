@@ -87,6 +87,11 @@ SIGNATURES = {
     "rsfm_precomp_sift_sqr_norm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_bf_match": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
     "rsfm_bf_match_noalloc": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
+    "rsfm_cross_check_matches_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                       ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
+    "rsfm_remove_match_conflicts_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_match_idp": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
     "rsfm_sift_desc_8b_to_4b": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_precomp_sift4b_sqr_norm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,

@@ -18,6 +18,7 @@ SOURCES = [
     "bf_match.cu",
     "bf_match_noalloc.cu",
     "bf_variants.cu",
+    "filters.cu",
     "bf_autotune.cpp",
     "host_filters.cpp",
     "diag.cu",

@@ -242,6 +242,39 @@ def remove_match_conflicts(fwd, nb_train):
     return _valid_matches(buf, n)
 
 
+_VM_DTYPE = np.dtype([("idxQuery", "<u4"), ("idxTrain", "<u4"), ("distance", "<f4")])
+
+
+def filter_matches_device(bestA, bestB=None, nb_train=None, cross_check=True, stream=None):
+    """Device-side crossCheckMatches (bestB given) or removeMatchConflicts (nb_train given).
+
+    bestA/bestB: int64 BestMatch tensors on the GPU. Returns (records, count): a [cap, 3] int32
+    device tensor of ValidMatch records and a 1-element int32 device tensor with their number;
+    nothing is copied to the host and nothing synchronizes.
+    """
+    lib = _lib.load()
+    nq = bestA.shape[0]
+    nt = bestB.shape[0] if cross_check else int(nb_train)
+    cap = max(1, min(nq, nt))
+    out = torch.empty((cap, 3), dtype=torch.int32, device=bestA.device)
+    count = torch.empty(1, dtype=torch.int32, device=bestA.device)
+    if cross_check:
+        st = lib.rsfm_cross_check_matches_device(_ptr(bestA), nq, _ptr(bestB), nt, _ptr(out), _ptr(count),
+                                                 _stream_ptr(stream))
+        _lib.check(st, "rsfm_cross_check_matches_device")
+    else:
+        st = lib.rsfm_remove_match_conflicts_device(_ptr(bestA), nq, nt, _ptr(out), _ptr(count), _stream_ptr(stream))
+        _lib.check(st, "rsfm_remove_match_conflicts_device")
+    return out, count
+
+
+def valid_matches_to_host(out, count):
+    """Copies the count, then only the surviving records, to the host (ValidMatch structured array)."""
+    n = int(count.item())
+    rec = out[:n].cpu().numpy()
+    return np.ascontiguousarray(rec).view(_VM_DTYPE).reshape(-1).copy()
+
+
 def device_error():
     lib = _lib.load()
     code = ctypes.c_uint32(0)
@@ -297,8 +330,20 @@ class BruteForceMatcher:
         self.stream.synchronize()
         return [(np.stack(unpack_best(t.bestA), 1), np.stack(unpack_best(t.bestB), 1)) for t in tasks]
 
-    def match_and_filter(self, queries, train, cross_check=True):
-        res = []
-        for fwd, bwd in self.match(queries, train):
-            res.append(cross_check_matches(fwd, bwd) if cross_check else remove_match_conflicts(fwd, len(bwd)))
-        return res
+    def match_and_filter(self, queries, train, cross_check=True, on_device=True):
+        """Matches, then filters: on the GPU by default (only surviving records cross to the
+        host), or with the host filters like the reference (bruteForceMatcher.cpp:426-442)."""
+        if not on_device:
+            res = []
+            for fwd, bwd in self.match(queries, train):
+                res.append(cross_check_matches(fwd, bwd) if cross_check else remove_match_conflicts(fwd, len(bwd)))
+            return res
+        if not queries:
+            return []
+        run = bf_match_4b if self.use_sift4b else bf_match if self.use_sqr_norm_precomp else bf_match_idp
+        with torch.cuda.stream(self.stream):
+            tasks = run(self._tasks(queries, train), stream=self.stream)
+            filtered = [filter_matches_device(t.bestA, t.bestB, nb_train=t.bestB.shape[0], cross_check=cross_check,
+                                              stream=self.stream) for t in tasks]
+        self.stream.synchronize()
+        return [valid_matches_to_host(out, count) for out, count in filtered]
