@@ -25,6 +25,7 @@
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <vector>
 
@@ -50,7 +51,7 @@ struct Cfg {
     static constexpr int kBStages = kWG == 4 ? 2 : 3;
 };
 constexpr uint32_t kMaxDist = 128u * 255u * 255u;  // largest possible squared L2 of uint8x128
-constexpr uint32_t kVBias = 1u << 23;                // makes (|b|^2 - d) + bias positive
+
 
 struct alignas(64) TaskDev {
     CUtensorMap tmA;
@@ -118,7 +119,7 @@ struct Smem {
     uint8_t a[kMaxRowTiles][kTileBytes];
     uint8_t b[Cfg<kWG>::kBStages][kTileBytes];
     int32_t nbk[kUnitCols];              // per unit column: row-key addend (31 - j % 32) - |b|^2 * 256
-    unsigned long long colmin[2][128];   // [block parity][column]: merge of the 4 lane quarters
+    int32_t colkey[2][4][128];           // [block parity][lane quarter][column]: quarter maxima
     // Row state of the current unit, per unit row r = 128 p + 32 q + lane:
     int32_t rowc[kUnitRows];             // column-key addend ((7-p) << 5 | (31-lane)) - |a|^2 * 256
     // Per warpgroup: tk = trigger threshold in row-key space (set from the global best at unit
@@ -184,7 +185,6 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         tmem_alloc(&S.tmemBase, 512);
         tmem_relinquish();
     }
-    for (uint32_t x = threadIdx.x; x < 2 * 128; x += blockDim.x) (&S.colmin[0][0])[x] = ~0ull;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -413,35 +413,37 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                     }
                     S.l2k[wg][r] = l2kP;
                 }
-                // ---- column flush: best key per column over this warp's 32 lanes, then over the
-                // four lane quarters in shared memory, then one global atomic per column.
+                // ---- column flush: best key per column over this warp's 32 lanes (butterfly),
+                // then over the four lane quarters: their keys go to shared memory and one thread
+                // per column merges them in row order, then one global atomic per column.
 #pragma unroll
                 for (int cc = 0; cc < kCPW; ++cc) {
                     int32_t v[32];
 #pragma unroll
                     for (int k = 0; k < 32; ++k) v[k] = ca[32 * cc + k];
                     column_max_butterfly(v, lane);
-                    const int32_t mine = v[0];
-                    // (2 a.b - |a|^2) = |b|^2 - d; row = 128 p + 32 q + lane
-                    const int32_t val = mine >> 8;
-                    const uint32_t pp = 7u - ((uint32_t(mine) >> 5) & 7u);
-                    const uint32_t ln = 31u - (uint32_t(mine) & 31u);
-                    const uint32_t rr = 128u * pp + 32u * q + ln;
-                    const unsigned long long key =
-                        (static_cast<unsigned long long>(uint32_t(int32_t(kVBias) - val)) << 32) | rr;
-                    atomicMin(&S.colmin[bpar][jw - blockBase + 32 * cc + lane], key);
+                    S.colkey[bpar][q][jw - blockBase + 32 * cc + lane] = v[0];
                 }
                 named_bar(2 + wg, 128);
                 if (t128 < 32 * kCPW) {
                     const uint32_t cc = jw - blockBase + t128;
-                    const unsigned long long key = S.colmin[bpar][cc];
-                    S.colmin[bpar][cc] = ~0ull;
+                    // Quarter keys order (|b|^2 - d, p, lane) within a quarter; across quarters the
+                    // row 128 p + 32 q + lane decides ties, so compare (value, -row) explicitly.
+                    long long best = LLONG_MIN;
+#pragma unroll
+                    for (uint32_t qq = 0; qq < 4; ++qq) {
+                        const int32_t k = S.colkey[bpar][qq][cc];
+                        const uint32_t rr = 128u * (7u - ((uint32_t(k) >> 5) & 7u)) + 32u * qq + (31u - (uint32_t(k) & 31u));
+                        best = max(best, static_cast<long long>(k >> 8) * 1024 + (1023 - rr));
+                    }
+                    const int32_t val = int32_t(best >> 10);  // (2 a.b - |a|^2) = |b|^2 - d
+                    const uint32_t rr = 1023u - uint32_t(best & 1023);
                     const uint32_t j = blockBase + cc;
-                    const uint32_t i = U.r0 + uint32_t(key & 0xFFFFFFFFu);
+                    const uint32_t i = U.r0 + rr;
                     if (j < T.nB && i < T.nA) {
                         const uint32_t xj = j - U.c0;  // |b_j|^2 from the staged row-key addend
                         const uint32_t nbj = ((31u - (xj & 31u)) - uint32_t(S.nbk[xj])) >> 8;
-                        const uint32_t d = uint32_t(key >> 32) - kVBias + nbj;
+                        const uint32_t d = nbj - uint32_t(val);
                         atomicMin(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
                     }
                 }
