@@ -156,6 +156,50 @@ int rsfm_cross_check_matches_device(const rsfm_best_match* matches, uint32_t nbQ
 int rsfm_remove_match_conflicts_device(const rsfm_best_match* matches, uint32_t nbQueryDesc, uint32_t nbTrainDesc,
                                        rsfm_valid_match* out, uint32_t* count, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- RANSAC match filter
+ * The filter that follows matching (RansacMatchFilter.h:33, RansacMatchFilter.cu:196-419):
+ * per image cell, random 3-match affine fits over the 3x3 cell neighbourhood; each cell's best
+ * model (or the best of every cell's models, tryOtherSolutions) votes for its inliers when it
+ * has >= 6. The reference seeds its generator from clock(); here `seed` makes runs repeatable.
+ * A cell whose neighbourhood holds fewer than 9 matches gets the zero model (no votes). */
+
+/* rmf::PtPair (RansacMatchFilter.cuh:20-24): left and right point of a match, 16-byte aligned. */
+typedef struct rsfm_pt_pair {
+    float lx, ly, rx, ry;
+} rsfm_pt_pair;
+
+/* One image pair for the device filter. matches: sorted by cell (cell of the left point);
+ * bounds[cols * rows + 1]: first match of each cell; votes: 4-byte aligned, nbMatches rounded
+ * up to a multiple of 4 bytes (one u8 per match); affineScratch: cols * rows x 6 floats.
+ * threshold: in pixels (cell width x relative threshold). All device memory. */
+typedef struct rsfm_ransac_task {
+    uint8_t* votes;
+    float* affineScratch;
+    const rsfm_pt_pair* matches;
+    const uint32_t* bounds;
+    uint32_t nbMatches, cols, rows;
+    float threshold;
+} rsfm_ransac_task;
+
+/* Replaces rmf::cudaRansacMatchFilter (RansacMatchFilter.cuh:27-34, .cu:393-419), plus `seed`.
+ * Fewer than 16 matches: votes are all zero. */
+int rsfm_ransac_match_filter(uint8_t* votes, float* affineScratch, const rsfm_pt_pair* matches, uint32_t nbMatches,
+                             const uint32_t* bounds, uint32_t cols, uint32_t rows, uint32_t nbRansacTests,
+                             float threshold, int tryOtherSolutions, uint32_t seed, cudaStream_t stream);
+
+/* Many image pairs in one launch per kernel (no reference counterpart; the reference launches per
+ * pair). */
+int rsfm_ransac_match_filter_batch(const rsfm_ransac_task* tasks, size_t nbTasks, uint32_t nbRansacTests,
+                                   int tryOtherSolutions, uint32_t seed, cudaStream_t stream);
+
+/* Replaces RansacMatchFilter::getInlierMask (RansacMatchFilter.h:33, .cpp:40-134): host matches
+ * in, host mask out (mask[n] = 1 when match n has >= minVotes votes). Bins the matches by cell
+ * on the host as the reference does (cell width = ceil(max(w, h) / cellCols), cell index from
+ * ceil(point / cell width), clamped), runs the device filter and synchronizes `stream`. */
+int rsfm_ransac_inlier_mask(int imgWidth, int imgHeight, const rsfm_pt_pair* matches, uint32_t nbMatches,
+                            uint32_t minVotes, uint32_t nbRansacTests, float relativeThreshold, uint32_t cellCols,
+                            int tryOtherAffines, uint32_t seed, uint8_t* mask, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- cascade hash
  * Descriptors are nbDesc x 128 uint8, 16-byte aligned. Weights are nbChannels x 128 int8 rows
  * (the reference's KArray<int32_t, 32> per channel), 16-byte aligned; 64 channels give the 8

@@ -46,6 +46,8 @@ def load():
         "orc_cashash_build_buckets": (None, [_P, u32, _P, _P]),
         "orc_cashash_find_best_match": (None, [_P, u32, _P, _P, _P, u32, _P, _P, _P, _P, ctypes.c_int]),
         "orc_cashash_match_ranked": (None, [_P, _P, _P, u32, _P, _P, _P, u32, i32, i32, u32, u32, _P, _P, _P, _P]),
+        "orc_ransac_models": (None, [_P, _P, u32, u32, u32, ctypes.c_float, u32, _P]),
+        "orc_ransac_votes": (None, [_P, u32, _P, u32, u32, _P, ctypes.c_float, ctypes.c_int, _P]),
         "orc_mlp_forward": (None, [_P, _P, _P, _P, _P, u32, _P, _P]),
         "orc_mlp_triplet_grad": (ctypes.c_double, [_P, _P, _P, _P, _P, _P, _P, u32, ctypes.c_float, _P, _P, _P, _P]),
         "orc_mlp_loss_grad": (ctypes.c_double, [_P, _P, _P, _P, _P, _P, _P, u32, ctypes.c_float, ctypes.c_int,
@@ -267,6 +269,53 @@ def mlp_triplet_grad(params, a, p, n, margin, kind=0, lam=0.0):
 
 # ---------------------------------------------------------------- reference kernels (GPU)
 REF_LIB_PATH = os.path.join(HERE, "_ref", "librsfm_ref.so")
+def ransac_bin(width, height, pairs, cell_cols=16):
+    """RansacMatchFilter.cpp:40-66: cell grid and stable cell-by-cell order of the matches.
+    pairs: float32 [n, 4] (lx, ly, rx, ry). Returns (sorted pairs, bounds, flat, cols, rows, cell_width)
+    with sorted[k] = pairs[flat[k]]."""
+    pairs = np.ascontiguousarray(pairs, dtype=np.float32)
+    cw = -(-max(width, height) // cell_cols)
+    cols, rows = -(-width // cw), -(-height // cw)
+    fcw = np.float32(cw)
+    y = np.ceil(pairs[:, 1] / fcw)
+    x = np.ceil(pairs[:, 0] / fcw)
+    i = np.minimum(np.maximum(y, np.float32(0)), np.float32(rows - 1)).astype(np.uint32)
+    j = np.minimum(np.maximum(x, np.float32(0)), np.float32(cols - 1)).astype(np.uint32)
+    cell = i * np.uint32(cols) + j
+    flat = np.argsort(cell, kind="stable").astype(np.uint32)
+    bounds = np.zeros(cols * rows + 1, dtype=np.uint32)
+    bounds[1:] = np.cumsum(np.bincount(cell, minlength=cols * rows))
+    return np.ascontiguousarray(pairs[flat]), bounds, flat, cols, rows, cw
+
+
+def ransac_votes(sorted_pairs, bounds, cols, rows, n_tests, threshold, try_other, seed):
+    """Per-cell models and votes of the filter (RansacMatchFilter.cu:196-389), seeded.
+    Returns (affines [cells, 6] float32, votes [n] uint8); fewer than 16 matches: zero votes."""
+    sorted_pairs = np.ascontiguousarray(sorted_pairs, dtype=np.float32)
+    bounds = np.ascontiguousarray(bounds, dtype=np.uint32)
+    n = len(sorted_pairs)
+    aff = np.zeros((cols * rows, 6), dtype=np.float32)
+    votes = np.zeros(n, dtype=np.uint8)
+    if n < 16:
+        return aff, votes
+    lib = load()
+    lib.orc_ransac_models(_c(sorted_pairs), _c(bounds), cols, rows, n_tests, float(threshold), seed, _c(aff))
+    lib.orc_ransac_votes(_c(sorted_pairs), n, _c(bounds), cols, rows, _c(aff), float(threshold), int(try_other),
+                         _c(votes))
+    return aff, votes
+
+
+def ransac_inlier_mask(width, height, pairs, min_votes=2, n_tests=256, rel_threshold=0.15, cell_cols=16,
+                       try_other=False, seed=0):
+    """RansacMatchFilter::getInlierMask (RansacMatchFilter.cpp:40-134) with a seed."""
+    sp, bounds, flat, cols, rows, cw = ransac_bin(width, height, pairs, cell_cols)
+    _, votes = ransac_votes(sp, bounds, cols, rows, n_tests, np.float32(cw) * np.float32(rel_threshold), try_other,
+                            seed)
+    mask = np.zeros(len(pairs), dtype=bool)
+    mask[flat] = votes >= min_votes
+    return mask
+
+
 _ref = None
 
 

@@ -31,6 +31,20 @@ class BestMatch(ctypes.Structure):
     _fields_ = [("index", ctypes.c_uint32), ("distance", ctypes.c_uint32)]
 
 
+class RansacTask(ctypes.Structure):
+    """rsfm_ransac_task (one image pair for the device RANSAC filter)."""
+    _fields_ = [
+        ("votes", ctypes.c_void_p),
+        ("affineScratch", ctypes.c_void_p),
+        ("matches", ctypes.c_void_p),
+        ("bounds", ctypes.c_void_p),
+        ("nbMatches", ctypes.c_uint32),
+        ("cols", ctypes.c_uint32),
+        ("rows", ctypes.c_uint32),
+        ("threshold", ctypes.c_float),
+    ]
+
+
 class SiftBFTask(ctypes.Structure):
     """SiftBruteForceMatchTask (bruteForceMatch.h:96-112)."""
     _fields_ = [
@@ -92,6 +106,14 @@ SIGNATURES = {
                                                        ctypes.c_void_p]),
     "rsfm_remove_match_conflicts_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
                                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_ransac_match_filter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                                ctypes.c_float, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_ransac_match_filter_batch": (ctypes.c_int, [ctypes.POINTER(RansacTask), ctypes.c_size_t, ctypes.c_uint32,
+                                                      ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_ransac_inlier_mask": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
+                                               ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_match_idp": (ctypes.c_int, [ctypes.POINTER(SiftBFTask), ctypes.c_size_t, ctypes.c_void_p]),
     "rsfm_sift_desc_8b_to_4b": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_precomp_sift4b_sqr_norm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,

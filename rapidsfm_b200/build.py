@@ -19,6 +19,7 @@ SOURCES = [
     "bf_match_noalloc.cu",
     "bf_variants.cu",
     "filters.cu",
+    "ransac.cu",
     "bf_autotune.cpp",
     "host_filters.cpp",
     "diag.cu",

@@ -63,3 +63,28 @@ def make_pair_torch(n_query, n_train, overlap, sigma, gen, device="cuda"):
     truth = torch.cat([src, torch.full((n_train - n_copy,), -1, dtype=torch.int64, device=device)])
     perm = torch.randperm(n_train, generator=gen, device=device)
     return q, t[perm].contiguous(), truth[perm]
+
+
+def make_ransac_matches(n, width=1600, height=1200, inlier_frac=0.7, noise=1.0, seed=0, cluster=None):
+    """Synthetic point matches for the RANSAC match filter: float32 [n, 4] (lx, ly, rx, ry) and the
+    true inlier mask. Inliers follow a smooth warp (similarity plus a gentle perspective bend) with
+    Gaussian noise; outliers have uniform random right points. cluster=(x, y, r): left points
+    drawn in that disc instead of the whole image (dense cells)."""
+    rng = np.random.default_rng(seed)
+    if cluster is None:
+        left = rng.uniform((0, 0), (width, height), (n, 2))
+    else:
+        cx, cy, r = cluster
+        ang = rng.uniform(0, 2 * np.pi, n)
+        rad = r * np.sqrt(rng.uniform(0, 1, n))
+        left = np.stack([cx + rad * np.cos(ang), cy + rad * np.sin(ang)], 1)
+    th = np.deg2rad(rng.uniform(-15, 15))
+    s = rng.uniform(0.8, 1.25)
+    R = s * np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    t = rng.uniform(-100, 100, 2)
+    c = left - (width / 2, height / 2)
+    bend = 1.0 + 2e-5 * (c[:, :1] * rng.uniform(-1, 1) + c[:, 1:] * rng.uniform(-1, 1))
+    right = (c @ R.T) / bend + (width / 2, height / 2) + t + rng.normal(0, noise, (n, 2))
+    inl = rng.uniform(0, 1, n) < inlier_frac
+    right[~inl] = rng.uniform((0, 0), (width, height), ((~inl).sum(), 2))
+    return np.concatenate([left, right], 1).astype(np.float32), inl
