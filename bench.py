@@ -402,6 +402,7 @@ def run_ours(args):
         extras["batched"] = run_batched(dev, stream)
         extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
         extras["hash"] = run_hash(dev, stream, n=1 << args.hash_log2)
+        extras["ransac"] = run_ransac(dev, stream)
 
     line = {
         "metric": METRIC,
@@ -673,6 +674,44 @@ def run_hash(dev, stream, n=1 << 24):
     return out
 
 
+def run_ransac(dev, stream, n_pairs=1000, n=4000, seed=6, cpu_pairs=8):
+    """RANSAC match filter (the step after matching) on n_pairs image pairs of n matches each
+    (1600x1200, 60 % inliers, 16 cell columns, 256 tests, tryOtherAffines as in the reference's
+    default config): all pairs in one batched device call vs one call per pair; the CPU oracle
+    (one thread) on a sample of pairs beside it. Work unit: inlier tests (one affine applied to one
+    match), counted from the cell bounds."""
+    import torch
+    from oracle import oracle as orc  # CPU comparison leg only
+    from rapidsfm_b200 import ransac, synth
+    rng = np.random.default_rng(seed)
+    tasks, host, tests = [], [], 0
+    for k in range(n_pairs):
+        pairs, _ = synth.make_ransac_matches(n, inlier_frac=0.6, seed=int(rng.integers(1 << 30)))
+        sp, bounds, _, cols, rows, cw = ransac.bin_matches(1600, 1200, pairs)
+        thr = float(np.float32(cw) * np.float32(0.15))
+        votes, aff = ransac.device_buffers(n, cols, rows, device=dev)
+        tasks.append(dict(votes=votes, affines=aff, matches=torch.from_numpy(sp).to(dev),
+                          bounds=torch.from_numpy(bounds.view(np.int32)).to(dev), cols=cols, rows=rows, threshold=thr))
+        if k < cpu_pairs:
+            host.append((sp, bounds, cols, rows, thr))
+        padded = np.pad(np.diff(bounds).astype(np.int64).reshape(rows, cols), 1)
+        hood = sum(padded[dy:dy + rows, dx:dx + cols] for dy in range(3) for dx in range(3)).ravel()
+        tests += int((hood[hood >= 9] * 256).sum() + hood.sum() * cols * rows + hood.sum())
+    batch_ms = _events_ms(lambda: ransac.ransac_match_filter_batch(tasks, try_other=True, seed=1, stream=stream), 5,
+                          stream)
+    single_ms = _events_ms(lambda: [ransac.ransac_match_filter(t["votes"], t["affines"], t["matches"], t["bounds"],
+                                                               t["cols"], t["rows"], 256, t["threshold"], True, 1,
+                                                               stream) for t in tasks[:100]], 3, stream) * n_pairs / 100
+    t0 = time.perf_counter()
+    for sp, bounds, cols, rows, thr in host:
+        orc.ransac_votes(sp, bounds, cols, rows, 256, thr, True, 1)
+    cpu_s = (time.perf_counter() - t0) / len(host)
+    return {"pairs": n_pairs, "matches_per_pair": n, "batched_ms": batch_ms,
+            "pairs_per_s": n_pairs / (batch_ms * 1e-3), "one_call_per_pair_ms": single_ms,
+            "inlier_tests_per_s": tests / (batch_ms * 1e-3),
+            "cpu_oracle_1_thread_pairs_per_s": 1.0 / cpu_s, "cpu_sample_pairs": len(host)}
+
+
 def R_lib():
     from rapidsfm_b200 import _lib
     return _lib.load()
@@ -688,8 +727,17 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and cascade-hash sections")
     ap.add_argument("--cascade-pairs", type=int, default=1000)
     ap.add_argument("--only-hash", action="store_true", help="run the hashing-throughput section alone (profiling)")
+    ap.add_argument("--only-ransac", action="store_true", help="run the RANSAC-filter section alone (profiling)")
+    ap.add_argument("--ransac-pairs", type=int, default=1000)
     ap.add_argument("--hash-log2", type=int, default=24, help="log2 of the descriptors in the hashing section")
     args = ap.parse_args()
+    if args.only_ransac:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"ransac": run_ransac(dev, torch.cuda.current_stream(dev), n_pairs=args.ransac_pairs)}),
+              flush=True)
+        return
     if args.only_hash:
         import torch
         dev = torch.device("cuda", 0)

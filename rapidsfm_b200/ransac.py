@@ -17,6 +17,24 @@ from . import _lib
 from .matcher import _ptr, _stream_ptr
 
 
+def bin_matches(width, height, matches, cell_cols=16):
+    """Cell grid and stable cell-by-cell order of the matches, as RansacMatchFilter.cpp:40-66
+    (cell width = ceil(max(w, h) / cellCols); cell = clamp(ceil(left point / cell width))).
+    Returns (sorted float32 [n, 4], bounds uint32 [cells + 1], order, cols, rows, cell_width) with
+    sorted[k] = matches[order[k]]."""
+    m = np.ascontiguousarray(matches, dtype=np.float32).reshape(-1, 4)
+    cw = -(-max(width, height) // cell_cols)
+    cols, rows = -(-width // cw), -(-height // cw)
+    f = np.float32(cw)
+    i = np.minimum(np.maximum(np.ceil(m[:, 1] / f), np.float32(0)), np.float32(rows - 1)).astype(np.uint32)
+    j = np.minimum(np.maximum(np.ceil(m[:, 0] / f), np.float32(0)), np.float32(cols - 1)).astype(np.uint32)
+    cell = i * np.uint32(cols) + j
+    order = np.argsort(cell, kind="stable").astype(np.uint32)
+    bounds = np.zeros(cols * rows + 1, dtype=np.uint32)
+    bounds[1:] = np.cumsum(np.bincount(cell, minlength=cols * rows))
+    return np.ascontiguousarray(m[order]), bounds, order, cols, rows, cw
+
+
 def ransac_match_filter(votes, affines, matches, bounds, cols, rows, n_tests=256, threshold=15.0,
                         try_other=True, seed=0, stream=None):
     """Device filter on one image pair: matches (float32 [n, 4], sorted by cell), bounds

@@ -41,3 +41,14 @@ def test_filter_is_seeded_and_small_inputs_vote_nothing(oracle):
     assert v1.max() <= 9
     _, v = oracle.ransac_votes(sp[:15], np.minimum(b, 15), cols, rows, 256, cw * 0.15, True, 5)
     assert v.sum() == 0
+
+
+def test_product_binning_equals_oracle(oracle):
+    from rapidsfm_b200 import ransac
+    pairs, _ = synth.make_ransac_matches(3000, seed=8)
+    pairs[:5, :2] = [[0, 0], [1600, 1200], [-1, -1], [100, 99.99], [1e6, 3]]
+    for cell_cols in (16, 7):
+        got = ransac.bin_matches(1600, 1200, pairs, cell_cols)
+        exp = oracle.ransac_bin(1600, 1200, pairs, cell_cols)
+        for g, e in zip(got, exp):
+            np.testing.assert_array_equal(np.asarray(g), np.asarray(e))
