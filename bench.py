@@ -727,6 +727,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and cascade-hash sections")
     ap.add_argument("--cascade-pairs", type=int, default=1000)
     ap.add_argument("--only-hash", action="store_true", help="run the hashing-throughput section alone (profiling)")
+    ap.add_argument("--only-cascade", action="store_true", help="run the cascade-hash section alone (profiling)")
     ap.add_argument("--only-ransac", action="store_true", help="run the RANSAC-filter section alone (profiling)")
     ap.add_argument("--ransac-pairs", type=int, default=1000)
     ap.add_argument("--hash-log2", type=int, default=24, help="log2 of the descriptors in the hashing section")
@@ -736,6 +737,13 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"ransac": run_ransac(dev, torch.cuda.current_stream(dev), n_pairs=args.ransac_pairs)}),
+              flush=True)
+        return
+    if args.only_cascade:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"cascade": run_cascade(dev, torch.cuda.current_stream(dev), n_pairs=args.cascade_pairs)}),
               flush=True)
         return
     if args.only_hash:
