@@ -16,8 +16,9 @@
 // seeds from clock(), so its output is not reproducible); a cell whose neighbourhood holds fewer
 // than 9 matches gets the zero model (the reference leaves its scratch slot unwritten); the 3x3
 // solve is Gaussian elimination with partial pivoting (the reference's solveGaussElim lives in
-// the missing cuda-utils submodule). Every float operation is written out in a fixed order and
-// built with -ffp-contract=off so the CUDA kernels (explicit _rn intrinsics) match bit for bit.
+// the missing cuda-utils submodule). Every float operation is written out in a fixed order
+// (std::fma where the kernels fuse) and built with -ffp-contract=off, so the CUDA kernels
+// (explicit _rn intrinsics) match bit for bit.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -84,10 +85,11 @@ float sqr_threshold(const Aff& t, float threshold) {
     return v * v;
 }
 
+// Fused multiply-adds (std::fma rounds once, as the GPU's FMA does), in the kernels' order.
 bool inlier(const Aff& t, const Pt& p, float sqrThr) {
-    const float dx = ((t.a[0] * p.lx + t.a[1] * p.ly) + t.a[2]) - p.rx;
-    const float dy = ((t.a[3] * p.lx + t.a[4] * p.ly) + t.a[5]) - p.ry;
-    return dx * dx + dy * dy < sqrThr;
+    const float dx = std::fma(t.a[0], p.lx, std::fma(t.a[1], p.ly, t.a[2])) - p.rx;
+    const float dy = std::fma(t.a[3], p.lx, std::fma(t.a[4], p.ly, t.a[5])) - p.ry;
+    return std::fma(dx, dx, dy * dy) < sqrThr;
 }
 
 struct Hood {

@@ -16,7 +16,8 @@
 // seeds from clock() and leaves some scratch unwritten): the seed is a parameter, and a cell whose
 // neighbourhood has fewer than 9 matches gets the zero model, which never has inliers. The 3x3
 // solve is Gaussian elimination with partial pivoting. All float arithmetic uses explicit
-// round-to-nearest intrinsics in a fixed order, so results are reproducible bit for bit.
+// round-to-nearest intrinsics (fused multiply-adds in the inlier test) in a fixed order, so
+// results are reproducible bit for bit.
 //
 // B200 mapping: one launch per kernel for a whole batch of image pairs (grid = cells x pairs),
 // 128 threads per cell; the neighbourhood's matches are staged in shared memory once and read as
@@ -67,10 +68,12 @@ __device__ __forceinline__ float sqr_threshold(const Aff& t, float threshold) {
     return __fmul_rn(v, v);
 }
 
+// |A l + t - r|^2 < thr with fused multiply-adds in a fixed order (the oracle uses std::fma, which
+// rounds once like the hardware FMA): 8 FP32 instructions per test.
 __device__ __forceinline__ bool inlier(const Aff& t, float4 p, float thr) {
-    const float dx = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(t.a[0], p.x), __fmul_rn(t.a[1], p.y)), t.a[2]), p.z);
-    const float dy = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(t.a[3], p.x), __fmul_rn(t.a[4], p.y)), t.a[5]), p.w);
-    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) < thr;
+    const float dx = __fsub_rn(__fmaf_rn(t.a[0], p.x, __fmaf_rn(t.a[1], p.y, t.a[2])), p.z);
+    const float dy = __fsub_rn(__fmaf_rn(t.a[3], p.x, __fmaf_rn(t.a[4], p.y, t.a[5])), p.w);
+    return __fmaf_rn(dx, dx, __fmul_rn(dy, dy)) < thr;
 }
 
 __device__ Aff solve3(const float4 (&p)[3]) {
