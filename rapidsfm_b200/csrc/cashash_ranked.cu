@@ -11,6 +11,8 @@
 // with the running top-K when a query has more candidates than the buffer holds.
 #include "common.h"
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 namespace rsfm_b200 {
@@ -329,6 +331,138 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
     }
 }
 
+// ---------------------------------------------------------------- one thread per query
+// The same matching with one query per thread (for topK <= kThreadTopK): the candidate walk,
+// duplicate test and Hamming key are per-thread scalar work with no cross-lane traffic, the
+// running top-K is a sorted register list (one compare-exchange pass per insertion; keys past
+// the kThreadTopK-th are rejected by one compare), and the re-rank reads each ranked train
+// descriptor as eight 16-byte loads. Results are identical to the warp kernel: same keys, same
+// set of the topK smallest, same exact re-rank rule.
+constexpr int kThreadTopK = 16;
+constexpr int kThreadBlock = 128;
+
+__device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
+                                                   uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
+                                                   const Out& O) {
+    const uint2 qk = __ldg(&Q.keys[i]);
+    const uint4 qc = __ldg(&Q.codes[i]);
+    uint32_t top[kThreadTopK];
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
+    uint32_t total = 0;
+    for (uint32_t s = 0; s < tables; ++s) {
+        const uint32_t bk = ((s < 4 ? qk.x : qk.y) >> (8 * (s & 3u))) & 0xFFu;
+        const uint32_t lo = bk ? __ldg(&T.ends[s * 256 + bk - 1]) : 0u;
+        const uint32_t hi = __ldg(&T.ends[s * 256 + bk]);
+        const uint32_t* list = T.buckets + size_t(s) * T.n;
+        // four candidates per step: their list entries, then their records, loaded together
+        for (uint32_t x = lo; x < hi; x += 4) {
+            uint32_t j[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) j[u] = x + u < hi ? __ldg(&list[x + u]) : 0xFFFFFFFFu;
+            uint2 tk[4];
+            uint4 tc[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (j[u] == 0xFFFFFFFFu) {
+                    tk[u] = make_uint2(0, 0);
+                    tc[u] = make_uint4(0, 0, 0, 0);
+                } else if (T.rec) {
+                    const uint4 r0 = __ldg(&T.rec[2 * size_t(j[u])]), r1 = __ldg(&T.rec[2 * size_t(j[u]) + 1]);
+                    tk[u] = make_uint2(r0.x, r0.y);
+                    tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
+                } else {
+                    tk[u] = __ldg(&T.keys[j[u]]);
+                    tc[u] = __ldg(&T.codes[j[u]]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (j[u] == 0xFFFFFFFFu || collides_before(tk[u], qk, s)) continue;
+                ++total;
+                const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
+                                   __popc(tc[u].w ^ qc.w);
+                uint32_t key = (h << 24) | j[u];
+                if (key < top[kThreadTopK - 1]) {
+#pragma unroll
+                    for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
+                        const uint32_t a = top[r];
+                        top[r] = min(a, key);
+                        key = max(a, key);
+                    }
+                }
+            }
+        }
+    }
+    // exact L2 of the topK best-ranked candidates
+    const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
+    uint4 q[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) q[k] = __ldg(&qd[k]);
+    const uint32_t nq = __ldg(&Q.sqr[i]);
+    uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) {
+        if (uint32_t(r) >= topK || top[r] == 0xFFFFFFFFu) continue;
+        const uint32_t jr = top[r] & 0xFFFFFFu;
+        const uint4* td = reinterpret_cast<const uint4*>(T.desc + size_t(jr) * 128);
+        uint32_t dot = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint4 t = __ldg(&td[k]);
+            dot = __dp4a(q[k].x, t.x, dot);
+            dot = __dp4a(q[k].y, t.y, dot);
+            dot = __dp4a(q[k].z, t.z, dot);
+            dot = __dp4a(q[k].w, t.w, dot);
+        }
+        const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
+        const uint32_t d = nq + ns - 2u * dot;
+        if (d < bd || (d == bd && jr < bj)) {
+            sd = bd;
+            bd = d;
+            bj = jr;
+        } else if (d < sd) {
+            sd = d;
+        }
+    }
+    O.best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
+    O.second[i] = sd;
+    uint32_t f = 0;
+    if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+    O.flags[i] = f;
+    if (O.nbCand) O.nbCand[i] = total;
+}
+
+__global__ void __launch_bounds__(kThreadBlock, 4) ranked_thread_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
+                                                                      uint32_t ratioNum, uint32_t ratioDen, Out O) {
+    const uint32_t i = blockIdx.x * kThreadBlock + threadIdx.x;
+    if (i < Q.n) match_query_thread(Q, T, i, tables, topK, ratioNum, ratioDen, O);
+}
+
+__global__ void __launch_bounds__(kThreadBlock, 4) ranked_thread_batch_kernel(
+    const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
+    uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
+    const uint32_t g = blockIdx.x * kThreadBlock + threadIdx.x;
+    if (g >= total) return;
+    uint32_t lo = 0, hi = nPairs - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&begin[mid]) <= g) lo = mid; else hi = mid - 1;
+    }
+    const PairDev& P = pairs[lo];
+    match_query_thread(P.q, P.t, g - __ldg(&begin[lo]), tables, topK, ratioNum, ratioDen, P.o);
+}
+
+// Kernel choice: one thread per query when topK fits the register list, unless
+// RSFM_RANKED_KERNEL=warp asks for the warp-per-query kernel.
+inline bool use_thread_kernel(uint32_t topK) {
+    static const int forced = [] {
+        const char* e = std::getenv("RSFM_RANKED_KERNEL");
+        return e && std::string(e) == "warp" ? 1 : 0;
+    }();
+    return !forced && topK <= uint32_t(kThreadTopK);
+}
+
 }  // namespace chr
 }  // namespace rsfm_b200
 
@@ -360,11 +494,16 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     if (!Q.desc || !Q.keys || !Q.codes || !Q.sqr) return RSFM_ERR_INVALID_ARG;
     if (train->nbDesc && (!T.desc || !T.keys || !T.codes || !T.ends || !T.buckets || !T.sqr))
         return RSFM_ERR_INVALID_ARG;
-    const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
     const chr::Out O{reinterpret_cast<unsigned long long*>(best), secondDist, flags, nbCandidates};
-    chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+    if (chr::use_thread_kernel(topK)) {
+        const uint32_t grid = (Q.n + chr::kThreadBlock - 1) / chr::kThreadBlock;
+        chr::ranked_thread_kernel<<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+    } else {
+        const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
+        chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+    }
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);
     launch_count_add(1);
@@ -448,11 +587,17 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
     launch_count_reset();
     if (!b) return RSFM_ERR_INVALID_ARG;
     if (b->total == 0) return RSFM_OK;
-    const uint32_t grid = std::min<uint32_t>((b->total + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
-    chr::ranked_batch_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total,
-                                                                   b->tables, b->topK, b->ratioNum, b->ratioDen);
+    if (chr::use_thread_kernel(b->topK)) {
+        const uint32_t grid = (b->total + chr::kThreadBlock - 1) / chr::kThreadBlock;
+        chr::ranked_thread_batch_kernel<<<grid, chr::kThreadBlock, 0, stream>>>(
+            b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
+    } else {
+        const uint32_t grid = std::min<uint32_t>((b->total + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
+        chr::ranked_batch_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total,
+                                                                       b->tables, b->topK, b->ratioNum, b->ratioDen);
+    }
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);
     launch_count_add(1);
