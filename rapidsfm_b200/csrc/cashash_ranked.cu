@@ -159,7 +159,7 @@ __device__ __forceinline__ void match_query(const Img& Q, const Img& T, uint32_t
     // Bucket ranges of all tables at once (lane s holds table s), then one flattened pass over
     // the concatenated member lists: lane l takes candidate base + l wherever it falls.
     uint32_t myLo = 0, mySize = 0;
-    if (lane < tables) {
+    if (lane < tables && T.n) {  // an empty train image has no tables
         const uint32_t bk = lane < 4 ? (qk.x >> (8 * lane)) & 0xFFu : (qk.y >> (8 * (lane - 4))) & 0xFFu;
         myLo = bk ? __ldg(&T.ends[lane * 256 + bk - 1]) : 0u;
         mySize = __ldg(&T.ends[lane * 256 + bk]) - myLo;
@@ -332,14 +332,15 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
 }
 
 // ---------------------------------------------------------------- one thread per query
-// The same matching with one query per thread (for topK <= kThreadTopK): the candidate walk,
+// The same matching with one query per thread (for topK <= kThreadTopK = 12): the candidate walk,
 // duplicate test and Hamming key are per-thread scalar work with no cross-lane traffic, the
 // running top-K is a sorted register list (one compare-exchange pass per insertion; keys past
 // the kThreadTopK-th are rejected by one compare), and the re-rank reads each ranked train
 // descriptor as eight 16-byte loads. Results are identical to the warp kernel: same keys, same
 // set of the topK smallest, same exact re-rank rule.
-constexpr int kThreadTopK = 16;
+constexpr int kThreadTopK = 12;
 constexpr int kThreadBlock = 128;
+constexpr int kThreadMinBlocks = 6;  // 80 registers, 24 warps per SM
 
 __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
                                                    uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
@@ -350,55 +351,64 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
 #pragma unroll
     for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
     uint32_t total = 0;
-    for (uint32_t s = 0; s < tables; ++s) {
-        const uint32_t bk = ((s < 4 ? qk.x : qk.y) >> (8 * (s & 3u))) & 0xFFu;
-        const uint32_t lo = bk ? __ldg(&T.ends[s * 256 + bk - 1]) : 0u;
-        const uint32_t hi = __ldg(&T.ends[s * 256 + bk]);
-        const uint32_t* list = T.buckets + size_t(s) * T.n;
-        // four candidates per step: their list entries, then their records, loaded together
-        for (uint32_t x = lo; x < hi; x += 4) {
-            uint32_t j[4];
+    // One walk over the concatenated bucket lists of all tables (a cursor that moves to the next
+    // table when a list ends), four candidates per step, so the threads of a warp stay together
+    // across table boundaries. An empty train image has no tables.
+    const uint32_t nt = T.n ? tables : 0u;
+    uint32_t s = 0, x = 0, hi = 0;
+    auto open_table = [&](uint32_t t) {
+        const uint32_t bk = ((t < 4 ? qk.x : qk.y) >> (8 * (t & 3u))) & 0xFFu;
+        x = bk ? __ldg(&T.ends[t * 256 + bk - 1]) : 0u;
+        hi = __ldg(&T.ends[t * 256 + bk]);
+    };
+    if (nt) open_table(0);
+    for (;;) {
+        uint32_t j[4], su[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) j[u] = x + u < hi ? __ldg(&list[x + u]) : 0xFFFFFFFFu;
-            uint2 tk[4];
-            uint4 tc[4];
+        for (int u = 0; u < 4; ++u) {
+            while (x == hi && s + 1 < nt) open_table(++s);
+            su[u] = s;
+            j[u] = x < hi ? __ldg(&T.buckets[size_t(s) * T.n + x++]) : 0xFFFFFFFFu;
+        }
+        if (j[0] == 0xFFFFFFFFu) break;
+        uint2 tk[4];
+        uint4 tc[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (j[u] == 0xFFFFFFFFu) {
-                    tk[u] = make_uint2(0, 0);
-                    tc[u] = make_uint4(0, 0, 0, 0);
-                } else if (T.rec) {
-                    const uint4 r0 = __ldg(&T.rec[2 * size_t(j[u])]), r1 = __ldg(&T.rec[2 * size_t(j[u]) + 1]);
-                    tk[u] = make_uint2(r0.x, r0.y);
-                    tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
-                } else {
-                    tk[u] = __ldg(&T.keys[j[u]]);
-                    tc[u] = __ldg(&T.codes[j[u]]);
-                }
+        for (int u = 0; u < 4; ++u) {
+            if (j[u] == 0xFFFFFFFFu) {
+                tk[u] = make_uint2(0, 0);
+                tc[u] = make_uint4(0, 0, 0, 0);
+            } else if (T.rec) {
+                const uint4 r0 = __ldg(&T.rec[2 * size_t(j[u])]), r1 = __ldg(&T.rec[2 * size_t(j[u]) + 1]);
+                tk[u] = make_uint2(r0.x, r0.y);
+                tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
+            } else {
+                tk[u] = __ldg(&T.keys[j[u]]);
+                tc[u] = __ldg(&T.codes[j[u]]);
             }
+        }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (j[u] == 0xFFFFFFFFu || collides_before(tk[u], qk, s)) continue;
-                ++total;
-                const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
-                                   __popc(tc[u].w ^ qc.w);
-                uint32_t key = (h << 24) | j[u];
-                if (key < top[kThreadTopK - 1]) {
+        for (int u = 0; u < 4; ++u) {
+            if (j[u] == 0xFFFFFFFFu || collides_before(tk[u], qk, su[u])) continue;
+            ++total;
+            const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
+                               __popc(tc[u].w ^ qc.w);
+            uint32_t key = (h << 24) | j[u];
+            if (key < top[kThreadTopK - 1]) {
 #pragma unroll
-                    for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
-                        const uint32_t a = top[r];
-                        top[r] = min(a, key);
-                        key = max(a, key);
-                    }
+                for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
+                    const uint32_t a = top[r];
+                    top[r] = min(a, key);
+                    key = max(a, key);
                 }
             }
         }
     }
     // exact L2 of the topK best-ranked candidates
     const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
-    uint4 q[8];
+    uint4 qr[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) q[k] = __ldg(&qd[k]);
+    for (int k = 0; k < 8; ++k) qr[k] = __ldg(&qd[k]);
     const uint32_t nq = __ldg(&Q.sqr[i]);
     uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
 #pragma unroll
@@ -409,11 +419,11 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
         uint32_t dot = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint4 t = __ldg(&td[k]);
-            dot = __dp4a(q[k].x, t.x, dot);
-            dot = __dp4a(q[k].y, t.y, dot);
-            dot = __dp4a(q[k].z, t.z, dot);
-            dot = __dp4a(q[k].w, t.w, dot);
+            const uint4 t = __ldg(&td[k]), q = qr[k];
+            dot = __dp4a(q.x, t.x, dot);
+            dot = __dp4a(q.y, t.y, dot);
+            dot = __dp4a(q.z, t.z, dot);
+            dot = __dp4a(q.w, t.w, dot);
         }
         const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
         const uint32_t d = nq + ns - 2u * dot;
@@ -433,24 +443,34 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
     if (O.nbCand) O.nbCand[i] = total;
 }
 
-__global__ void __launch_bounds__(kThreadBlock, 4) ranked_thread_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
+__global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
                                                                       uint32_t ratioNum, uint32_t ratioDen, Out O) {
-    const uint32_t i = blockIdx.x * kThreadBlock + threadIdx.x;
-    if (i < Q.n) match_query_thread(Q, T, i, tables, topK, ratioNum, ratioDen, O);
+    const uint32_t t = blockIdx.x * kThreadBlock + threadIdx.x;
+    if (t < Q.n) match_query_thread(Q, T, Q.buckets ? __ldg(&Q.buckets[t]) : t, tables, topK, ratioNum, ratioDen, O);
 }
 
-__global__ void __launch_bounds__(kThreadBlock, 4) ranked_thread_batch_kernel(
-    const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
-    uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
-    const uint32_t g = blockIdx.x * kThreadBlock + threadIdx.x;
-    if (g >= total) return;
+__device__ __forceinline__ uint32_t pair_of(const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t g) {
     uint32_t lo = 0, hi = nPairs - 1;
     while (lo < hi) {
         const uint32_t mid = (lo + hi + 1) >> 1;
         if (__ldg(&begin[mid]) <= g) lo = mid; else hi = mid - 1;
     }
-    const PairDev& P = pairs[lo];
-    match_query_thread(P.q, P.t, g - __ldg(&begin[lo]), tables, topK, ratioNum, ratioDen, P.o);
+    return lo;
+}
+
+__global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_batch_kernel(
+    const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
+    uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
+    const uint32_t g = blockIdx.x * kThreadBlock + threadIdx.x;
+    if (g >= total) return;
+    const uint32_t p = pair_of(begin, nPairs, g);
+    const PairDev& P = pairs[p];
+    uint32_t i = g - __ldg(&begin[p]);
+    // Queries in the order of the query image's first-table bucket lists (when it has them):
+    // neighbouring threads then share their first table's candidate list, walk it in step and
+    // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
+    if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
+    match_query_thread(P.q, P.t, i, tables, topK, ratioNum, ratioDen, P.o);
 }
 
 // Kernel choice: one thread per query when topK fits the register list, unless
