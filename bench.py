@@ -586,7 +586,7 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
         torch.cuda.synchronize()
         hash_s = time.perf_counter() - t0
         rows = {}
-        for tables in (2, 3, 4, 6):
+        for tables in (2, 3, 4, 6, 8):
             batch = ch.RankedBatch(ranked, tables, 10)
             ms = _events_ms(lambda: batch.launch(stream), 3, stream)
             hit = torch.zeros((), dtype=torch.int64, device=dev)
@@ -617,6 +617,14 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
         p6 = out["plain"]["tables"]["6"]
         ok = [v for v in out["learned"]["tables"].values() if v["recall"] >= p6["recall"]]
         out["learned_speedup_at_plain_recall"] = (p6["match_ms"] / min(v["match_ms"] for v in ok)) if ok else None
+
+        def at98(name):
+            t = out[name]["fewest_tables_at_98pct_recall"]
+            return out[name]["tables"][str(t)]["match_ms"] if t else None
+
+        a, b = at98("plain"), at98("learned")
+        out["learned_speedup_at_98pct_recall"] = a / b if a and b else None
+        out["plain_speedup_vs_brute_force_at_98pct_recall"] = out["brute_force_plan_ms"] / a if a else None
     return out
 
 
