@@ -73,19 +73,27 @@ __global__ void bias_kernel(int32_t* __restrict__ bias, const int8_t* __restrict
 }
 
 // ---------------------------------------------------------------- projection (tcgen05)
-// 128 descriptors per tile: TMA loads the raw bytes (128-byte swizzle), threads halve them in
-// place (x >> 1 fits int8), one thread issues s8 x s8 UMMAs (M=128, N=channels, K=128) against
-// the weights (s8, loaded once per CTA), each thread reads its descriptor's channel sums from
-// its TMEM lane and packs the sign bits.
-constexpr int kHashThreads = 256;  // two threads per TMEM lane: each takes half of the channel groups
-constexpr int kHashStages = 4;  // descriptor tiles in flight per CTA (two CTAs per SM)
+// Warp-specialised, one CTA per SM, tiles of 128 descriptors flowing through four roles:
+//   warp 0      TMA producer: raw descriptor tiles into a kHashStages-deep ring
+//   warps 2-5   halve every byte in place ((x & 0xFE) >> 1 fits int8, the reference's transform)
+//   warp 1      TMEM owner and UMMA issuer: s8 x s8 UMMAs (M=128, N=channels, K=128) against the
+//               weights (loaded once) into one of two TMEM accumulators; its commit also frees
+//               the descriptor stage
+//   warps 6-29  epilogue: six warps per TMEM lane quarter, one per 32-channel group, read the
+//               channel sums, add the bias and pack the sign bits
+// so the HBM stream, the halving, the MMA and the sign packing of different tiles overlap.
+constexpr int kHashStages = 8;
+constexpr int kHashHalvers = 4;
+constexpr int kHashEpi = 24;
+constexpr int kHashThreads = 32 * (2 + kHashHalvers + kHashEpi);
 struct HashSmem {
     uint8_t desc[kHashStages][128 * 128];
     uint8_t w[192 * 128];
     int32_t bias[192];
     uint32_t hist[8][256];
-    uint64_t full[kHashStages];
-    uint64_t mma;
+    uint64_t full[kHashStages], halved[kHashStages], empty[kHashStages];
+    uint64_t accFull[2], accEmpty[2];
+    uint64_t wbar;
     uint32_t tmem;
 };
 
@@ -104,107 +112,129 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
     for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) (&S.hist[0][0])[x] = 0;
     for (int c = tid; c < channels; c += kHashThreads) S.bias[c] = bias[c];
     if (tid == 0) {
-        for (int b = 0; b < kHashStages; ++b) mbar_init(&S.full[b], 1);
-        mbar_init(&S.mma, 1);
+        for (int b = 0; b < kHashStages; ++b) {
+            mbar_init(&S.full[b], 1);
+            mbar_init(&S.halved[b], 32 * kHashHalvers);
+            mbar_init(&S.empty[b], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&S.accFull[b], 1);
+            mbar_init(&S.accEmpty[b], kHashEpi);
+        }
+        mbar_init(&S.wbar, 1);
         fence_mbar_init();
     }
-    if (warp == 0) {
-        tmem_alloc(&S.tmem, 256);
+    if (warp == 1) {
+        tmem_alloc(&S.tmem, 512);  // two accumulators of up to 192 columns, at columns 0 and 256
         tmem_relinquish();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem;
-    uint32_t* err_ = err;
-    // weights once (channels rows of 128 bytes), then the first descriptor tile
-    if (tid == 0) {
-        mbar_arrive_expect_tx(&S.mma, uint32_t(channels) * 128u);
-        for (int r = 0; r < channels; r += 64) tma_load_2d(S.w + r * 128, &tmW, &S.mma, 0, r);
-        for (uint32_t k = 0; k + 1 < uint32_t(kHashStages); ++k) {
-            const uint32_t t = blockIdx.x + k * gridDim.x;
-            if (t < tiles) {
-                mbar_arrive_expect_tx(&S.full[k], 128u * 128u);
-                tma_load_2d(S.desc[k], &tmDesc, &S.full[k], 0, int32_t(t * 128u));
+    if (warp == 0) {
+        // ---- TMA producer
+        if (lane == 0) {
+            mbar_arrive_expect_tx(&S.wbar, uint32_t(channels) * 128u);
+            for (int r = 0; r < channels; r += 64) tma_load_2d(S.w + r * 128, &tmW, &S.wbar, 0, r);
+            uint32_t k = 0;
+            for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+                const uint32_t st = k % kHashStages;
+                if (k >= uint32_t(kHashStages)) mbar_wait(&S.empty[st], ((k / kHashStages) - 1) & 1u, err, kDevTimeoutTmaEmpty);
+                mbar_arrive_expect_tx(&S.full[st], 128u * 128u);
+                tma_load_2d(S.desc[st], &tmDesc, &S.full[st], 0, int32_t(tile * 128u));
             }
         }
-    }
-    mbar_wait(&S.mma, 0, err_, kDevTimeoutTmaFull);
-    uint32_t it = 0, mmaPhase = 1;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-        const uint32_t buf = it % kHashStages;
-        // prefetch kHashStages-1 tiles ahead into the buffer the previous iteration has finished with
-        const uint32_t ahead = tile + (kHashStages - 1) * gridDim.x;
-        if (tid == 0 && ahead < tiles) {
-            const uint32_t nb = (it + kHashStages - 1) % kHashStages;
-            mbar_arrive_expect_tx(&S.full[nb], 128u * 128u);
-            tma_load_2d(S.desc[nb], &tmDesc, &S.full[nb], 0, int32_t(ahead * 128u));
-        }
-        mbar_wait(&S.full[buf], (it / kHashStages) & 1u, err_, kDevTimeoutTmaFull);
-        // halve every byte in place: (x & 0xFE) >> 1
-        uint4* d4 = reinterpret_cast<uint4*>(S.desc[buf]);
-#pragma unroll
-        for (int k = 0; k < 1024 / kHashThreads; ++k) {
-            uint4 v = d4[tid + kHashThreads * k];
-            v.x = (v.x & 0xFEFEFEFEu) >> 1;
-            v.y = (v.y & 0xFEFEFEFEu) >> 1;
-            v.z = (v.z & 0xFEFEFEFEu) >> 1;
-            v.w = (v.w & 0xFEFEFEFEu) >> 1;
-            d4[tid + kHashThreads * k] = v;
-        }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
+    } else if (warp == 1) {
+        // ---- UMMA issuer
+        if (lane == 0) {
+            mbar_wait(&S.wbar, 0, err, kDevTimeoutTmaFull);
             const uint32_t idesc = idesc_s8s8_s32(128, channels);
-            const uint32_t a = smem_u32(S.desc[buf]), b = smem_u32(S.w);
+            const uint32_t bw = smem_u32(S.w);
+            uint32_t k = 0;
+            for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+                const uint32_t st = k % kHashStages, b = k & 1u;
+                mbar_wait(&S.halved[st], (k / kHashStages) & 1u, err, kDevTimeoutTmaFull);
+                if (k >= 2) mbar_wait(&S.accEmpty[b], ((k >> 1) - 1) & 1u, err, kDevTimeoutAccEmpty);
+                tc_fence_after();
+                const uint32_t a = smem_u32(S.desc[st]);
 #pragma unroll
-            for (uint32_t k = 0; k < 4; ++k)
-                umma_i8(tmem, umma_desc_k_sw128(a + 32u * k), umma_desc_k_sw128(b + 32u * k), idesc, k);
-            umma_commit(&S.mma);
-        }
-        __syncwarp();
-        mbar_wait(&S.mma, mmaPhase, err_, kDevTimeoutAccFull);
-        mmaPhase ^= 1u;
-        tc_fence_after();
-        // Warp w reads TMEM lanes 32 (w % 4).. (its descriptors) and the 32-channel groups
-        // cw = half, half + 2, ... (half = w / 4): keys are groups 0-1, the remap code groups 2-5.
-        const uint32_t q = warp & 3u, half = warp >> 2;
-        const uint32_t i = tile * 128u + 32u * q + lane;
-        for (int cw = int(half); cw < channels / 32; cw += 2) {
-            uint32_t v[32];
-            tmem_ld32(tmem + ((32u * q) << 16) + 32u * cw, v);
-            tmem_wait_ld();
-            // sign bits of (sum + bias), shifted in from the top channel down: one funnel shift per
-            // channel; bit k = [sum_k + bias_k >= 0] after the final inversion
-            uint32_t neg = 0;
-            const int4* b4 = reinterpret_cast<const int4*>(&S.bias[32 * cw]);
-#pragma unroll
-            for (int k4 = 7; k4 >= 0; --k4) {
-                const int4 bb = b4[k4];
-                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 3]) + bb.w), neg, 1);
-                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 2]) + bb.z), neg, 1);
-                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 1]) + bb.y), neg, 1);
-                neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 0]) + bb.x), neg, 1);
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    umma_i8(tmem + 256u * b, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(bw + 32u * kk), idesc, kk);
+                umma_commit(&S.empty[st]);
+                umma_commit(&S.accFull[b]);
             }
-            const uint32_t bits = ~neg;
-            if (i < n) {
-                if (cw < 2) {
-                    reinterpret_cast<uint32_t*>(keys + size_t(i) * 8)[cw] = bits;
-                    if (histogram) {
+        }
+    } else if (warp < 2 + kHashHalvers) {
+        // ---- halving: 128 threads, 8 x 16 bytes each per tile
+        const uint32_t h = tid - 64;
+        uint32_t k = 0;
+        for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+            const uint32_t st = k % kHashStages;
+            mbar_wait(&S.full[st], (k / kHashStages) & 1u, err, kDevTimeoutTmaFull);
+            uint4* d4 = reinterpret_cast<uint4*>(S.desc[st]);
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) atomicAdd(&S.hist[4 * cw + b][(bits >> (8 * b)) & 0xFFu], 1u);
+            for (int r = 0; r < 1024 / (32 * kHashHalvers); ++r) {
+                uint4 v = d4[h + 32 * kHashHalvers * r];
+                v.x = (v.x & 0xFEFEFEFEu) >> 1;
+                v.y = (v.y & 0xFEFEFEFEu) >> 1;
+                v.z = (v.z & 0xFEFEFEFEu) >> 1;
+                v.w = (v.w & 0xFEFEFEFEu) >> 1;
+                d4[h + 32 * kHashHalvers * r] = v;
+            }
+            fence_proxy_async_smem();  // generic-proxy writes, read next by the UMMA (async proxy)
+            mbar_arrive(&S.halved[st]);
+        }
+    } else {
+        // ---- epilogue. Warp w reads TMEM lanes 32 (w % 4).. (its descriptors) and the 32-channel
+        // group cw = (w - 6) / 4: keys are groups 0-1, the remap code groups 2-5.
+        const uint32_t e = warp - (2 + kHashHalvers);
+        const uint32_t q = warp & 3u;
+        const int cw = int(e >> 2);
+        uint32_t k = 0;
+        for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+            const uint32_t b = k & 1u;
+            mbar_wait(&S.accFull[b], (k >> 1) & 1u, err, kDevTimeoutAccFull);
+            tc_fence_after();
+            const uint32_t i = tile * 128u + 32u * q + lane;
+            if (cw < channels / 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem + 256u * b + ((32u * q) << 16) + 32u * cw, v);
+                tmem_wait_ld();
+                // sign bits of (sum + bias), shifted in from the top channel down: one funnel shift
+                // per channel; bit k = [sum_k + bias_k >= 0] after the final inversion
+                uint32_t neg = 0;
+                const int4* b4 = reinterpret_cast<const int4*>(&S.bias[32 * cw]);
+#pragma unroll
+                for (int k4 = 7; k4 >= 0; --k4) {
+                    const int4 bb = b4[k4];
+                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 3]) + bb.w), neg, 1);
+                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 2]) + bb.z), neg, 1);
+                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 1]) + bb.y), neg, 1);
+                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 0]) + bb.x), neg, 1);
+                }
+                const uint32_t bits = ~neg;
+                if (i < n) {
+                    if (cw < 2) {
+                        reinterpret_cast<uint32_t*>(keys + size_t(i) * 8)[cw] = bits;
+                        if (histogram) {
+#pragma unroll
+                            for (int bt = 0; bt < 4; ++bt)
+                                atomicAdd(&S.hist[4 * cw + bt][(bits >> (8 * bt)) & 0xFFu], 1u);
+                        }
+                    } else if (remap) {
+                        remap[size_t(i) * 4 + (cw - 2)] = bits;
                     }
-                } else if (remap) {
-                    remap[size_t(i) * 4 + (cw - 2)] = bits;
                 }
             }
+            // Released after the packing: measured faster than releasing right after the TMEM
+            // load (and faster than four independent shift chains instead of one).
+            tc_fence_before();  // (tcgen05.ld and its wait are warp-collective: the warp is converged)
+            if (lane == 0) mbar_arrive(&S.accEmpty[b]);
         }
-        tc_fence_before();
-        __syncthreads();  // TMEM and the descriptor buffer are reused by the next iteration
     }
+    __syncthreads();
     if (histogram) {
-        __syncthreads();
         for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) {
             const uint32_t c = (&S.hist[0][0])[x];
             if (c) atomicAdd(&histogram[x], c);
@@ -212,7 +242,7 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 256);
+    if (warp == 1) tmem_dealloc(tmem, 512);
 }
 
 // ---------------------------------------------------------------- histogram
@@ -341,7 +371,7 @@ int hash_launch(const void* weights, const int32_t* bias, int channels, const vo
         attr = true;
     }
     const uint32_t tiles = (n + 127) / 128;
-    const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(2 * sm_count()));
+    const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(sm_count()));
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
     hash_kernel<<<grid, kHashThreads, smem, stream>>>(tmD, tmW, bias, channels, n, keys, remap, histogram,
