@@ -63,3 +63,34 @@ def test_host_cross_check_matches_oracle(rsfm, oracle):
     assert len(got) == len(exp) > 0
     for f in ("idxQuery", "idxTrain", "distance"):
         np.testing.assert_array_equal(got[f], exp[f])
+
+
+def test_new_entry_points_validate_without_gpu(rsfm):
+    """Argument checks of the dp4a-matcher, 4-bit, device-filter and RANSAC entry points run
+    before any CUDA call (status 1 = invalid argument, 2 = capacity)."""
+    lib = rsfm._lib.load()
+    T = rsfm._lib.SiftBFTask
+    null = (T * 1)(T(10, 10, 0, 0, 0, 0, 0, 0))
+    for fn in (lib.rsfm_bf_match_idp, lib.rsfm_bf_match_4b):
+        assert fn(null, 1, None) == 1
+        assert fn((T * 1)(T(10, 10, 0x1001, 0x2000, 0x3000, 0x4000, 0x5000, 0x6000)), 1, None) == 1  # misaligned
+        big = (T * 1)(T(0x7FFFFF01, 10, 0x1000, 0x2000, 0x3000, 0x4000, 0x5000, 0x6000))
+        assert fn(big, 1, None) == 2
+        assert fn(null, 0, None) == 0
+    # the 4-bit matcher needs the norms, the dp4a matcher does not read them
+    no_norms = (T * 1)(T(0x7FFFFF01, 10, 0x1000, 0x2000, 0x3000, 0x4000, 0, 0))
+    assert lib.rsfm_bf_match_4b(no_norms, 1, None) == 1
+    assert lib.rsfm_bf_match_idp(no_norms, 1, None) == 2
+    assert lib.rsfm_sift_desc_8b_to_4b(None, None, 5, None) == 1
+    assert lib.rsfm_sift_desc_8b_to_4b(0x1000, 0x1008, 5, None) == 1  # source not 16-byte aligned
+    assert lib.rsfm_sift_desc_8b_to_4b(None, None, 0, None) == 0
+    assert lib.rsfm_precomp_sift4b_sqr_norm(None, None, 5, None) == 1
+    assert lib.rsfm_cross_check_matches_device(0x1000, 5, 0x2000, 5, 0x3000, None, None) == 1
+    assert lib.rsfm_cross_check_matches_device(None, 5, 0x2000, 5, 0x3000, 0x4000, None) == 1
+    assert lib.rsfm_remove_match_conflicts_device(0x1000, 5, 5, 0x3000, None, None) == 1
+    assert lib.rsfm_remove_match_conflicts_device(0x1000, 5, 5, None, 0x4000, None) == 1
+    assert lib.rsfm_ransac_match_filter(0x1001, 0x2000, 0x3000, 100, 0x4000, 16, 12, 256, 15.0, 1, 0, None) == 1
+    assert lib.rsfm_ransac_match_filter(0x1000, 0x2000, 0x3000, 100, 0x4000, 300, 300, 256, 15.0, 1, 0, None) == 1
+    assert lib.rsfm_ransac_match_filter(None, None, None, 0, None, 16, 12, 256, 15.0, 1, 0, None) == 0
+    assert lib.rsfm_ransac_inlier_mask(0, 1200, None, 0, 2, 256, 0.15, 16, 1, 0, None, None) == 1
+    assert lib.rsfm_ransac_inlier_mask(1600, 1200, None, 0, 2, 256, 0.15, 16, 1, 0, None, None) == 0
