@@ -281,6 +281,20 @@ int rsfm_cashash_find_best_match_ex(const rsfm_cashash_image* queries, const uin
                                     const rsfm_cashash_result* results, uint32_t nbTasks, uint32_t flags,
                                     cudaStream_t stream);
 
+/* One independent pair for rsfm_cashash_find_best_match_pairs. */
+typedef struct rsfm_cashash_pair {
+    rsfm_cashash_image query, train;
+    uint32_t querySize, trainSize;
+    rsfm_cashash_result result;
+} rsfm_cashash_pair;
+
+/* findBestMatch over many independent (query image, train image) pairs in one launch (no
+ * reference counterpart: the reference matches the queries of one call against a single train
+ * image). Per pair the same results as rsfm_cashash_find_best_match_ex on that pair; `pairs` is
+ * a host array (at most 65535); flags as for _ex. */
+int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
+                                       cudaStream_t stream);
+
 /* Image for ranked cascade-hash matching (no reference counterpart): keys = 8 bucket-key bytes
  * per descriptor and codes = the 128-bit remap code (rsfm_cashash_compute_hash with 192
  * channels, or the learned hash), bucket lists per scheme at buckets[s * nbDesc + lower(s, b)]

@@ -70,6 +70,12 @@ class CasHashResult(ctypes.Structure):
     _fields_ = [("query", ctypes.c_void_p), ("train", ctypes.c_void_p)]
 
 
+class CasHashPair(ctypes.Structure):
+    """rsfm_cashash_pair (one independent pair of a batched findBestMatch)."""
+    _fields_ = [("query", CasHashImage), ("train", CasHashImage), ("querySize", ctypes.c_uint32),
+                ("trainSize", ctypes.c_uint32), ("result", CasHashResult)]
+
+
 class RankedImage(ctypes.Structure):
     _fields_ = [("desc", ctypes.c_void_p), ("keys", ctypes.c_void_p), ("codes", ctypes.c_void_p),
                 ("bucketEnds", ctypes.c_void_p), ("buckets", ctypes.c_void_p), ("sqrNormDesc", ctypes.c_void_p),
@@ -146,6 +152,8 @@ SIGNATURES = {
                                                     ctypes.POINTER(CasHashImage), ctypes.c_uint32,
                                                     ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_void_p,
                                                     ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_cashash_find_best_match_pairs": (ctypes.c_int, [ctypes.POINTER(CasHashPair), ctypes.c_uint32,
+                                                          ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,
                                                        ctypes.POINTER(CasHashImage), ctypes.c_uint32,
                                                        ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_uint32,

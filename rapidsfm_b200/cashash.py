@@ -224,6 +224,24 @@ class CascadeMatcher:
         return out
 
 
+def find_best_match_pairs(pairs, per_scheme_lists=True, stream=None):
+    """findBestMatch over many independent (query, train) RankedImage pairs in one launch
+    (rsfm_cashash_find_best_match_pairs); returns per pair (best int64 [nq], best int64 [nt])."""
+    lib = _lib.load()
+
+    def ci(img):
+        return _lib.CasHashImage(img.desc.data_ptr(), img.upper.data_ptr(), img.buckets.data_ptr(), img.sqr.data_ptr())
+
+    outs = [(torch.empty(q.n, dtype=torch.int64, device=q.desc.device),
+             torch.empty(t.n, dtype=torch.int64, device=q.desc.device)) for q, t in pairs]
+    arr = (_lib.CasHashPair * len(pairs))(*[
+        _lib.CasHashPair(ci(q), ci(t), q.n, t.n, _lib.CasHashResult(a.data_ptr(), b.data_ptr()))
+        for (q, t), (a, b) in zip(pairs, outs)])
+    _lib.check(lib.rsfm_cashash_find_best_match_pairs(arr, len(pairs), 1 if per_scheme_lists else 0,
+                                                      _stream_ptr(stream)), "rsfm_cashash_find_best_match_pairs")
+    return outs
+
+
 def find_best_match(queries, train, per_scheme_lists=True, max_bucket_sizes=None, stream=None):
     """cashash::findBestMatch (cascadeHash.h:106-107) over RankedImages: every (query, train)
     descriptor pair sharing a bucket in any of the 8 schemes is scored by exact L2; returns per query

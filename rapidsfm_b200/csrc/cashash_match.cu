@@ -19,6 +19,7 @@
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
+#include <vector>
 
 namespace rsfm_b200 {
 namespace chm {
@@ -97,183 +98,247 @@ __global__ void init_kernel(const __grid_constant__ Params P, uint32_t nTrain, u
     if (t == 0 && x == 0) *P.counter = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) match_kernel(const __grid_constant__ Params P, uint32_t nTrain,
-                                                         const uint32_t* __restrict__ qSizes) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem& S = smem_aligned_1024<Smem>(smem_raw);
+// What one work item (scheme s, bucket k) needs: the query images that share one train image.
+struct ItemCtx {
+    const ImageDev* q;                  // nTasks query images
+    unsigned long long* const* qBest;   // per task
+    unsigned long long* const* tBest;   // per task (entries may be null: one direction only)
+    ImageDev t;
+    uint32_t nTasks, nTrain, schemeOffset;
+    bool bidir;
+};
+
+// All threads of the CTA call this together for one item.
+__device__ __forceinline__ void process_item(Smem& S, const ItemCtx& C, uint32_t s, uint32_t k, uint32_t tmem,
+                                             uint32_t idesc, uint32_t& mmaPhase, uint32_t* err) {
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t* tEnds = C.t.ends + s * 256;
+    const uint32_t tb = k ? tEnds[k - 1] : 0u, te = tEnds[k];
+    const uint32_t nT = te - tb;
+    if (nT == 0) return;
+    // Query members of every task in this bucket, cut into 32-row segments.
+    if (tid < C.nTasks) {
+        const uint32_t* qe = C.q[tid].ends + s * 256;
+        const uint32_t b0 = k ? qe[k - 1] : 0u;
+        S.qBeg[tid] = b0;
+        S.qCnt[tid] = qe[k] - b0;
+    }
+    __syncthreads();
     if (tid == 0) {
+        uint32_t g = 0;
+        for (uint32_t t = 0; t < C.nTasks; ++t) {
+            S.segBase[t] = g;
+            g += (S.qCnt[t] + 31u) / 32u;
+        }
+        S.segBase[C.nTasks] = g;
+    }
+    __syncthreads();
+    const uint32_t nSeg = S.segBase[C.nTasks];
+    const uint32_t nColBlocks = (nT + 63u) / 64u;
+    for (uint32_t g0 = 0; g0 < nSeg; g0 += 4) {
+        // ---- gather this tile's 4 segments (one per warp), rows sorted by query index
+        const uint32_t g = g0 + warp;
+        uint32_t task = 0;
+        if (g < nSeg)
+            while (task + 1 < C.nTasks && S.segBase[task + 1] <= g) ++task;
+        uint32_t q = kNoRow;
+        if (g < nSeg) {
+            const uint32_t m = (g - S.segBase[task]) * 32u + lane;
+            if (m < S.qCnt[task]) {
+                const uint32_t nQ = C.q[task].ends[255];
+                q = C.q[task].buckets[size_t(s) * nQ * C.schemeOffset + S.qBeg[task] + m];
+            }
+        }
+        q = warp_sort(q, lane);
+        const uint32_t row = 32u * warp + lane;
+        S.rowQ[row] = q;
+        S.rowNA[row] = q != kNoRow ? C.q[task].sqr[q] : kBigNorm;
+        {
+            const uint8_t* src = q != kNoRow ? C.q[task].desc + size_t(q) * 128 : C.q[0].desc;
+#pragma unroll
+            for (uint32_t c = 0; c < 8; ++c) cp_async16(S.a + sw128(row, c), src + 16 * c, q != kNoRow);
+        }
+        const uint32_t rowTask = task;
+        const bool rowValid = q != kNoRow;
+        // row state across column blocks: best (d, train index)
+        uint32_t bestD = 0xFFFFFFFFu, bestT = 0xFFFFFFFFu;
+        for (uint32_t cb = 0; cb < nColBlocks; ++cb) {
+            // ---- train block: up to 64 members, sorted by index (rank sort in shared memory)
+            if (cb > 0 || g0 == 0 || nColBlocks > 1) {
+                if (tid < 64) {
+                    const uint32_t c = cb * 64u + tid;
+                    S.colT[tid] = c < nT ? C.t.buckets[size_t(s) * C.nTrain * C.schemeOffset + tb + c] : kNoRow;
+                }
+                __syncthreads();
+                uint32_t v = kNoRow, rank = 0;
+                if (tid < 64) {
+                    v = S.colT[tid];
+                    for (uint32_t o = 0; o < 64; ++o) {
+                        const uint32_t w = S.colT[o];
+                        rank += (w < v) || (w == v && o < tid);
+                    }
+                }
+                __syncthreads();
+                if (tid < 64) {
+                    S.colT[rank] = v;
+                    S.colNB[rank] = v != kNoRow ? C.t.sqr[v] : kBigNorm;
+                }
+                __syncthreads();
+                // gather: 64 rows x 8 chunks, 4 per thread
+#pragma unroll
+                for (uint32_t x = 0; x < 4; ++x) {
+                    const uint32_t r = (tid >> 3) + 16u * x, c = tid & 7u;
+                    const uint32_t tv = S.colT[r];
+                    const uint8_t* src = tv != kNoRow ? C.t.desc + size_t(tv) * 128 + 16 * c : C.t.desc;
+                    cp_async16(S.b + sw128(r, c), src, tv != kNoRow);
+                }
+            }
+            cp_async_wait_all();
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t a = smem_u32(S.a), b = smem_u32(S.b);
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    umma_i8(tmem, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk), idesc, kk);
+                umma_commit(&S.mma);
+            }
+            __syncwarp();
+            mbar_wait(&S.mma, mmaPhase, err, kDevTimeoutAccFull);
+            mmaPhase ^= 1u;
+            tc_fence_after();
+            // ---- epilogue: warp = segment (32 rows), 64 columns in two chunks
+            const uint32_t nA = S.rowNA[row];
+#pragma unroll
+            for (uint32_t ch = 0; ch < 2; ++ch) {
+                uint32_t x[32];
+                tmem_ld32(tmem + ((32u * warp) << 16) + 32u * ch, x);
+                tmem_wait_ld();
+                uint32_t rmin = 0xFFFFFFFFu;
+#pragma unroll
+                for (uint32_t c = 0; c < 32; ++c) {
+                    const uint32_t d = nA + S.colNB[32 * ch + c] - 2u * x[c];
+                    x[c] = d;
+                    rmin = min(rmin, (d << 6) | (32u * ch + c));
+                }
+                // row: chunk minimum (ties -> lowest column = lowest train index in the block)
+                const uint32_t cd = rmin >> 6, cc = rmin & 63u;
+                if (rowValid && cd < kValidD) {
+                    const uint32_t tIdx = S.colT[cc];
+                    if (cd < bestD || (cd == bestD && tIdx < bestT)) {
+                        bestD = cd;
+                        bestT = tIdx;
+                    }
+                }
+                // columns: warp minimum of (d, lane) (lanes sorted by query index)
+                if (C.bidir) {
+                    uint32_t mine = 0xFFFFFFFFu;
+#pragma unroll
+                    for (uint32_t c = 0; c < 32; ++c) {
+                        const uint32_t key = rowValid && x[c] < kValidD ? ((x[c] << 5) | lane) : 0xFFFFFFFFu;
+                        const uint32_t m = __reduce_min_sync(0xffffffffu, key);
+                        mine = (lane == c) ? m : mine;
+                    }
+                    const uint32_t tIdx = S.colT[32 * ch + lane];
+                    if (mine != 0xFFFFFFFFu && tIdx != kNoRow) {
+                        const uint32_t qIdx = S.rowQ[32 * warp + (mine & 31u)];
+                        atomicMin(&C.tBest[rowTask][tIdx], (static_cast<unsigned long long>(mine >> 5) << 32) | qIdx);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncthreads();  // TMEM and the B block are reused by the next block / tile
+        }
+        if (rowValid && bestD != 0xFFFFFFFFu)
+            atomicMin(&C.qBest[rowTask][q], (static_cast<unsigned long long>(bestD) << 32) | bestT);
+        __syncthreads();  // the A tile is reused by the next tile
+    }
+}
+
+__device__ __forceinline__ void kernel_setup(Smem& S, uint32_t& tmem) {
+    if (threadIdx.x == 0) {
         mbar_init(&S.mma, 1);
         fence_mbar_init();
     }
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tmem_alloc(&S.tmem, 64);
         tmem_relinquish();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = S.tmem;
+    tmem = S.tmem;
+}
+
+__device__ __forceinline__ void kernel_teardown(uint32_t tmem) {
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) tmem_dealloc(tmem, 64);
+}
+
+// Query images of one call against one train image (the reference's findBestMatch shape).
+__global__ void __launch_bounds__(kThreads) match_kernel(const __grid_constant__ Params P, uint32_t nTrain,
+                                                         const uint32_t* __restrict__ qSizes) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Smem& S = smem_aligned_1024<Smem>(smem_raw);
+    uint32_t tmem;
+    kernel_setup(S, tmem);
     const uint32_t idesc = idesc_u8u8_s32(128, 64);
     uint32_t mmaPhase = 0;
-    const bool bidir = P.tBest[0] != nullptr;
-
+    const ItemCtx C{P.q, P.qBest, P.tBest, P.t, P.nTasks, nTrain, P.schemeOffset, P.tBest[0] != nullptr};
     for (;;) {
-        if (tid == 0) S.item = atomicAdd(P.counter, 1u);
+        if (threadIdx.x == 0) S.item = atomicAdd(P.counter, 1u);
         __syncthreads();
         const uint32_t item = S.item;
         if (item >= 8u * 256u) break;
         // Spread schemes: consecutive items are different buckets of different schemes.
-        const uint32_t s = item & 7u, k = item >> 3;
-        const uint32_t* tEnds = P.t.ends + s * 256;
-        const uint32_t tb = k ? tEnds[k - 1] : 0u, te = tEnds[k];
-        const uint32_t nT = te - tb;
-        if (nT == 0) {
-            __syncthreads();
-            continue;
-        }
-        // Query members of every task in this bucket, cut into 32-row segments.
-        if (tid < P.nTasks) {
-            const uint32_t* qe = P.q[tid].ends + s * 256;
-            const uint32_t b0 = k ? qe[k - 1] : 0u;
-            S.qBeg[tid] = b0;
-            S.qCnt[tid] = qe[k] - b0;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t g = 0;
-            for (uint32_t t = 0; t < P.nTasks; ++t) {
-                S.segBase[t] = g;
-                g += (S.qCnt[t] + 31u) / 32u;
-            }
-            S.segBase[P.nTasks] = g;
-        }
-        __syncthreads();
-        const uint32_t nSeg = S.segBase[P.nTasks];
-        const uint32_t nColBlocks = (nT + 63u) / 64u;
-        for (uint32_t g0 = 0; g0 < nSeg; g0 += 4) {
-            // ---- gather this tile's 4 segments (one per warp), rows sorted by query index
-            const uint32_t g = g0 + warp;
-            uint32_t task = 0;
-            if (g < nSeg)
-                while (task + 1 < P.nTasks && S.segBase[task + 1] <= g) ++task;
-            uint32_t q = kNoRow;
-            if (g < nSeg) {
-                const uint32_t m = (g - S.segBase[task]) * 32u + lane;
-                if (m < S.qCnt[task]) {
-                    const uint32_t nQ = P.q[task].ends[255];
-                    q = P.q[task].buckets[size_t(s) * nQ * P.schemeOffset + S.qBeg[task] + m];
-                }
-            }
-            q = warp_sort(q, lane);
-            const uint32_t row = 32u * warp + lane;
-            S.rowQ[row] = q;
-            S.rowNA[row] = q != kNoRow ? P.q[task].sqr[q] : kBigNorm;
-            {
-                const uint8_t* src = q != kNoRow ? P.q[task].desc + size_t(q) * 128 : P.q[0].desc;
-#pragma unroll
-                for (uint32_t c = 0; c < 8; ++c) cp_async16(S.a + sw128(row, c), src + 16 * c, q != kNoRow);
-            }
-            const uint32_t rowTask = task;
-            const bool rowValid = q != kNoRow;
-            // row state across column blocks: best (d, train index)
-            uint32_t bestD = 0xFFFFFFFFu, bestT = 0xFFFFFFFFu;
-            for (uint32_t cb = 0; cb < nColBlocks; ++cb) {
-                // ---- train block: up to 64 members, sorted by index (rank sort in shared memory)
-                if (cb > 0 || g0 == 0 || nColBlocks > 1) {
-                    if (tid < 64) {
-                        const uint32_t c = cb * 64u + tid;
-                        S.colT[tid] = c < nT ? P.t.buckets[size_t(s) * nTrain * P.schemeOffset + tb + c] : kNoRow;
-                    }
-                    __syncthreads();
-                    uint32_t v = kNoRow, rank = 0;
-                    if (tid < 64) {
-                        v = S.colT[tid];
-                        for (uint32_t o = 0; o < 64; ++o) {
-                            const uint32_t w = S.colT[o];
-                            rank += (w < v) || (w == v && o < tid);
-                        }
-                    }
-                    __syncthreads();
-                    if (tid < 64) {
-                        S.colT[rank] = v;
-                        S.colNB[rank] = v != kNoRow ? P.t.sqr[v] : kBigNorm;
-                    }
-                    __syncthreads();
-                    // gather: 64 rows x 8 chunks, 4 per thread
-#pragma unroll
-                    for (uint32_t x = 0; x < 4; ++x) {
-                        const uint32_t r = (tid >> 3) + 16u * x, c = tid & 7u;
-                        const uint32_t tv = S.colT[r];
-                        const uint8_t* src = tv != kNoRow ? P.t.desc + size_t(tv) * 128 + 16 * c : P.t.desc;
-                        cp_async16(S.b + sw128(r, c), src, tv != kNoRow);
-                    }
-                }
-                cp_async_wait_all();
-                fence_proxy_async_smem();
-                __syncthreads();
-                if (tid == 0) {
-                    tc_fence_after();
-                    const uint32_t a = smem_u32(S.a), b = smem_u32(S.b);
-#pragma unroll
-                    for (uint32_t kk = 0; kk < 4; ++kk)
-                        umma_i8(tmem, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk), idesc, kk);
-                    umma_commit(&S.mma);
-                }
-                __syncwarp();
-                mbar_wait(&S.mma, mmaPhase, P.err, kDevTimeoutAccFull);
-                mmaPhase ^= 1u;
-                tc_fence_after();
-                // ---- epilogue: warp = segment (32 rows), 64 columns in two chunks
-                const uint32_t nA = S.rowNA[row];
-#pragma unroll
-                for (uint32_t ch = 0; ch < 2; ++ch) {
-                    uint32_t x[32];
-                    tmem_ld32(tmem + ((32u * warp) << 16) + 32u * ch, x);
-                    tmem_wait_ld();
-                    uint32_t rmin = 0xFFFFFFFFu;
-#pragma unroll
-                    for (uint32_t c = 0; c < 32; ++c) {
-                        const uint32_t d = nA + S.colNB[32 * ch + c] - 2u * x[c];
-                        x[c] = d;
-                        rmin = min(rmin, (d << 6) | (32u * ch + c));
-                    }
-                    // row: chunk minimum (ties -> lowest column = lowest train index in the block)
-                    const uint32_t cd = rmin >> 6, cc = rmin & 63u;
-                    if (rowValid && cd < kValidD) {
-                        const uint32_t tIdx = S.colT[cc];
-                        if (cd < bestD || (cd == bestD && tIdx < bestT)) {
-                            bestD = cd;
-                            bestT = tIdx;
-                        }
-                    }
-                    // columns: warp minimum of (d, lane) (lanes sorted by query index)
-                    if (bidir) {
-                        uint32_t mine = 0xFFFFFFFFu;
-#pragma unroll
-                        for (uint32_t c = 0; c < 32; ++c) {
-                            const uint32_t key = rowValid && x[c] < kValidD ? ((x[c] << 5) | lane) : 0xFFFFFFFFu;
-                            const uint32_t m = __reduce_min_sync(0xffffffffu, key);
-                            mine = (lane == c) ? m : mine;
-                        }
-                        const uint32_t tIdx = S.colT[32 * ch + lane];
-                        if (mine != 0xFFFFFFFFu && tIdx != kNoRow) {
-                            const uint32_t qIdx = S.rowQ[32 * warp + (mine & 31u)];
-                            atomicMin(&P.tBest[rowTask][tIdx], (static_cast<unsigned long long>(mine >> 5) << 32) | qIdx);
-                        }
-                    }
-                }
-                tc_fence_before();
-                __syncthreads();  // TMEM and the B block are reused by the next block / tile
-            }
-            if (rowValid && bestD != 0xFFFFFFFFu)
-                atomicMin(&P.qBest[rowTask][q], (static_cast<unsigned long long>(bestD) << 32) | bestT);
-            __syncthreads();  // the A tile is reused by the next tile
-        }
+        process_item(S, C, item & 7u, item >> 3, tmem, idesc, mmaPhase, P.err);
+        __syncthreads();  // S.item is rewritten next
     }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 64);
+    kernel_teardown(tmem);
+}
+
+// Many independent (query image, train image) pairs: items (pair, scheme, bucket) from one counter.
+struct PairDev {
+    ImageDev q, t;
+    unsigned long long* qBest;
+    unsigned long long* tBest;
+    uint32_t nQ, nT;
+};
+
+__global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* counter) {
+    const PairDev& P = pairs[blockIdx.y];
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < max(P.nQ, P.nT); x += gridDim.x * blockDim.x) {
+        if (x < P.nQ) P.qBest[x] = ~0ull;
+        if (P.tBest && x < P.nT) P.tBest[x] = ~0ull;
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *counter = 0;
+}
+
+__global__ void __launch_bounds__(kThreads) match_pairs_kernel(const PairDev* __restrict__ pairs, uint32_t nPairs,
+                                                               uint32_t schemeOffset, uint32_t* counter,
+                                                               uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Smem& S = smem_aligned_1024<Smem>(smem_raw);
+    uint32_t tmem;
+    kernel_setup(S, tmem);
+    const uint32_t idesc = idesc_u8u8_s32(128, 64);
+    uint32_t mmaPhase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) S.item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = S.item;
+        if (item >= nPairs * 2048u) break;
+        const PairDev& P = pairs[item >> 11];
+        const uint32_t local = item & 2047u;
+        if (P.nQ && P.nT) {
+            const ItemCtx C{&P.q, &P.qBest, &P.tBest, P.t, 1u, P.nT, schemeOffset, P.tBest != nullptr};
+            process_item(S, C, local & 7u, local >> 3, tmem, idesc, mmaPhase, err);
+        }
+        __syncthreads();  // S.item is rewritten next
+    }
+    kernel_teardown(tmem);
 }
 
 }  // namespace chm
@@ -360,6 +425,65 @@ extern "C" int rsfm_cashash_find_best_match(const rsfm_cashash_image* queries, c
     (void)maxQueryBucketSize;  // the persistent kernel sizes its tiles from the buckets themselves
     (void)maxTrainBucketSize;
     return find_best_match_impl(queries, querySize, train, trainSize, results, nbTasks, 0u, stream);
+}
+
+extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
+                                                  cudaStream_t stream) {
+    launch_count_reset();
+    if (nbPairs == 0) return RSFM_OK;
+    if (!pairs || nbPairs > 65535u) return RSFM_ERR_INVALID_ARG;
+    std::vector<chm::PairDev> host(nbPairs);
+    uint32_t maxN = 1;
+    auto bad = [](const rsfm_cashash_image& m) {
+        return !m.desc || !m.bucketEnds || !m.buckets || !m.sqrNormDesc || (reinterpret_cast<uintptr_t>(m.desc) & 15u);
+    };
+    for (uint32_t p = 0; p < nbPairs; ++p) {
+        const rsfm_cashash_pair& in = pairs[p];
+        if (in.querySize && !in.result.query) return RSFM_ERR_INVALID_ARG;
+        if (in.querySize && in.trainSize && (bad(in.query) || bad(in.train))) return RSFM_ERR_INVALID_ARG;
+        chm::PairDev& d = host[p];
+        d.q = {static_cast<const uint8_t*>(in.query.desc), in.query.bucketEnds, in.query.buckets, in.query.sqrNormDesc};
+        d.t = {static_cast<const uint8_t*>(in.train.desc), in.train.bucketEnds, in.train.buckets, in.train.sqrNormDesc};
+        d.qBest = reinterpret_cast<unsigned long long*>(in.result.query);
+        d.tBest = reinterpret_cast<unsigned long long*>(in.result.train);
+        d.nQ = in.querySize;
+        d.nT = in.trainSize;
+        maxN = std::max(maxN, std::max(d.nQ, d.nT));
+    }
+    cudaMemPool_t pool = nullptr;
+    const int ps = scratch_pool(&pool);
+    if (ps != RSFM_OK) return ps;
+    uint8_t* scratch = nullptr;
+    const size_t tableBytes = sizeof(chm::PairDev) * nbPairs;
+    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), 256 + tableBytes, pool, stream));
+    auto* counter = reinterpret_cast<uint32_t*>(scratch);
+    auto* table = reinterpret_cast<chm::PairDev*>(scratch + 256);
+    int st = RSFM_OK;
+    // pageable source: the copy is staged before the call returns, so `host` may go out of scope
+    if (cudaMemcpyAsync(table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) st = RSFM_ERR_CUDA;
+    static bool attr = false;
+    const size_t smem = sizeof(chm::Smem) + 1024;
+    if (st == RSFM_OK && !attr) {
+        if (cudaFuncSetAttribute(chm::match_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+            cudaSuccess)
+            st = RSFM_ERR_CUDA;
+        else
+            attr = true;
+    }
+    if (st == RSFM_OK) {
+        chm::pairs_init_kernel<<<dim3(std::min<uint32_t>((maxN + 255) / 256, 64u), nbPairs), 256, 0, stream>>>(table,
+                                                                                                          counter);
+        void* tok = nullptr;
+        const bool prof = profile_begin(stream, &tok);
+        chm::match_pairs_kernel<<<uint32_t(4 * sm_count()), chm::kThreads, smem, stream>>>(
+            table, nbPairs, (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u, counter, device_error_word());
+        if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
+        if (prof) profile_end(stream, tok);
+        launch_count_add(2);
+    }
+    const cudaError_t e = cudaFreeAsync(scratch, stream);
+    if (st == RSFM_OK && e != cudaSuccess) st = RSFM_ERR_CUDA;
+    return st;
 }
 
 extern "C" int rsfm_cashash_find_best_match_ex(const rsfm_cashash_image* queries, const uint32_t* querySize,

@@ -266,3 +266,43 @@ def test_find_best_match_timing_vs_reference(rsfm, oracle, ref):
     for (a, b), (c, d) in zip(outs["ref"], outs["ours"]):
         np.testing.assert_array_equal(a, c)
         np.testing.assert_array_equal(b, d)
+
+
+@pytest.mark.parametrize("flags", [0, 1])
+def test_find_best_match_pairs(rsfm, oracle, flags):
+    """Many independent (query, train) pairs in one launch: each pair's results equal the oracle's
+    findBestMatch on that pair (including pairs with an empty side)."""
+    rng = np.random.default_rng(77 + flags)
+    sizes = [(897, 700), (164, 2000), (1, 5), (0, 300), (300, 0), (2000, 2000)]
+    pairs, imgs = [], []
+    for nq, nt in sizes:
+        side = []
+        for n in (nq, nt):
+            desc = rng.integers(0, 256, size=(max(n, 1), 128), dtype=np.int64).astype(np.uint8)[:n]
+            keys = rng.integers(0, 256, size=(max(n, 1), 8), dtype=np.int64).astype(np.uint8)[:n]
+            side.append((desc, keys, _image(oracle, desc, keys) if n else None))
+        imgs.append(side)
+    dummy = _image(oracle, np.zeros((1, 128), np.uint8), np.zeros((1, 8), np.uint8))
+    res = []
+    arr = []
+    for (qd, qk, qi), (td, tk, ti) in imgs:
+        a = torch.empty(max(len(qd), 1), dtype=torch.int64, device="cuda")
+        b = torch.empty(max(len(td), 1), dtype=torch.int64, device="cuda")
+        res.append((a, b))
+        arr.append(rsfm._lib.CasHashPair(_ci(rsfm, qi or dummy), _ci(rsfm, ti or dummy), len(qd), len(td),
+                                         rsfm._lib.CasHashResult(a.data_ptr(), b.data_ptr())))
+    lib = rsfm._lib.load()
+    c = (rsfm._lib.CasHashPair * len(arr))(*arr)
+    rsfm._lib.check(lib.rsfm_cashash_find_best_match_pairs(c, len(arr), flags, None), "pairs")
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    for ((qd, qk, qi), (td, tk, ti)), (a, b) in zip(imgs, res):
+        got_q = a.cpu().numpy().view(np.uint32).reshape(-1, 2)[:len(qd)]
+        got_t = b.cpu().numpy().view(np.uint32).reshape(-1, 2)[:len(td)]
+        if len(qd) == 0 or len(td) == 0:
+            assert (got_q == 0xFFFFFFFF).all() and (got_t == 0xFFFFFFFF).all()
+            continue
+        eq, et = oracle.cashash_find_best_match(qd, qi["upper"], qi["host_buckets"], td, ti["upper"],
+                                                ti["host_buckets"], per_scheme=bool(flags))
+        np.testing.assert_array_equal(got_q, eq)
+        np.testing.assert_array_equal(got_t, et)
