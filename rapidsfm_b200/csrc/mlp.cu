@@ -93,23 +93,37 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
     const uint32_t laneBase = (32u * q) << 16;
     const uint32_t row = 32u * q + lane;
 
-    // thread t converts half t%2 of row t/2 (64 bytes -> 64 bf16 = one panel row)
-    auto convert_x = [&](uint32_t tile) {
-        const uint32_t r = tid >> 1, hh = tid & 1u, i = tile * 128u + r;
-        uint4 raw[4] = {};
-        if (i < n) {
-            const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 64 * hh);
+    // Thread t converts half t%2 of row t/2 (64 bytes -> 64 bf16 = one panel row). The raw bytes of
+    // a tile are loaded into registers one tile ahead (fetch_x), so their DRAM latency overlaps
+    // the previous tile's work instead of sitting between the two layers' MMAs.
+    uint4 raw[4];
+    auto fetch_x = [&](uint32_t tile) {
+        const uint32_t i = tile * 128u + (tid >> 1);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) raw[k] = src[k];
+        for (int k = 0; k < 4; ++k) raw[k] = make_uint4(0, 0, 0, 0);
+        if (i < n) {
+            const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 64 * (tid & 1u));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) raw[k] = __ldg(&src[k]);
         }
-        const uint8_t* b = reinterpret_cast<const uint8_t*>(raw);
+    };
+    // x / 64 in bf16, exact for x in 0..255: the float with bits 0x4B0000xx is 2^23 + x, so
+    // fma(that, 2^-6, -2^17) = x / 64 exactly, and its low 16 bits are zero (the bf16 is its top half).
+    auto bf16x2_of_bytes = [](uint32_t w, uint32_t lo, uint32_t hi) {
+        const float a = __fmaf_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + lo)), 1.f / 64, -131072.f);
+        const float b = __fmaf_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + hi)), 1.f / 64, -131072.f);
+        return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632u);
+    };
+    auto convert_x = [&]() {
+        const uint32_t r = tid >> 1, hh = tid & 1u;
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(raw);
 #pragma unroll
         for (uint32_t c = 0; c < 8; ++c) {
             uint4 o;
-            o.x = pack_bf16x2(b[8 * c + 0] * (1.f / 64), b[8 * c + 1] * (1.f / 64));
-            o.y = pack_bf16x2(b[8 * c + 2] * (1.f / 64), b[8 * c + 3] * (1.f / 64));
-            o.z = pack_bf16x2(b[8 * c + 4] * (1.f / 64), b[8 * c + 5] * (1.f / 64));
-            o.w = pack_bf16x2(b[8 * c + 6] * (1.f / 64), b[8 * c + 7] * (1.f / 64));
+            o.x = bf16x2_of_bytes(w[2 * c], 0, 1);
+            o.y = bf16x2_of_bytes(w[2 * c], 2, 3);
+            o.z = bf16x2_of_bytes(w[2 * c + 1], 0, 1);
+            o.w = bf16x2_of_bytes(w[2 * c + 1], 2, 3);
             *reinterpret_cast<uint4*>(S.x[hh] + sw128(r, c)) = o;
         }
         fence_proxy_async_smem();
@@ -141,7 +155,9 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
 
     uint32_t ph1 = 0, ph2 = 0;
     if (blockIdx.x * 128u < n) {
-        convert_x(blockIdx.x);
+        fetch_x(blockIdx.x);
+        convert_x();
+        if (blockIdx.x + gridDim.x < (n + 127u) / 128u) fetch_x(blockIdx.x + gridDim.x);
         __syncthreads();
         issue_layer1();
     }
@@ -177,7 +193,10 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
         fence_proxy_async_smem();
         __syncthreads();  // H complete; TMEM columns 0-255 read; X free (layer 1 done)
         issue_layer2();
-        if (hasNext) convert_x(next);
+        if (hasNext) {
+            convert_x();  // tile `next`, fetched one tile ago
+            if (next + gridDim.x < (n + 127u) / 128u) fetch_x(next + gridDim.x);
+        }
         tc_fence_before();
         __syncthreads();  // next X complete
         if (hasNext) issue_layer1();  // TMEM columns 0-255 are free: their reads finished above
