@@ -346,6 +346,14 @@ __global__ void __launch_bounds__(kThreads) match_pairs_kernel(const PairDev* __
 
 using namespace rsfm_b200;
 
+// Resident CTAs per SM for the persistent item kernels: each holds ~28 KB of shared memory and
+// 64 TMEM columns, so eight fit (512 columns); more CTAs hide more of an item's chain of
+// dependent loads (bucket bounds, member lists, rows).
+#ifndef RSFM_FBM_CTAS_PER_SM
+#define RSFM_FBM_CTAS_PER_SM 8
+#endif
+constexpr uint32_t kFbmCtasPerSm = RSFM_FBM_CTAS_PER_SM;
+
 static int find_best_match_impl(const rsfm_cashash_image* queries, const uint32_t* querySize,
                                 const rsfm_cashash_image* train, uint32_t trainSize,
                                 const rsfm_cashash_result* results, uint32_t nbTasks, uint32_t flags,
@@ -404,7 +412,7 @@ static int find_best_match_impl(const rsfm_cashash_image* queries, const uint32_
         }
         const uint32_t maxN = std::max(std::max(maxQ, trainSize), 1u);
         chm::init_kernel<<<dim3((maxN + 255) / 256, n), 256, 0, stream>>>(P, trainSize, maxQ, qSizes);
-        const uint32_t grid = uint32_t(4 * sm_count());
+        const uint32_t grid = uint32_t(kFbmCtasPerSm * sm_count());
         void* tok = nullptr;
         const bool prof = profile_begin(stream, &tok);
         chm::match_kernel<<<grid, chm::kThreads, smem, stream>>>(P, trainSize, qSizes);
@@ -475,7 +483,7 @@ extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs
                                                                                                           counter);
         void* tok = nullptr;
         const bool prof = profile_begin(stream, &tok);
-        chm::match_pairs_kernel<<<uint32_t(4 * sm_count()), chm::kThreads, smem, stream>>>(
+        chm::match_pairs_kernel<<<uint32_t(kFbmCtasPerSm * sm_count()), chm::kThreads, smem, stream>>>(
             table, nbPairs, (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u, counter, device_error_word());
         if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
         if (prof) profile_end(stream, tok);
