@@ -361,6 +361,34 @@ typedef struct rsfm_mlp {
 int rsfm_mlp_hash(const rsfm_mlp* model, const void* desc, uint32_t nbDesc, uint8_t* keys, uint32_t* codes,
                   float* outputs, cudaStream_t stream);
 
+/* Batched registration of images for ranked matching (no reference counterpart; the reference
+ * prepares one image per call, bruteForceMatcher.cpp:63-107). The hasher is the random projection
+ * (weights/bias with nbChannels = 192: keys + 128-bit codes, histogram fused) or, when mlp is
+ * non-NULL, the learned hash. Per job all outputs are device memory sized for nbDesc descriptors:
+ * keys [n][8] (8-byte aligned), codes [n][4] (16-byte aligned), sqrNormDesc [n], bucketEnds
+ * [8][256] inclusive upper bounds, maxBucketSize [1], buckets [8][n] (bucket lists at
+ * s * n + lower), records [n][8] words (32-byte aligned). scratch: device uint32 [2][8][256],
+ * reused image after image. Everything is enqueued on `stream`; nothing synchronizes. */
+typedef struct rsfm_ranked_hasher {
+    const void* weights;
+    const int32_t* bias;
+    int channels;
+    const rsfm_mlp* mlp;
+} rsfm_ranked_hasher;
+typedef struct rsfm_ranked_image_job {
+    const void* desc;
+    uint32_t nbDesc;
+    uint8_t* keys;
+    uint32_t* codes;
+    uint32_t* sqrNormDesc;
+    uint32_t* bucketEnds;
+    uint32_t* maxBucketSize;
+    uint32_t* buckets;
+    uint32_t* records;
+} rsfm_ranked_image_job;
+int rsfm_ranked_register_images(const rsfm_ranked_hasher* hasher, const rsfm_ranked_image_job* jobs, uint32_t nbJobs,
+                                uint32_t* scratch, cudaStream_t stream);
+
 /* Triplet trainer for the learned hash. Parameters are one f32 block w1 | b1 | w2 | b2
  * (32768 + 256 + 32768 + 128 floats); the trainer keeps fp32 masters, Adam moments (beta 0.9 /
  * 0.999, eps 1e-8) and the bf16 copies the hash reads. Loss per triplet (anchor, positive,

@@ -70,6 +70,19 @@ class CasHashResult(ctypes.Structure):
     _fields_ = [("query", ctypes.c_void_p), ("train", ctypes.c_void_p)]
 
 
+class RankedHasher(ctypes.Structure):
+    """rsfm_ranked_hasher: random projection (weights, bias, channels) or learned hash (mlp)."""
+    _fields_ = [("weights", ctypes.c_void_p), ("bias", ctypes.c_void_p), ("channels", ctypes.c_int),
+                ("mlp", ctypes.c_void_p)]
+
+
+class RankedImageJob(ctypes.Structure):
+    """rsfm_ranked_image_job: one image of rsfm_ranked_register_images."""
+    _fields_ = [("desc", ctypes.c_void_p), ("nbDesc", ctypes.c_uint32), ("keys", ctypes.c_void_p),
+                ("codes", ctypes.c_void_p), ("sqrNormDesc", ctypes.c_void_p), ("bucketEnds", ctypes.c_void_p),
+                ("maxBucketSize", ctypes.c_void_p), ("buckets", ctypes.c_void_p), ("records", ctypes.c_void_p)]
+
+
 class CasHashPair(ctypes.Structure):
     """rsfm_cashash_pair (one independent pair of a batched findBestMatch)."""
     _fields_ = [("query", CasHashImage), ("train", CasHashImage), ("querySize", ctypes.c_uint32),
@@ -152,6 +165,8 @@ SIGNATURES = {
                                                     ctypes.POINTER(CasHashImage), ctypes.c_uint32,
                                                     ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_void_p,
                                                     ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_ranked_register_images": (ctypes.c_int, [ctypes.POINTER(RankedHasher), ctypes.POINTER(RankedImageJob),
+                                                   ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_pairs": (ctypes.c_int, [ctypes.POINTER(CasHashPair), ctypes.c_uint32,
                                                           ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,

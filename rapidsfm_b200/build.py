@@ -20,6 +20,7 @@ SOURCES = [
     "bf_variants.cu",
     "filters.cu",
     "ransac.cu",
+    "ranked_register.cpp",
     "bf_autotune.cpp",
     "host_filters.cpp",
     "diag.cu",

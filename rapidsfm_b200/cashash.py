@@ -57,6 +57,15 @@ class RankedImage:
                    "rsfm_ranked_pack_records")
         self.n = n
 
+    @classmethod
+    def from_parts(cls, desc, keys, codes, sqr, upper, max_bucket, buckets, records):
+        """An image whose buffers were filled elsewhere (register_ranked_images)."""
+        self = cls.__new__(cls)
+        self.desc, self.keys, self.codes, self.sqr = desc, keys, codes, sqr
+        self.upper, self._max, self.buckets, self.records = upper, max_bucket, buckets, records
+        self.n = desc.shape[0]
+        return self
+
     def max_bucket_size(self):
         return int(self._max.item())
 
@@ -64,6 +73,51 @@ class RankedImage:
         return _lib.RankedImage(self.desc.data_ptr(), self.keys.data_ptr(), self.codes.data_ptr(),
                                 self.upper.data_ptr(), self.buckets.data_ptr(), self.sqr.data_ptr(), self.n,
                                 self.records.data_ptr())
+
+
+def register_ranked_images(hasher, descs, stream=None):
+    """Hashes and indexes many images with one library call (rsfm_ranked_register_images): per image
+    the 8 bucket keys, the 128-bit code, squared norms, bucket bounds and lists and the packed
+    records. hasher: a CasHash with 192 channels or a learned_hash.LearnedHash. Returns one
+    RankedImage per descriptor tensor; their buffers are views of a few shared allocations."""
+    lib = _lib.load()
+    for d in descs:
+        _check_desc(d)
+    if not descs:
+        return []
+    dev = descs[0].device
+    ns = [int(d.shape[0]) for d in descs]
+    offs = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    total = max(int(offs[-1]), 1)
+    keys = torch.empty((total, 8), dtype=torch.uint8, device=dev)
+    codes = torch.empty((total, 4), dtype=torch.int32, device=dev)
+    sqr = torch.empty(total, dtype=torch.int32, device=dev)
+    buckets = torch.empty(8 * total, dtype=torch.int32, device=dev)
+    records = torch.empty((total, 8), dtype=torch.int32, device=dev)
+    upper = torch.empty((len(descs), 8, 256), dtype=torch.int32, device=dev)
+    maxb = torch.empty(len(descs), dtype=torch.int32, device=dev)
+    scratch = torch.empty((2, 8, 256), dtype=torch.int32, device=dev)
+    if hasattr(hasher, "model"):  # learned hash
+        h = _lib.RankedHasher(None, None, 0, ctypes.cast(ctypes.pointer(hasher.model), ctypes.c_void_p))
+    else:
+        if hasher.channels != 192:
+            raise ValueError("ranked matching needs the 192-channel projection (keys and 128-bit codes)")
+        h = _lib.RankedHasher(hasher.w.data_ptr(), hasher.bias.data_ptr(), 192, None)
+    imgs, jobs = [], []
+    for k, (d, n) in enumerate(zip(descs, ns)):
+        o = int(offs[k])
+        img = RankedImage.from_parts(d, keys[o:o + n], codes[o:o + n], sqr[o:o + n], upper[k], maxb[k:k + 1],
+                                     buckets[8 * o:8 * (o + n)].view(8, n), records[o:o + n])
+        imgs.append(img)
+        jobs.append(_lib.RankedImageJob(d.data_ptr(), n, keys[o].data_ptr() if n else keys.data_ptr(),
+                                        codes[o].data_ptr() if n else codes.data_ptr(),
+                                        sqr[o].data_ptr() if n else sqr.data_ptr(), upper[k].data_ptr(),
+                                        maxb[k].data_ptr(), buckets[8 * o].data_ptr() if n else buckets.data_ptr(),
+                                        records[o].data_ptr() if n else records.data_ptr()))
+    arr = (_lib.RankedImageJob * len(jobs))(*jobs)
+    _lib.check(lib.rsfm_ranked_register_images(ctypes.byref(h), arr, len(jobs), _p(scratch), _stream_ptr(stream)),
+               "rsfm_ranked_register_images")
+    return imgs
 
 
 def match_ranked(query, train, tables=6, top_k=10, ratio_num=RATIO_NUM_08, ratio_den=RATIO_DEN_08,

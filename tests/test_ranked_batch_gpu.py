@@ -61,3 +61,28 @@ def test_cascade_matcher_fallback_is_exact(rsfm, oracle):
     assert cm2.fallback_pairs == []
     agree = (b2.cpu().numpy().view(np.uint32).reshape(-1, 2)[:, 0] == efwd[:, 0]).mean()
     assert agree > 0.5
+
+
+@pytest.mark.parametrize("kind", ["projection", "learned"])
+def test_register_images_matches_per_image(rsfm, kind):
+    """One rsfm_ranked_register_images call gives every image exactly the buffers the per-image
+    path builds (keys, codes, norms, bucket bounds and lists, records, largest bucket)."""
+    from rapidsfm_b200 import cashash as ch
+    from rapidsfm_b200 import learned_hash as lh
+    rng = np.random.default_rng(11)
+    descs = [_dev(synth.make_pair(n, 1, 0.5, 8.0, seed=int(rng.integers(1 << 30)))[0]) for n in (3000, 1, 700, 4096)]
+    if kind == "projection":
+        h = ch.CasHash(ch.gaussian_weights(6))
+        for d in descs:
+            h.fit(d)
+    else:
+        h = lh.LearnedHash(np.load(lh.default_params_path()))
+    got = ch.register_ranked_images(h, descs)
+    torch.cuda.synchronize()
+    for d, g in zip(descs, got):
+        k, c = h.hash(d)[:2]
+        e = ch.RankedImage(d, k, c)
+        torch.cuda.synchronize()
+        for name in ("keys", "codes", "sqr", "upper", "buckets", "records"):
+            assert torch.equal(getattr(g, name), getattr(e, name)), name
+        assert g.max_bucket_size() == e.max_bucket_size()
