@@ -86,3 +86,23 @@ def test_register_images_matches_per_image(rsfm, kind):
         for name in ("keys", "codes", "sqr", "upper", "buckets", "records"):
             assert torch.equal(getattr(g, name), getattr(e, name)), name
         assert g.max_bucket_size() == e.max_bucket_size()
+
+
+def test_batch_with_empty_train_image(rsfm):
+    """A pair whose train image has no descriptors: no candidates, best {~0, ~0}, no fault."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(9))
+    q, t, _ = synth.make_pair(500, 400, 0.5, 8.0, seed=91)
+    dq, dt = _dev(q), _dev(t)
+    cas.fit(dq)
+    empty = torch.empty((0, 128), dtype=torch.uint8, device="cuda")
+    imgs = ch.register_ranked_images(cas, [dq, dt, empty])
+    batch = ch.RankedBatch([(imgs[0], imgs[2]), (imgs[0], imgs[1])], 6, 10, count_candidates=True)
+    (b0, s0, f0, c0), (b1, s1, f1, c1) = batch.launch()
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    assert bool((b0 == -1).all()) and int(c0.sum()) == 0 and int(f0.sum()) == 0
+    eb, es, ef, ec = ch.match_ranked(imgs[0], imgs[1], 6, 10, count_candidates=True)
+    torch.cuda.synchronize()
+    assert torch.equal(b1, eb) and torch.equal(c1, ec)
+    batch.close()
