@@ -593,13 +593,7 @@ static int epilogue_groups() {
 
 template <int kWG>
 static int ensure_attr() {
-    static bool attrSet = false;
-    if (!attrSet) {
-        RSFM_CUDA_TRY(cudaFuncSetAttribute(bf_match_kernel<kWG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(smem_bytes<kWG>())));
-        attrSet = true;
-    }
-    return RSFM_OK;
+    return set_max_dynamic_smem(reinterpret_cast<const void*>(bf_match_kernel<kWG>), smem_bytes<kWG>());
 }
 
 template <int kWG>

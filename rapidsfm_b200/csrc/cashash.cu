@@ -365,11 +365,8 @@ int hash_launch(const void* weights, const int32_t* bias, int channels, const vo
     st = encode_desc_tmap(&tmW, weights, uint64_t(channels), 64);
     if (st != RSFM_OK) return st;
     const size_t smem = sizeof(HashSmem) + 1024;
-    static bool attr = false;
-    if (!attr) {
-        RSFM_CUDA_TRY(cudaFuncSetAttribute(hash_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr = true;
-    }
+    st = set_max_dynamic_smem(reinterpret_cast<const void*>(hash_kernel), smem);
+    if (st != RSFM_OK) return st;
     const uint32_t tiles = (n + 127) / 128;
     const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(sm_count()));
     void* tok = nullptr;

@@ -369,11 +369,10 @@ static int find_best_match_impl(const rsfm_cashash_image* queries, const uint32_
     if (ps != RSFM_OK) return ps;
     RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&counter), 4 + 4 * chm::kMaxTasks, pool, stream));
     qSizes = counter + 1;
-    static bool attr = false;
     const size_t smem = sizeof(chm::Smem) + 1024;
-    if (!attr) {
-        RSFM_CUDA_TRY(cudaFuncSetAttribute(chm::match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr = true;
+    {
+        const int sa = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_kernel), smem);
+        if (sa != RSFM_OK) return sa;
     }
     int st = RSFM_OK;
     for (uint32_t i0 = 0; i0 < nbTasks && st == RSFM_OK; i0 += chm::kMaxTasks) {
@@ -469,15 +468,8 @@ extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs
     int st = RSFM_OK;
     // pageable source: the copy is staged before the call returns, so `host` may go out of scope
     if (cudaMemcpyAsync(table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) st = RSFM_ERR_CUDA;
-    static bool attr = false;
     const size_t smem = sizeof(chm::Smem) + 1024;
-    if (st == RSFM_OK && !attr) {
-        if (cudaFuncSetAttribute(chm::match_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
-            cudaSuccess)
-            st = RSFM_ERR_CUDA;
-        else
-            attr = true;
-    }
+    if (st == RSFM_OK) st = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_pairs_kernel), smem);
     if (st == RSFM_OK) {
         chm::pairs_init_kernel<<<dim3(std::min<uint32_t>((maxN + 255) / 256, 64u), nbPairs), 256, 0, stream>>>(table,
                                                                                                           counter);

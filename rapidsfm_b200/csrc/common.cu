@@ -1,5 +1,9 @@
 // Host helpers: tensor-map encoding, device error word, status strings, launch accounting.
 #include "common.h"
+
+#include <mutex>
+#include <set>
+#include <utility>
 #include <cudaTypedefs.h>
 #include <mutex>
 #include <cstdio>
@@ -127,3 +131,19 @@ extern "C" const char* rsfm_status_string(int status) {
 extern "C" uint32_t rsfm_last_launch_count(void) { return t_launches; }
 
 extern "C" const char* rsfm_last_cuda_error(void) { return t_last_error; }
+
+namespace rsfm_b200 {
+
+int set_max_dynamic_smem(const void* kernel, size_t bytes) {
+    int dev = 0;
+    RSFM_CUDA_TRY(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({kernel, dev})) return RSFM_OK;
+    RSFM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    done.insert({kernel, dev});
+    return RSFM_OK;
+}
+
+}  // namespace rsfm_b200

@@ -36,6 +36,9 @@ int encode_desc_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint32_t
 int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows);
 
 int sm_count();
+// Raises a kernel's dynamic shared-memory limit on the current device, once per (kernel, device):
+// the attribute belongs to the device's context, so a process using several GPUs sets it on each.
+int set_max_dynamic_smem(const void* kernel, size_t bytes);
 // Stream-ordered scratch pool of this library on the current device (keeps its memory).
 int scratch_pool(cudaMemPool_t* pool);
 

@@ -459,10 +459,9 @@ extern "C" int rsfm_mlp_hash(const rsfm_mlp* m, const void* desc, uint32_t nbDes
         (reinterpret_cast<uintptr_t>(keys) & 7u))
         return RSFM_ERR_INVALID_ARG;
     const size_t smem = sizeof(mlp::InfSmem) + 1024;
-    static bool attr = false;
-    if (!attr) {
-        RSFM_CUDA_TRY(cudaFuncSetAttribute(mlp::infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr = true;
+    {
+        const int sa = set_max_dynamic_smem(reinterpret_cast<const void*>(mlp::infer_kernel), smem);
+        if (sa != RSFM_OK) return sa;
     }
     const uint32_t tiles = (nbDesc + 127) / 128;
     const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(sm_count()));
