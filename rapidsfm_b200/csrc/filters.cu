@@ -8,8 +8,9 @@
 // cross to the host instead of both BestMatch arrays (bruteForceMatcher.cpp:355-369 copies those).
 //
 // Both are stable compactions: pass 1 counts the survivors of each 4096-item block; pass 2 has
-// every block sum the counts before it, re-evaluate its items, scan them and write its records in
-// order (the block with the last items also writes the total). Conflict removal first reduces the
+// every block sum the counts before it (above 1024 blocks a one-CTA scan pass does that first),
+// re-evaluate its items, scan them and write its records in order (the block with the last items
+// also writes the total). Conflict removal first reduces the
 // queries per train descriptor with a 64-bit atomicMin on (distance << 32 | query), which is the
 // lexicographic minimum the strict-< loop keeps.
 #include "common.h"
@@ -70,16 +71,53 @@ __global__ void __launch_bounds__(kThreads) count_kernel(Src src, uint32_t* __re
     }
 }
 
+// Exclusive prefix of the block counts in place, one CTA of kThreads walking them in chunks
+// (used when there are many blocks; with few, each block sums the counts before it itself).
+__global__ void __launch_bounds__(kThreads) scan_kernel(uint32_t* __restrict__ counts, uint32_t n) {
+    __shared__ uint32_t warpSum[kThreads / 32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += kThreads) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n ? counts[i] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        if (lane == 31) warpSum[warp] = incl;
+        __syncthreads();
+        uint32_t before = carry, total = 0;
+        for (uint32_t w = 0; w < kThreads / 32; ++w) {
+            if (w < warp) before += warpSum[w];
+            total += warpSum[w];
+        }
+        if (i < n) counts[i] = before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+constexpr uint32_t kDirectSumBlocks = 1024;  // up to this many blocks, each sums its predecessors
+
 template <class Src>
 __global__ void __launch_bounds__(kThreads) write_kernel(Src src, const uint32_t* __restrict__ blockCounts,
-                                                         rsfm_valid_match* __restrict__ out,
+                                                         bool scanned, rsfm_valid_match* __restrict__ out,
                                                          uint32_t* __restrict__ count) {
     __shared__ uint32_t warpSum[kThreads / 32];
     __shared__ uint32_t blockOffset;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // records before this block
+    // records before this block (already an exclusive prefix when `scanned`)
     uint32_t before = 0;
-    for (uint32_t k = threadIdx.x; k < blockIdx.x; k += kThreads) before += blockCounts[k];
+    if (scanned) {
+        if (threadIdx.x == 0) before = blockCounts[blockIdx.x];
+    } else {
+        for (uint32_t k = threadIdx.x; k < blockIdx.x; k += kThreads) before += blockCounts[k];
+    }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
     if (lane == 0) warpSum[warp] = before;
@@ -144,7 +182,13 @@ int compact(const Src& src, uint32_t items, rsfm_valid_match* out, uint32_t* cou
     const uint32_t blocks = (items + kPerBlock - 1) / kPerBlock;
     count_kernel<Src><<<blocks, kThreads, 0, stream>>>(src, blockCounts);
     RSFM_CUDA_TRY(cudaGetLastError());
-    write_kernel<Src><<<blocks, kThreads, 0, stream>>>(src, blockCounts, out, count);
+    const bool scanned = blocks > kDirectSumBlocks;
+    if (scanned) {
+        scan_kernel<<<1, kThreads, 0, stream>>>(blockCounts, blocks);
+        RSFM_CUDA_TRY(cudaGetLastError());
+        ++*launches;
+    }
+    write_kernel<Src><<<blocks, kThreads, 0, stream>>>(src, blockCounts, scanned, out, count);
     RSFM_CUDA_TRY(cudaGetLastError());
     *launches += 2;
     return RSFM_OK;

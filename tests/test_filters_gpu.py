@@ -18,20 +18,27 @@ def _best_tensor(a):
 def _random_best(rng, nq, nt, dist_hi=50):
     fwd = np.stack([rng.integers(0, nt, nq), rng.integers(0, dist_hi, nq)], 1).astype(np.uint32)
     bwd = np.stack([rng.integers(0, nq, nt), rng.integers(0, dist_hi, nt)], 1).astype(np.uint32)
-    for j in range(0, nt, 2):  # plant mutual pairs
-        i = rng.integers(0, nq)
-        fwd[i, 0] = j
-        bwd[j, 0] = i
+    js = np.arange(0, nt, 2)  # plant mutual pairs
+    iq = rng.integers(0, nq, len(js))
+    fwd[iq, 0] = js
+    bwd[js, 0] = iq
     fwd[rng.integers(0, nq, max(1, nq // 20)), 0] = 0xFFFFFFFF        # no match
     fwd[rng.integers(0, nq, max(1, nq // 50)), 0] = nt + 5            # out of range: skipped
     fwd[rng.integers(0, nq, max(1, nq // 50)), 1] = 0xFFFFFFFF        # distance ~0u
     return fwd, bwd
 
 
-@pytest.mark.parametrize("nq,nt", [(1, 1), (700, 500), (4096, 4097), (20000, 9000), (9000, 20000)])
+@pytest.mark.parametrize("nq,nt", [(1, 1), (700, 500), (4096, 4097), (20000, 9000), (9000, 20000),
+                                   (5_000_000, 4_500_000)])  # the last: more than 1024 blocks (scan pass)
 def test_device_filters_match_host(rsfm, oracle, nq, nt):
     rng = np.random.default_rng(nq + nt)
     fwd, bwd = _random_best(rng, nq, nt)
+    if nq > 1_000_000:  # the host filters are the reference here; the oracle loop is skipped
+        out, cnt = rsfm.filter_matches_device(_best_tensor(fwd), _best_tensor(bwd))
+        np.testing.assert_array_equal(rsfm.valid_matches_to_host(out, cnt), rsfm.cross_check_matches(fwd, bwd))
+        out, cnt = rsfm.filter_matches_device(_best_tensor(fwd), nb_train=nt, cross_check=False)
+        np.testing.assert_array_equal(rsfm.valid_matches_to_host(out, cnt), rsfm.remove_match_conflicts(fwd, nt))
+        return
     out, cnt = rsfm.filter_matches_device(_best_tensor(fwd), _best_tensor(bwd))
     got = rsfm.valid_matches_to_host(out, cnt)
     exp = rsfm.cross_check_matches(fwd, bwd)
