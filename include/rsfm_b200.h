@@ -389,6 +389,17 @@ typedef struct rsfm_ranked_image_job {
 int rsfm_ranked_register_images(const rsfm_ranked_hasher* hasher, const rsfm_ranked_image_job* jobs, uint32_t nbJobs,
                                 uint32_t* scratch, cudaStream_t stream);
 
+/* rsfm_ranked_register_images for images stored back to back (no reference counterpart): desc
+ * holds all images' descriptors, image i being rows imageBegin[i] .. imageBegin[i + 1] - 1
+ * (imageBegin: host array of nbImages + 1, imageBegin[0] = 0); keys, codes, sqrNormDesc and
+ * records are laid out the same way; buckets holds image i's lists [8][n_i] at 8 * imageBegin[i];
+ * bucketEnds [nbImages][8][256]; maxBucketSize [nbImages]. The per-descriptor steps (hash, norms,
+ * records) run once over all descriptors and each bucket-build step once for all images. */
+int rsfm_ranked_register_flat(const rsfm_ranked_hasher* hasher, const void* desc, const uint32_t* imageBegin,
+                              uint32_t nbImages, uint8_t* keys, uint32_t* codes, uint32_t* sqrNormDesc,
+                              uint32_t* bucketEnds, uint32_t* maxBucketSize, uint32_t* buckets, uint32_t* records,
+                              cudaStream_t stream);
+
 /* Triplet trainer for the learned hash. Parameters are one f32 block w1 | b1 | w2 | b2
  * (32768 + 256 + 32768 + 128 floats); the trainer keeps fp32 masters, Adam moments (beta 0.9 /
  * 0.999, eps 1e-8) and the bf16 copies the hash reads. Loss per triplet (anchor, positive,

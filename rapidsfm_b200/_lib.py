@@ -167,6 +167,10 @@ SIGNATURES = {
                                                     ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_ranked_register_images": (ctypes.c_int, [ctypes.POINTER(RankedHasher), ctypes.POINTER(RankedImageJob),
                                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_ranked_register_flat": (ctypes.c_int, [ctypes.POINTER(RankedHasher), ctypes.c_void_p,
+                                                 ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_pairs": (ctypes.c_int, [ctypes.POINTER(CasHashPair), ctypes.c_uint32,
                                                           ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,

@@ -75,11 +75,66 @@ class RankedImage:
                                 self.records.data_ptr())
 
 
+def _ranked_hasher(hasher):
+    if hasattr(hasher, "model"):  # learned hash
+        return _lib.RankedHasher(None, None, 0, ctypes.cast(ctypes.pointer(hasher.model), ctypes.c_void_p))
+    if hasher.channels != 192:
+        raise ValueError("ranked matching needs the 192-channel projection (keys and 128-bit codes)")
+    return _lib.RankedHasher(hasher.w.data_ptr(), hasher.bias.data_ptr(), 192, None)
+
+
 def register_ranked_images(hasher, descs, stream=None):
-    """Hashes and indexes many images with one library call (rsfm_ranked_register_images): per image
-    the 8 bucket keys, the 128-bit code, squared norms, bucket bounds and lists and the packed
-    records. hasher: a CasHash with 192 channels or a learned_hash.LearnedHash. Returns one
-    RankedImage per descriptor tensor; their buffers are views of a few shared allocations."""
+    """Hashes and indexes many images at once (rsfm_ranked_register_flat): per image the 8 bucket
+    keys, the 128-bit code, squared norms, bucket bounds and lists and the packed records. The
+    descriptors are first copied back to back into one buffer; every per-descriptor step then runs
+    once over all of them and every bucket-build step once for all images. hasher: a CasHash with
+    192 channels or a learned_hash.LearnedHash. Returns one RankedImage per input (views of shared
+    buffers, including the packed copy of its descriptors)."""
+    lib = _lib.load()
+    for d in descs:
+        _check_desc(d)
+    if not descs:
+        return []
+    dev = descs[0].device
+    ns = [int(d.shape[0]) for d in descs]
+    offs = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    total = int(offs[-1])
+    if total >= (1 << 32):
+        raise ValueError("at most 2^32 - 1 descriptors per registration call")
+    cap = max(total, 1)
+    with torch.cuda.stream(stream) if stream is not None else _nullctx():
+        flat = torch.cat(descs) if total else torch.empty((1, 128), dtype=torch.uint8, device=dev)
+    keys = torch.empty((cap, 8), dtype=torch.uint8, device=dev)
+    codes = torch.empty((cap, 4), dtype=torch.int32, device=dev)
+    sqr = torch.empty(cap, dtype=torch.int32, device=dev)
+    buckets = torch.empty(8 * cap, dtype=torch.int32, device=dev)
+    records = torch.empty((cap, 8), dtype=torch.int32, device=dev)
+    upper = torch.empty((len(descs), 8, 256), dtype=torch.int32, device=dev)
+    maxb = torch.empty(len(descs), dtype=torch.int32, device=dev)
+    h = _ranked_hasher(hasher)
+    begin = (ctypes.c_uint32 * (len(descs) + 1))(*[int(x) for x in offs])
+    _lib.check(lib.rsfm_ranked_register_flat(ctypes.byref(h), _p(flat), begin, len(descs), _p(keys), _p(codes),
+                                             _p(sqr), _p(upper), _p(maxb), _p(buckets), _p(records),
+                                             _stream_ptr(stream)), "rsfm_ranked_register_flat")
+    imgs = []
+    for k, n in enumerate(ns):
+        o = int(offs[k])
+        imgs.append(RankedImage.from_parts(flat[o:o + n], keys[o:o + n], codes[o:o + n], sqr[o:o + n], upper[k],
+                                           maxb[k:k + 1], buckets[8 * o:8 * (o + n)].view(8, n), records[o:o + n]))
+    return imgs
+
+
+class _nullctx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def register_ranked_images_per_image(hasher, descs, stream=None):
+    """The same with one library call that loops over the images (rsfm_ranked_register_images):
+    for outputs that live in caller-chosen, separate buffers."""
     lib = _lib.load()
     for d in descs:
         _check_desc(d)
@@ -97,12 +152,7 @@ def register_ranked_images(hasher, descs, stream=None):
     upper = torch.empty((len(descs), 8, 256), dtype=torch.int32, device=dev)
     maxb = torch.empty(len(descs), dtype=torch.int32, device=dev)
     scratch = torch.empty((2, 8, 256), dtype=torch.int32, device=dev)
-    if hasattr(hasher, "model"):  # learned hash
-        h = _lib.RankedHasher(None, None, 0, ctypes.cast(ctypes.pointer(hasher.model), ctypes.c_void_p))
-    else:
-        if hasher.channels != 192:
-            raise ValueError("ranked matching needs the 192-channel projection (keys and 128-bit codes)")
-        h = _lib.RankedHasher(hasher.w.data_ptr(), hasher.bias.data_ptr(), 192, None)
+    h = _ranked_hasher(hasher)
     imgs, jobs = [], []
     for k, (d, n) in enumerate(zip(descs, ns)):
         o = int(offs[k])

@@ -264,8 +264,8 @@ __global__ void histogram_kernel(uint32_t* __restrict__ hist, const uint2* __res
 
 // ---------------------------------------------------------------- bucket bounds (one block)
 // Warp s scans scheme s: lane l owns buckets [8l, 8l+8).
-__global__ void bounds_kernel(uint32_t* __restrict__ lower, uint32_t* __restrict__ upper, uint32_t* maxBucket,
-                              const uint32_t* __restrict__ hist) {
+__device__ __forceinline__ void bounds_block(uint32_t* __restrict__ lower, uint32_t* __restrict__ upper, uint32_t* maxBucket,
+                                             const uint32_t* __restrict__ hist) {
     __shared__ uint32_t wmax[8];
     const uint32_t s = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t v[8], sum = 0, mx = 0;
@@ -297,22 +297,30 @@ __global__ void bounds_kernel(uint32_t* __restrict__ lower, uint32_t* __restrict
         *maxBucket = m;
     }
 }
+__global__ void bounds_kernel(uint32_t* __restrict__ lower, uint32_t* __restrict__ upper, uint32_t* maxBucket,
+                              const uint32_t* __restrict__ hist) {
+    bounds_block(lower, upper, maxBucket, hist);
+}
 
 // ---------------------------------------------------------------- buckets (stable)
 constexpr uint32_t kChunk = 1024;
 // (1) per-chunk histograms: chunkHist[c][8][256]
-__global__ void chunk_hist_kernel(uint32_t* __restrict__ chunkHist, const uint2* __restrict__ keys, uint32_t n) {
+// one chunk's 8 x 256 key counts into row (2048 words)
+__device__ __forceinline__ void chunk_hist_block(uint32_t* __restrict__ row, const uint2* __restrict__ keys, uint32_t n,
+                                                 uint32_t c) {
     __shared__ uint32_t h[8][256];
     for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) (&h[0][0])[x] = 0;
     __syncthreads();
-    const uint32_t c = blockIdx.x;
     for (uint32_t i = c * kChunk + threadIdx.x; i < min(n, (c + 1) * kChunk); i += blockDim.x) {
         const uint2 k = keys[i];
 #pragma unroll
         for (int s = 0; s < 8; ++s) atomicAdd(&h[s][((s < 4 ? k.x : k.y) >> (8 * (s & 3))) & 0xFFu], 1u);
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) chunkHist[size_t(c) * 2048 + x] = (&h[0][0])[x];
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) row[x] = (&h[0][0])[x];
+}
+__global__ void chunk_hist_kernel(uint32_t* __restrict__ chunkHist, const uint2* __restrict__ keys, uint32_t n) {
+    chunk_hist_block(chunkHist + size_t(blockIdx.x) * 2048, keys, n, blockIdx.x);
 }
 // (2) per (scheme, bucket): exclusive offsets over chunks, starting at the allocator's lower
 // bound; the allocator ends at the upper bound, like the reference's buildBuckets.
@@ -330,10 +338,11 @@ __global__ void chunk_offsets_kernel(uint32_t* __restrict__ chunkHist, uint32_t*
 }
 // (3) fill: warp s of block c walks chunk c in order for scheme s; ranks within a step come from
 // __match_any_sync, so members land in ascending descriptor order.
-__global__ void __launch_bounds__(256) fill_kernel(const uint8_t* __restrict__ keys, uint32_t n,
-                                                   const uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ buckets) {
+__device__ __forceinline__ void fill_block(const uint8_t* __restrict__ keys, uint32_t n,
+                                           const uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ buckets,
+                                           uint32_t c) {
     __shared__ uint32_t cnt[8][256];
-    const uint32_t s = threadIdx.x >> 5, lane = threadIdx.x & 31u, c = blockIdx.x;
+    const uint32_t s = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     for (uint32_t x = lane; x < 256; x += 32) cnt[s][x] = 0;
     __syncwarp();
     const uint32_t lt = (1u << lane) - 1u;
@@ -352,6 +361,74 @@ __global__ void __launch_bounds__(256) fill_kernel(const uint8_t* __restrict__ k
         if (in && (peers & lt) == 0) cnt[s][key] += __popc(peers);
         __syncwarp();
     }
+}
+__global__ void __launch_bounds__(256) fill_kernel(const uint8_t* __restrict__ keys, uint32_t n,
+                                                   const uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ buckets) {
+    fill_block(keys, n, chunkOff, buckets, blockIdx.x);
+}
+
+// ---------------------------------------------------------------- many images in one layout
+// Images stored back to back (descriptors, keys, records) with buckets [8][n_i] at 8 * begin_i:
+// the per-image steps of the bucket build run for all images in one launch each (grid.y = image),
+// image i's chunk c being chunk chunkBegin[i] + c of the shared chunk scratch.
+struct FlatImages {
+    const uint32_t* begin;       // [nImages + 1] first descriptor of each image
+    const uint32_t* chunkBegin;  // [nImages + 1] first chunk (kChunk descriptors) of each image
+};
+
+__global__ void flat_hist_kernel(uint32_t* __restrict__ hist, const uint2* __restrict__ keys, FlatImages F) {
+    __shared__ uint32_t h[8][256];
+    const uint32_t img = blockIdx.y, c = blockIdx.x;
+    const uint32_t b = F.begin[img], n = F.begin[img + 1] - b;
+    if (c * kChunk >= n) return;
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) (&h[0][0])[x] = 0;
+    __syncthreads();
+    for (uint32_t i = c * kChunk + threadIdx.x; i < min(n, (c + 1) * kChunk); i += blockDim.x) {
+        const uint2 k = keys[b + i];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) atomicAdd(&h[s][((s < 4 ? k.x : k.y) >> (8 * (s & 3))) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < 8 * 256; x += blockDim.x) {
+        const uint32_t v = (&h[0][0])[x];
+        if (v) atomicAdd(&hist[size_t(img) * 2048 + x], v);
+    }
+}
+
+__global__ void flat_bounds_kernel(uint32_t* __restrict__ lower, uint32_t* __restrict__ upper,
+                                   uint32_t* __restrict__ maxBucket, const uint32_t* __restrict__ hist) {
+    const size_t o = size_t(blockIdx.x) * 2048;
+    bounds_block(lower + o, upper + o, maxBucket + blockIdx.x, hist + o);
+}
+
+__global__ void flat_chunk_hist_kernel(uint32_t* __restrict__ chunkHist, const uint2* __restrict__ keys, FlatImages F) {
+    const uint32_t img = blockIdx.y, c = blockIdx.x;
+    const uint32_t b = F.begin[img], n = F.begin[img + 1] - b;
+    if (c * kChunk >= n) return;
+    chunk_hist_block(chunkHist + size_t(F.chunkBegin[img] + c) * 2048, keys + b, n, c);
+}
+
+__global__ void flat_chunk_offsets_kernel(uint32_t* __restrict__ chunkHist, uint32_t* __restrict__ lower, FlatImages F) {
+    const uint32_t img = blockIdx.y;
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= 2048) return;
+    const uint32_t c0 = F.chunkBegin[img], c1 = F.chunkBegin[img + 1];
+    uint32_t run = lower[size_t(img) * 2048 + x];
+    for (uint32_t c = c0; c < c1; ++c) {
+        const uint32_t h = chunkHist[size_t(c) * 2048 + x];
+        chunkHist[size_t(c) * 2048 + x] = run;
+        run += h;
+    }
+    lower[size_t(img) * 2048 + x] = run;
+}
+
+__global__ void __launch_bounds__(256) flat_fill_kernel(const uint8_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ chunkOff,
+                                                        uint32_t* __restrict__ buckets, FlatImages F) {
+    const uint32_t img = blockIdx.y, c = blockIdx.x;
+    const uint32_t b = F.begin[img], n = F.begin[img + 1] - b;
+    if (c * kChunk >= n) return;
+    fill_block(keys + size_t(b) * 8, n, chunkOff + size_t(F.chunkBegin[img]) * 2048, buckets + size_t(b) * 8, c);
 }
 
 int hash_launch(const void* weights, const int32_t* bias, int channels, const void* desc, uint32_t n, uint8_t* keys,
@@ -463,4 +540,81 @@ extern "C" int rsfm_cashash_build_buckets(const uint8_t* bucketIndices, uint32_t
     cudaError_t f = cudaFreeAsync(scratch, stream);
     launch_count_add(3);
     return (e == cudaSuccess && f == cudaSuccess) ? RSFM_OK : RSFM_ERR_CUDA;
+}
+
+extern "C" int rsfm_ranked_register_flat(const rsfm_ranked_hasher* hasher, const void* desc,
+                                         const uint32_t* imageBegin, uint32_t nbImages, uint8_t* keys,
+                                         uint32_t* codes, uint32_t* sqrNormDesc, uint32_t* bucketEnds,
+                                         uint32_t* maxBucketSize, uint32_t* buckets, uint32_t* records,
+                                         cudaStream_t stream) {
+    launch_count_reset();
+    if (nbImages == 0) return RSFM_OK;
+    if (!hasher || !imageBegin || nbImages > 65535u || imageBegin[0] != 0) return RSFM_ERR_INVALID_ARG;
+    const bool mlp = hasher->mlp != nullptr;
+    if (!mlp && (!hasher->weights || !hasher->bias || hasher->channels != 192)) return RSFM_ERR_INVALID_ARG;
+    const uint32_t total = imageBegin[nbImages];
+    std::vector<uint32_t> tables(2 * (size_t(nbImages) + 1));
+    uint32_t maxChunks = 1;
+    for (uint32_t i = 0; i <= nbImages; ++i) {
+        if (i > 0 && imageBegin[i] < imageBegin[i - 1]) return RSFM_ERR_INVALID_ARG;
+        tables[i] = imageBegin[i];
+        if (i > 0) {
+            const uint32_t chunks = (imageBegin[i] - imageBegin[i - 1] + ch::kChunk - 1) / ch::kChunk;
+            tables[nbImages + 1 + i] = tables[nbImages + i] + chunks;
+            maxChunks = std::max(maxChunks, chunks);
+        } else {
+            tables[nbImages + 1] = 0;
+        }
+    }
+    if (total > 0 && (!desc || !keys || !codes || !sqrNormDesc || !buckets || !records)) return RSFM_ERR_INVALID_ARG;
+    if (!bucketEnds || !maxBucketSize) return RSFM_ERR_INVALID_ARG;
+    uint32_t launches = 0;
+    int st = RSFM_OK;
+    if (total > 0) {  // per-descriptor steps over all images at once
+        st = mlp ? rsfm_mlp_hash(hasher->mlp, desc, total, keys, codes, nullptr, stream)
+                 : rsfm_cashash_compute_hash(hasher->weights, hasher->bias, 192, desc, total, keys, codes, nullptr, stream);
+        launches += rsfm_last_launch_count();
+        if (st == RSFM_OK) st = rsfm_precomp_sift_sqr_norm(sqrNormDesc, desc, total, stream);
+        launches += rsfm_last_launch_count();
+        if (st == RSFM_OK) st = rsfm_ranked_pack_records(keys, codes, sqrNormDesc, total, records, stream);
+        launches += rsfm_last_launch_count();
+        if (st != RSFM_OK) return st;
+    }
+    // scratch: tables, histograms and lower bounds per image, chunk histograms
+    const uint32_t chunksTotal = tables[2 * size_t(nbImages) + 1];
+    const size_t tableBytes = (tables.size() * 4 + 255) & ~size_t(255);
+    const size_t perImage = size_t(nbImages) * 2048 * 4;
+    cudaMemPool_t pool = nullptr;
+    st = scratch_pool(&pool);
+    if (st != RSFM_OK) return st;
+    uint8_t* scratch = nullptr;
+    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch),
+                                          tableBytes + 2 * perImage + size_t(chunksTotal) * 2048 * 4, pool, stream));
+    auto* dTables = reinterpret_cast<uint32_t*>(scratch);
+    auto* hist = reinterpret_cast<uint32_t*>(scratch + tableBytes);
+    auto* lower = reinterpret_cast<uint32_t*>(scratch + tableBytes + perImage);
+    auto* chunkHist = reinterpret_cast<uint32_t*>(scratch + tableBytes + 2 * perImage);
+    const ch::FlatImages F{dTables, dTables + nbImages + 1};
+    cudaError_t e = cudaMemcpyAsync(dTables, tables.data(), tables.size() * 4, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, perImage, stream);
+    if (e == cudaSuccess) {
+        const dim3 g(maxChunks, nbImages);
+        const auto* k2 = reinterpret_cast<const uint2*>(keys);
+        ch::flat_hist_kernel<<<g, 256, 0, stream>>>(hist, k2, F);
+        ch::flat_bounds_kernel<<<nbImages, 256, 0, stream>>>(lower, bucketEnds, maxBucketSize, hist);
+        ch::flat_chunk_hist_kernel<<<g, 256, 0, stream>>>(chunkHist, k2, F);
+        ch::flat_chunk_offsets_kernel<<<dim3(8, nbImages), 256, 0, stream>>>(chunkHist, lower, F);
+        ch::flat_fill_kernel<<<g, 256, 0, stream>>>(keys, chunkHist, buckets, F);
+        e = cudaGetLastError();
+        launches += 5;
+    }
+    const cudaError_t f = cudaFreeAsync(scratch, stream);
+    if (e == cudaSuccess) e = f;
+    if (e != cudaSuccess) {
+        set_last_cuda_error(e, "rsfm_ranked_register_flat");
+        return RSFM_ERR_CUDA;
+    }
+    launch_count_reset();
+    launch_count_add(launches);
+    return RSFM_OK;
 }

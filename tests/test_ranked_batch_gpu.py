@@ -77,9 +77,15 @@ def test_register_images_matches_per_image(rsfm, kind):
             h.fit(d)
     else:
         h = lh.LearnedHash(np.load(lh.default_params_path()))
-    got = ch.register_ranked_images(h, descs)
-    torch.cuda.synchronize()
+    for got in (ch.register_ranked_images(h, descs), ch.register_ranked_images_per_image(h, descs)):
+        torch.cuda.synchronize()
+        _check_registered(h, descs, got)
+
+
+def _check_registered(h, descs, got):
+    from rapidsfm_b200 import cashash as ch
     for d, g in zip(descs, got):
+        assert torch.equal(g.desc, d)
         k, c = h.hash(d)[:2]
         e = ch.RankedImage(d, k, c)
         torch.cuda.synchronize()
