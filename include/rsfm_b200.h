@@ -291,7 +291,8 @@ typedef struct rsfm_cashash_pair {
 /* findBestMatch over many independent (query image, train image) pairs in one launch (no
  * reference counterpart: the reference matches the queries of one call against a single train
  * image). Per pair the same results as rsfm_cashash_find_best_match_ex on that pair; `pairs` is
- * a host array (at most 65535); flags as for _ex. */
+ * a host array (at most 65535); flags as for _ex. The call synchronizes `stream` once (the work
+ * list of 32 x 32 sub-items is sized from a device-side count). */
 int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
                                        cudaStream_t stream);
 

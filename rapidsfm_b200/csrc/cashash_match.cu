@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kThreads) match_kernel(const __grid_constant__
     kernel_teardown(tmem);
 }
 
-// Many independent (query image, train image) pairs: items (pair, scheme, bucket) from one counter.
+// Many independent (query image, train image) pairs.
 struct PairDev {
     ImageDev q, t;
     unsigned long long* qBest;
@@ -316,29 +316,220 @@ __global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* c
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *counter = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) match_pairs_kernel(const PairDev* __restrict__ pairs, uint32_t nPairs,
-                                                               uint32_t schemeOffset, uint32_t* counter,
-                                                               uint32_t* err) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem& S = smem_aligned_1024<Smem>(smem_raw);
+// ---------------------------------------------------------------- pairs by 32 x 32 sub-items
+// With one query image per item the buckets hold tens of members, so a 128-row tile per item is
+// mostly padding. Here an item (pair, scheme, bucket) is cut into sub-items of 32 query x 32 train
+// members; a CTA takes four sub-items at once: warp w gathers sub-item w's 32 query rows into A
+// rows 32w.. and its 32 train rows into B rows 32w.., one UMMA (M = N = 128) computes all 128 x 128
+// products, and warp w reads only its diagonal 32 x 32 block of the accumulator. Row and column
+// minima are merged across sub-items by the same 64-bit atomicMin as everywhere else.
+struct SubItem {
+    uint32_t item;  // pair * 2048 + bucket * 8 + scheme
+    uint32_t seg;   // query segment << 16 | train segment
+};
+
+struct SubSmem {
+    uint8_t a[128 * 128];
+    uint8_t b[128 * 128];
+    uint32_t rowQ[128], rowNA[128];
+    uint32_t colT[128], colNB[128];
+    uint64_t mma;
     uint32_t tmem;
-    kernel_setup(S, tmem);
-    const uint32_t idesc = idesc_u8u8_s32(128, 64);
-    uint32_t mmaPhase = 0;
-    for (;;) {
-        if (threadIdx.x == 0) S.item = atomicAdd(counter, 1u);
-        __syncthreads();
-        const uint32_t item = S.item;
-        if (item >= nPairs * 2048u) break;
-        const PairDev& P = pairs[item >> 11];
-        const uint32_t local = item & 2047u;
+};
+
+__device__ __forceinline__ void item_ranges(const PairDev& P, uint32_t local, uint32_t schemeOffset, uint32_t& qb,
+                                            uint32_t& nQ, uint32_t& tb, uint32_t& nT, uint32_t& s) {
+    s = local & 7u;
+    const uint32_t k = local >> 3;
+    const uint32_t* qe = P.q.ends + s * 256;
+    const uint32_t* te = P.t.ends + s * 256;
+    qb = k ? __ldg(&qe[k - 1]) : 0u;
+    nQ = __ldg(&qe[k]) - qb;
+    tb = k ? __ldg(&te[k - 1]) : 0u;
+    nT = __ldg(&te[k]) - tb;
+    qb += s * P.nQ * schemeOffset;
+    tb += s * P.nT * schemeOffset;
+}
+
+// sub-items per item: ceil(nQ / 32) * ceil(nT / 32) (0 for an empty side or pair)
+__global__ void subitem_count_kernel(const PairDev* __restrict__ pairs, uint32_t nItems, uint32_t schemeOffset,
+                                     uint32_t* __restrict__ counts) {
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nItems; it += gridDim.x * blockDim.x) {
+        const PairDev& P = pairs[it >> 11];
+        uint32_t c = 0;
         if (P.nQ && P.nT) {
-            const ItemCtx C{&P.q, &P.qBest, &P.tBest, P.t, 1u, P.nT, schemeOffset, P.tBest != nullptr};
-            process_item(S, C, local & 7u, local >> 3, tmem, idesc, mmaPhase, err);
+            uint32_t qb, nQ, tb, nT, s;
+            item_ranges(P, it & 2047u, schemeOffset, qb, nQ, tb, nT, s);
+            c = ((nQ + 31u) / 32u) * ((nT + 31u) / 32u);
         }
-        __syncthreads();  // S.item is rewritten next
+        counts[it] = c;
     }
-    kernel_teardown(tmem);
+}
+
+// exclusive prefix in place by one CTA of 1024 threads; the total goes to counts[n]
+__global__ void __launch_bounds__(1024) subitem_scan_kernel(uint32_t* __restrict__ counts, uint32_t n) {
+    __shared__ uint32_t warpSum[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n ? counts[i] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        if (lane == 31) warpSum[warp] = incl;
+        __syncthreads();
+        uint32_t before = carry, total = 0;
+        for (uint32_t w = 0; w < 32; ++w) {
+            if (w < warp) before += warpSum[w];
+            total += warpSum[w];
+        }
+        if (i < n) counts[i] = before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[n] = carry;
+}
+
+__global__ void subitem_expand_kernel(const PairDev* __restrict__ pairs, uint32_t nItems, uint32_t schemeOffset,
+                                      const uint32_t* __restrict__ offsets, SubItem* __restrict__ subs) {
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nItems; it += gridDim.x * blockDim.x) {
+        const uint32_t o = offsets[it], c = offsets[it + 1] - o;
+        if (!c) continue;
+        const PairDev& P = pairs[it >> 11];
+        uint32_t qb, nQ, tb, nT, s;
+        item_ranges(P, it & 2047u, schemeOffset, qb, nQ, tb, nT, s);
+        const uint32_t segT = (nT + 31u) / 32u;
+        for (uint32_t x = 0; x < c; ++x) subs[o + x] = SubItem{it, ((x / segT) << 16) | (x % segT)};
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) match_subitems_kernel(const PairDev* __restrict__ pairs,
+                                                                  const SubItem* __restrict__ subs,
+                                                                  const uint32_t* __restrict__ total,
+                                                                  uint32_t schemeOffset, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    SubSmem& S = smem_aligned_1024<SubSmem>(smem_raw);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    if (tid == 0) {
+        mbar_init(&S.mma, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&S.tmem, 128);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    const uint32_t idesc = idesc_u8u8_s32(128, 128);
+    uint32_t mmaPhase = 0;
+    const uint32_t nSubs = *total;
+    // Everything a warp needs for one sub-item, fetched one unit ahead (its chain of dependent
+    // loads - sub-item, bucket bounds, member lists, norms - overlaps the current unit's MMA).
+    struct Fetched {
+        uint32_t q, t, nA, nB;
+        const uint8_t* qd;
+        const uint8_t* td;
+        unsigned long long* qBest;
+        unsigned long long* tBest;
+    };
+    const uint8_t* dummy = reinterpret_cast<const uint8_t*>(subs);  // zero-byte cp.async source
+    auto fetch = [&](uint32_t si) {
+        Fetched f{kNoRow, kNoRow, kBigNorm, kBigNorm, dummy, dummy, nullptr, nullptr};
+        const bool have = si < nSubs;
+        const SubItem sub = have ? subs[si] : SubItem{0u, 0u};
+        const PairDev& P = pairs[sub.item >> 11];
+        uint32_t qb = 0, nQ = 0, tb = 0, nT = 0, s = 0;
+        if (have) item_ranges(P, sub.item & 2047u, schemeOffset, qb, nQ, tb, nT, s);
+        const uint32_t m = (sub.seg >> 16) * 32u + lane, c = (sub.seg & 0xFFFFu) * 32u + lane;
+        f.q = warp_sort(have && m < nQ ? __ldg(&P.q.buckets[qb + m]) : kNoRow, lane);
+        f.t = warp_sort(have && c < nT ? __ldg(&P.t.buckets[tb + c]) : kNoRow, lane);
+        if (f.q != kNoRow) {
+            f.nA = __ldg(&P.q.sqr[f.q]);
+            f.qd = P.q.desc + size_t(f.q) * 128;
+        }
+        if (f.t != kNoRow) {
+            f.nB = __ldg(&P.t.sqr[f.t]);
+            f.td = P.t.desc + size_t(f.t) * 128;
+        }
+        if (have) {
+            f.qBest = P.qBest;
+            f.tBest = P.tBest;
+        }
+        return f;
+    };
+    Fetched cur = fetch(4u * blockIdx.x + warp);
+    for (uint32_t unit = blockIdx.x; 4u * unit < nSubs; unit += gridDim.x) {
+        // ---- warp w: sub-item 4 unit + w (rows and columns sorted by index)
+        const uint32_t row = 32u * warp + lane;
+        S.rowQ[row] = cur.q;
+        S.rowNA[row] = cur.nA;
+        S.colT[row] = cur.t;
+        S.colNB[row] = cur.nB;
+#pragma unroll
+        for (uint32_t ch = 0; ch < 8; ++ch) {
+            cp_async16(S.a + sw128(row, ch), cur.qd + (cur.q != kNoRow ? 16 * ch : 0), cur.q != kNoRow);
+            cp_async16(S.b + sw128(row, ch), cur.td + (cur.t != kNoRow ? 16 * ch : 0), cur.t != kNoRow);
+        }
+        cp_async_wait_all();
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a = smem_u32(S.a), b = smem_u32(S.b);
+#pragma unroll
+            for (uint32_t kk = 0; kk < 4; ++kk)
+                umma_i8(tmem, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk), idesc, kk);
+            umma_commit(&S.mma);
+        }
+        const Fetched nxt = fetch(4u * (unit + gridDim.x) + warp);
+        __syncwarp();
+        mbar_wait(&S.mma, mmaPhase, err, kDevTimeoutAccFull);
+        mmaPhase ^= 1u;
+        tc_fence_after();
+        // ---- epilogue: warp w's diagonal block (TMEM lanes 32w.., columns 32w..)
+        uint32_t x[32];
+        tmem_ld32(tmem + ((32u * warp) << 16) + 32u * warp, x);
+        tmem_wait_ld();
+        const uint32_t nA = S.rowNA[row];
+        const bool rowValid = cur.q != kNoRow;
+        uint32_t rmin = 0xFFFFFFFFu;
+#pragma unroll
+        for (uint32_t k = 0; k < 32; ++k) {
+            const uint32_t d = nA + S.colNB[32 * warp + k] - 2u * x[k];
+            x[k] = d;
+            rmin = min(rmin, (d << 5) | k);  // ties -> lowest column = lowest train index (sorted)
+        }
+        const uint32_t cd = rmin >> 5;
+        if (rowValid && cd < kValidD)
+            atomicMin(&cur.qBest[cur.q], (static_cast<unsigned long long>(cd) << 32) | S.colT[32 * warp + (rmin & 31u)]);
+        if (cur.tBest) {
+            uint32_t mine = 0xFFFFFFFFu;
+#pragma unroll
+            for (uint32_t k = 0; k < 32; ++k) {
+                const uint32_t key = rowValid && x[k] < kValidD ? ((x[k] << 5) | lane) : 0xFFFFFFFFu;
+                const uint32_t mk = __reduce_min_sync(0xffffffffu, key);
+                mine = (lane == k) ? mk : mine;
+            }
+            if (mine != 0xFFFFFFFFu && cur.t != kNoRow)
+                atomicMin(&cur.tBest[cur.t], (static_cast<unsigned long long>(mine >> 5) << 32) |
+                                                 S.rowQ[32 * warp + (mine & 31u)]);
+        }
+        tc_fence_before();
+        __syncthreads();  // tiles and TMEM are reused by the next unit
+        cur = nxt;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 128);
 }
 
 }  // namespace chm
@@ -468,19 +659,49 @@ extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs
     int st = RSFM_OK;
     // pageable source: the copy is staged before the call returns, so `host` may go out of scope
     if (cudaMemcpyAsync(table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) st = RSFM_ERR_CUDA;
-    const size_t smem = sizeof(chm::Smem) + 1024;
-    if (st == RSFM_OK) st = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_pairs_kernel), smem);
+    const uint32_t schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+    const uint32_t nItems = nbPairs * 2048u;
+    uint32_t* offsets = nullptr;
+    chm::SubItem* subs = nullptr;
+    uint32_t nSubs = 0;
+    const size_t smem = sizeof(chm::SubSmem) + 1024;
+    if (st == RSFM_OK) st = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_subitems_kernel), smem);
+    if (st == RSFM_OK && cudaMallocFromPoolAsync(reinterpret_cast<void**>(&offsets), (size_t(nItems) + 1) * 4, pool,
+                                                 stream) != cudaSuccess)
+        st = RSFM_ERR_CUDA;
     if (st == RSFM_OK) {
         chm::pairs_init_kernel<<<dim3(std::min<uint32_t>((maxN + 255) / 256, 64u), nbPairs), 256, 0, stream>>>(table,
                                                                                                           counter);
-        void* tok = nullptr;
-        const bool prof = profile_begin(stream, &tok);
-        chm::match_pairs_kernel<<<uint32_t(kFbmCtasPerSm * sm_count()), chm::kThreads, smem, stream>>>(
-            table, nbPairs, (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u, counter, device_error_word());
-        if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
-        if (prof) profile_end(stream, tok);
-        launch_count_add(2);
+        const uint32_t g = std::min<uint32_t>((nItems + 255) / 256, uint32_t(8 * sm_count()));
+        chm::subitem_count_kernel<<<g, 256, 0, stream>>>(table, nItems, schemeOffset, offsets);
+        chm::subitem_scan_kernel<<<1, 1024, 0, stream>>>(offsets, nItems);
+        launch_count_add(3);
+        // the sub-item list is sized from its count: one read-back (the call synchronizes the stream)
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(&nSubs, offsets + nItems, 4, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            st = RSFM_ERR_CUDA;
     }
+    if (st == RSFM_OK && nSubs > 0) {
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&subs), size_t(nSubs) * sizeof(chm::SubItem), pool,
+                                    stream) != cudaSuccess)
+            st = RSFM_ERR_CUDA;
+        if (st == RSFM_OK) {
+            const uint32_t g = std::min<uint32_t>((nItems + 255) / 256, uint32_t(8 * sm_count()));
+            chm::subitem_expand_kernel<<<g, 256, 0, stream>>>(table, nItems, schemeOffset, offsets, subs);
+            const uint32_t units = (nSubs + 3u) / 4u;
+            const uint32_t grid = std::min<uint32_t>(units, uint32_t(4 * sm_count()));  // 4 x 128 TMEM columns
+            void* tok = nullptr;
+            const bool prof = profile_begin(stream, &tok);
+            chm::match_subitems_kernel<<<grid, chm::kThreads, smem, stream>>>(table, subs, offsets + nItems,
+                                                                               schemeOffset, device_error_word());
+            if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
+            if (prof) profile_end(stream, tok);
+            launch_count_add(2);
+        }
+    }
+    if (subs) cudaFreeAsync(subs, stream);
+    if (offsets) cudaFreeAsync(offsets, stream);
     const cudaError_t e = cudaFreeAsync(scratch, stream);
     if (st == RSFM_OK && e != cudaSuccess) st = RSFM_ERR_CUDA;
     return st;
