@@ -336,8 +336,12 @@ def find_best_match_pairs(pairs, per_scheme_lists=True, stream=None):
     def ci(img):
         return _lib.CasHashImage(img.desc.data_ptr(), img.upper.data_ptr(), img.buckets.data_ptr(), img.sqr.data_ptr())
 
-    outs = [(torch.empty(q.n, dtype=torch.int64, device=q.desc.device),
-             torch.empty(t.n, dtype=torch.int64, device=q.desc.device)) for q, t in pairs]
+    # one allocation for every pair's results (the call synchronizes the stream once, so host work
+    # per pair would show up as device idle time)
+    sizes = [n for q, t in pairs for n in (q.n, t.n)]
+    flat = torch.empty(sum(sizes), dtype=torch.int64, device=pairs[0][0].desc.device) if pairs else None
+    views = torch.split(flat, sizes) if pairs else ()
+    outs = list(zip(views[0::2], views[1::2]))
     arr = (_lib.CasHashPair * len(pairs))(*[
         _lib.CasHashPair(ci(q), ci(t), q.n, t.n, _lib.CasHashResult(a.data_ptr(), b.data_ptr()))
         for (q, t), (a, b) in zip(pairs, outs)])
