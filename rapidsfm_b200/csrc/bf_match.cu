@@ -14,14 +14,17 @@
 // Work decomposition. A "unit" is a block of up to kMaxRowTiles*128 A rows times a range of up to
 // kMaxColBlocks 128-column B blocks. Persistent CTAs take units round-robin. Per CTA:
 //   warp 0      TMA producer: A row tiles (resident for the unit), B column blocks (ring)
-//   warp 1      TMEM allocator and UMMA issuer (one thread): per (B block, A row tile) one
-//               128x128x128 int8 product into one of four TMEM accumulators
-//   warps 2..   epilogue, 2 or 4 warpgroups; warpgroup w owns 128/G columns of every tile
-// Each epilogue thread owns one TMEM lane (one A row of the tile). It keeps, in registers, a
-// column accumulator holding for each of its columns the best packed column key over the unit's
-// row tiles, so the cross-lane column reduction runs once per B block instead of once per tile.
-// Row maxima are thread-local; the exact row second-best needs per-chunk work only for chunks
-// that can still become the row's best. Row state lives in shared memory per (warpgroup, row).
+//   warp 1      TMEM allocator and UMMA issuer (one thread): per (B block, A row tile) two
+//               128x128x128 int8 products into one of two TMEM accumulator pairs: the tile
+//               (lane = A row, column = B column) and its transpose (lane = B column, column =
+//               A row), from the same shared-memory operands with their roles swapped
+//   warps 2..   epilogue, 2 or 4 warpgroups; warpgroup w owns 128/G columns of every tile and,
+//               in the transpose, the same number of rows
+// Both reductions are thread-local: from the tile an epilogue thread reads one A row (its row
+// minimum), from the transpose one B column over the warpgroup's row slice (its column minimum,
+// kept in a register across the unit's row tiles and published with one global atomic per B
+// block). The exact row second-best needs per-chunk work only for chunks that can still become
+// the row's best. Row state lives in shared memory per (warpgroup, row).
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
@@ -40,7 +43,8 @@ constexpr int kTileBytes = 128 * 128;  // 128 descriptors x 128 bytes
 constexpr int kUnitRows = kMaxRowTiles * 128;
 constexpr int kMaxColBlocks = 8;       // B blocks per unit
 constexpr int kUnitCols = kMaxColBlocks * 128;
-constexpr int kAccBufs = 4;            // TMEM accumulators of 128 columns (all 512 columns)
+constexpr int kAccBufs = 2;            // TMEM accumulator pairs (all 512 columns)
+constexpr uint32_t kAccCols = 256;     // per pair: the 128 x 128 tile and its transpose
 // Epilogue warpgroups kWG in {2, 4}: warpgroup w owns 128/kWG columns of every tile, i.e.
 // kCPW = 4/kWG chunks of 32 columns per warp. Four warpgroups leave room for two B stages.
 template <int kWG>
@@ -119,7 +123,6 @@ struct Smem {
     uint8_t a[kMaxRowTiles][kTileBytes];
     uint8_t b[Cfg<kWG>::kBStages][kTileBytes];
     int32_t nbk[kUnitCols];              // per unit column: row-key addend (31 - j % 32) - |b|^2 * 256
-    int32_t colkey[2][4][128];           // [block parity][lane quarter][column]: quarter maxima
     // Row state of the current unit, per unit row r = 128 p + 32 q + lane:
     int32_t rowc[kUnitRows];             // column-key addend ((7-p) << 5 | (31-lane)) - |a|^2 * 256
     // Per warpgroup: tk = trigger threshold in row-key space (set from the global best at unit
@@ -137,22 +140,6 @@ struct Smem {
 
 __device__ __forceinline__ void named_bar(uint32_t id, uint32_t n) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-
-// Cross-lane maximum of 32 per-lane columns: afterwards v[0] of lane l holds the maximum over
-// the 32 lanes of column l. Five butterfly levels; at each, a lane keeps the half of its
-// remaining columns selected by its lane bit and takes the maximum with its partner's copy.
-__device__ __forceinline__ void column_max_butterfly(int32_t (&v)[32], uint32_t lane) {
-#pragma unroll
-    for (int s = 16; s >= 1; s >>= 1) {
-        const bool up = (lane & uint32_t(s)) != 0u;
-#pragma unroll
-        for (int i = 0; i < s; ++i) {
-            const int32_t lo = v[i], hi = v[i + s];
-            const int32_t r = __shfl_xor_sync(0xffffffffu, up ? lo : hi, s);
-            v[i] = max(up ? hi : lo, r);
-        }
-    }
 }
 
 template <int kWG>
@@ -248,9 +235,12 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                         // K step k = +32 bytes = +2 in the descriptor's start-address field (the
                         // tiles sit below 256 KB, so the 14-bit field cannot carry).
                         const uint64_t aDesc = aDesc0 + uint64_t(p) * (kTileBytes >> 4);
-                        const uint32_t d = tmem + buf * 128u;
+                        // tile (rows x columns) and its transpose (columns x rows), side by side
+                        const uint32_t d = tmem + buf * kAccCols;
 #pragma unroll
                         for (uint32_t k = 0; k < 4; ++k) umma_i8(d, aDesc + 2u * k, bDesc + 2u * k, idesc, k);
+#pragma unroll
+                        for (uint32_t k = 0; k < 4; ++k) umma_i8(d + 128u, bDesc + 2u * k, aDesc + 2u * k, idesc, k);
                         umma_commit(&S.accFull[buf]);
                         if (b + 1 == U.cb) umma_commit(&S.aEmpty[p]);
                         ++acc;
@@ -265,14 +255,15 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        // Keys are kept in "max is better" form. For thread (q, lane) and row tile p let
-        //   c = (7 - p) << 5 | (31 - lane)                 (8 bits, constant per thread and tile)
+        // Keys are kept in "max is better" form. For row 128 p + 32 m + l of a unit let
+        //   c = (7 - p) << 5 | (31 - l)                    (8 bits)
+        //   rowc = c - |a|^2 * 256                         (staged per unit row)
         //   column key  ck = (2 a.b - |a|^2) * 256 + c     = (dot << 9) + rowc
         //   row key     rk = ck + (31 - k) - |b|^2 * 256   = -d * 256 + c + (31 - k)
-        // (k = column within the 32-column chunk). A column's maximum ck over (p, lane) is its
-        // smallest d, ties going to the smallest row (p first, then lane): the column flush needs
-        // no repacking. Within one thread and tile c is constant and c + (31 - k) < 287, so row
-        // keys of one chunk order by (d, k); u = rk - c = -d * 256 + (31 - k) decodes both.
+        // (k = column within the 32-column chunk). A column's maximum ck over the rows of one
+        // 32-row slice (fixed m, any p and l) is its smallest d, ties going to the smallest row.
+        // Within one row c is constant and c + (31 - k) < 287, so row keys of one chunk order by
+        // (d, k); u = rk - c = -d * 256 + (31 - k) decodes both.
         //
         // Row state lives in shared memory, per warpgroup and unit row: tk = trigger threshold,
         // l1j = column of the own best, l2k = max over the other keys that can matter for the
@@ -288,7 +279,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
         const uint32_t laneBase = (32u * q) << 16;
         constexpr int kRowIt = kUnitRows / (32 * kEpiWarps);
         constexpr int kColIt = (kUnitCols + 32 * kEpiWarps - 1) / (32 * kEpiWarps);
-        uint32_t acc = 0, blk = 0;
+        uint32_t acc = 0;
         for (uint32_t u = blockIdx.x; u < P.totalUnits; u += gridDim.x) {
             const Unit U = decode_unit(P, u);
             const TaskDev& T = task_of(P, U.task);
@@ -330,13 +321,15 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 if (x < uint32_t(kUnitCols)) S.nbk[x] = int32_t((31u - (x & 31u)) - (nb[it] << 8));
             }
             named_bar(1, 32 * kEpiWarps);
-            for (uint32_t b = 0; b < U.cb; ++b, ++blk) {
-                const uint32_t bpar = blk & 1u;
+            for (uint32_t b = 0; b < U.cb; ++b) {
                 const uint32_t blockBase = U.c0 + 128u * b;
-                const uint32_t jw = blockBase + 32u * kCPW * wg;  // first column of this warp
-                int32_t ca[32 * kCPW];
+                const uint32_t jw = blockBase + 32u * kCPW * wg;  // first column of this warp (row side)
+                // Column side: this thread's column of the block is 32 q + lane; its rows in every
+                // tile are the warpgroup's slice 32 (kCPW wg + cc) + k, k < 32. colBest[cc] is the
+                // best column key over the slice's rows of all the unit's tiles.
+                int32_t colBest[kCPW];
 #pragma unroll
-                for (int k = 0; k < 32 * kCPW; ++k) ca[k] = INT32_MIN;
+                for (int cc = 0; cc < kCPW; ++cc) colBest[cc] = INT32_MIN;
 #pragma unroll 1
                 for (uint32_t p = 0; p < U.pt; ++p) {
                     const uint32_t r = 128u * p + t128;
@@ -347,16 +340,38 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                     const uint32_t buf = acc % kAccBufs;
                     mbar_wait(&S.accFull[buf], (acc / kAccBufs) & 1u, err, kDevTimeoutAccFull);
                     tc_fence_after();
-                    uint32_t x[32 * kCPW];
+                    uint32_t x[32 * kCPW], y[32 * kCPW];
 #pragma unroll
-                    for (int cc = 0; cc < kCPW; ++cc)
-                        tmem_ld32(tmem + laneBase + buf * 128u + 32u * (kCPW * wg + cc),
-                                  *reinterpret_cast<uint32_t(*)[32]>(&x[32 * cc]));
+                    for (int cc = 0; cc < kCPW; ++cc) {
+                        const uint32_t col = buf * kAccCols + 32u * (kCPW * wg + cc);
+                        tmem_ld32(tmem + laneBase + col, *reinterpret_cast<uint32_t(*)[32]>(&x[32 * cc]));
+                        tmem_ld32(tmem + laneBase + col + 128u, *reinterpret_cast<uint32_t(*)[32]>(&y[32 * cc]));
+                    }
                     tmem_wait_ld();
-                    // The accumulator is in registers now: hand the TMEM buffer back to the MMA.
+                    // The accumulators are in registers now: hand the TMEM buffer back to the MMA.
                     tc_fence_before();  // (tcgen05.ld and its wait are warp-collective: the warp is converged)
                     if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
                     ++acc;
+                    // ---- column side: ck = (dot << 9) + rowc of the row (ties -> smallest row)
+#pragma unroll
+                    for (int cc = 0; cc < kCPW; ++cc) {
+                        int32_t m[4] = {INT32_MIN, INT32_MIN, INT32_MIN, INT32_MIN};
+                        const int4* rc4 = reinterpret_cast<const int4*>(&S.rowc[128u * p + 32u * (kCPW * wg + cc)]);
+#pragma unroll
+                        for (int k8 = 0; k8 < 4; ++k8) {
+                            const int4 va = rc4[2 * k8], vb = rc4[2 * k8 + 1];
+                            const int32_t rcv[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+                            int32_t ck[8];
+#pragma unroll
+                            for (int e8 = 0; e8 < 8; ++e8)
+                                ck[e8] = int32_t((y[32 * cc + 8 * k8 + e8] << 9) + uint32_t(rcv[e8]));
+#pragma unroll
+                            for (int e4 = 0; e4 < 4; ++e4) m[e4] = __vimax3_s32(m[e4], ck[e4], ck[e4 + 4]);
+                        }
+                        colBest[cc] = max(colBest[cc], max(max(m[0], m[1]), max(m[2], m[3])));
+                    }
+                    // ---- row side: row keys without the row constant, rk' = (dot << 9) + nbk;
+                    // the row key of the thresholds is rk' + rowc.
 #pragma unroll
                     for (int cc = 0; cc < kCPW; ++cc) {
                         const uint32_t j0 = jw + 32u * cc;
@@ -371,31 +386,34 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                             for (int e8 = 0; e8 < 8; ++e8) {
                                 const int k = 32 * cc + 8 * k8 + e8;
                                 // Modular 32-bit arithmetic: the true keys always fit in int32.
-                                const int32_t ck = int32_t((x[k] << 9) + uint32_t(rowcP));
-                                ca[k] = max(ca[k], ck);
-                                rk[e8] = int32_t(uint32_t(ck) + uint32_t(nbv[e8]));
+                                rk[e8] = int32_t((x[k] << 9) + uint32_t(nbv[e8]));
                                 x[k] = uint32_t(rk[e8]);
                             }
 #pragma unroll
                             for (int e4 = 0; e4 < 4; ++e4) m[e4] = __vimax3_s32(m[e4], rk[e4], rk[e4 + 4]);
                         }
-                        int32_t rmax = max(max(m[0], m[1]), max(m[2], m[3]));
+                        // Chunk keys x[] and their maximum R live in a space offset by `off` from
+                        // the row-key space (off = rowc; 0 after the ragged-edge conversion).
+                        int32_t R = max(max(m[0], m[1]), max(m[2], m[3]));
+                        int32_t off = rowcP;
                         // Columns past nbDescB only occur in a task's last block: drop them there.
                         if (j0 + 32u > T.nB) {
-                            rmax = INT32_MIN;
+                            R = INT32_MIN;
+                            off = 0;
 #pragma unroll
                             for (int k = 0; k < 32; ++k) {
-                                if (j0 + k >= T.nB) x[32 * cc + k] = uint32_t(INT32_MIN);
-                                rmax = max(rmax, int32_t(x[32 * cc + k]));
+                                x[32 * cc + k] = (j0 + k >= T.nB) ? uint32_t(INT32_MIN) : x[32 * cc + k] + uint32_t(rowcP);
+                                R = max(R, int32_t(x[32 * cc + k]));
                             }
                         }
+                        const int32_t rmax = int32_t(uint32_t(R) + uint32_t(off));
                         if (__any_sync(0xffffffffu, rmax >= tkP)) {
                             // Second key of the chunk: keys within a chunk are distinct, so
-                            // min over k of (rmax - 1 - key) (unsigned) skips exactly the maximum.
+                            // min over k of (R - 1 - key) (unsigned) skips exactly the maximum.
                             uint32_t mn = 0xFFFFFFFFu;
 #pragma unroll
-                            for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(rmax) - 1u - x[32 * cc + k]);
-                            const int32_t s2 = int32_t(uint32_t(rmax) - 1u - mn);
+                            for (int k = 0; k < 32; ++k) mn = min(mn, uint32_t(R) - 1u - x[32 * cc + k]);
+                            const int32_t s2 = int32_t(uint32_t(R) - 1u - mn + uint32_t(off));
                             if (rmax >= tkP) {
                                 const uint32_t c = uint32_t(rowcP) & 255u;
                                 // the previous own best (key of distance d1: tk - 256) becomes a second
@@ -413,38 +431,22 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                     }
                     S.l2k[wg][r] = l2kP;
                 }
-                // ---- column flush: best key per column over this warp's 32 lanes (butterfly),
-                // then over the four lane quarters: their keys go to shared memory and one thread
-                // per column merges them in row order, then one global atomic per column.
+                // ---- column publish: one global atomic per (column, row slice); no cross-warp
+                // step. Key = (|b|^2 - d) * 256 + code, code = (7 - p) << 5 | (31 - k).
+                const uint32_t jb = 32u * q + lane;  // column within the block
+                const uint32_t j = blockBase + jb;
+                if (j < T.nB) {
+                    const uint32_t xj = j - U.c0;  // |b_j|^2 from the staged row-key addend
+                    const uint32_t nbj = ((31u - (xj & 31u)) - uint32_t(S.nbk[xj])) >> 8;
 #pragma unroll
-                for (int cc = 0; cc < kCPW; ++cc) {
-                    int32_t v[32];
-#pragma unroll
-                    for (int k = 0; k < 32; ++k) v[k] = ca[32 * cc + k];
-                    column_max_butterfly(v, lane);
-                    S.colkey[bpar][q][jw - blockBase + 32 * cc + lane] = v[0];
-                }
-                named_bar(2 + wg, 128);
-                if (t128 < 32 * kCPW) {
-                    const uint32_t cc = jw - blockBase + t128;
-                    // Quarter keys order (|b|^2 - d, p, lane) within a quarter; across quarters the
-                    // row 128 p + 32 q + lane decides ties, so compare (value, -row) explicitly.
-                    long long best = LLONG_MIN;
-#pragma unroll
-                    for (uint32_t qq = 0; qq < 4; ++qq) {
-                        const int32_t k = S.colkey[bpar][qq][cc];
-                        const uint32_t rr = 128u * (7u - ((uint32_t(k) >> 5) & 7u)) + 32u * qq + (31u - (uint32_t(k) & 31u));
-                        best = max(best, static_cast<long long>(k >> 8) * 1024 + (1023 - rr));
-                    }
-                    const int32_t val = int32_t(best >> 10);  // (2 a.b - |a|^2) = |b|^2 - d
-                    const uint32_t rr = 1023u - uint32_t(best & 1023);
-                    const uint32_t j = blockBase + cc;
-                    const uint32_t i = U.r0 + rr;
-                    if (j < T.nB && i < T.nA) {
-                        const uint32_t xj = j - U.c0;  // |b_j|^2 from the staged row-key addend
-                        const uint32_t nbj = ((31u - (xj & 31u)) - uint32_t(S.nbk[xj])) >> 8;
-                        const uint32_t d = nbj - uint32_t(val);
-                        atomicMin(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
+                    for (int cc = 0; cc < kCPW; ++cc) {
+                        const uint32_t code = uint32_t(colBest[cc]) & 255u;
+                        const uint32_t rr = 128u * (7u - (code >> 5)) + 32u * (kCPW * wg + cc) + (31u - (code & 31u));
+                        const uint32_t i = U.r0 + rr;
+                        if (i < T.nA) {
+                            const uint32_t d = nbj - uint32_t(colBest[cc] >> 8);
+                            atomicMin(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
+                        }
                     }
                 }
             }
@@ -555,7 +557,7 @@ __global__ void sqr_norm_kernel(uint32_t* __restrict__ out, const uint4* __restr
 template <int kWG>
 static size_t smem_bytes() { return sizeof(Smem<kWG>) + 1024; }
 
-// Unit shape: as many A rows per unit as possible (fewer column flushes), then columns, keeping
+// Unit shape: as many A rows per unit as possible (fewer column atomics), then columns, keeping
 // at least ~2 units per SM when the problem allows.
 static void choose_shape(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, int nsm, uint32_t& rowTiles,
                          uint32_t& colBlocks) {
