@@ -329,8 +329,10 @@ class CascadeMatcher:
 
 
 def find_best_match_pairs(pairs, per_scheme_lists=True, stream=None):
-    """findBestMatch over many independent (query, train) RankedImage pairs in one launch
-    (rsfm_cashash_find_best_match_pairs); returns per pair (best int64 [nq], best int64 [nt])."""
+    """findBestMatch over many independent (query, train) RankedImage pairs in one call
+    (rsfm_cashash_find_best_match_pairs: one matching launch over 32 x 32 bucket sub-items of all
+    pairs; the call synchronizes `stream` once, to size the sub-item list). Returns per pair
+    (best int64 [nq], best int64 [nt]), views of one shared allocation."""
     lib = _lib.load()
 
     def ci(img):

@@ -112,3 +112,31 @@ def test_batch_with_empty_train_image(rsfm):
     torch.cuda.synchronize()
     assert torch.equal(b1, eb) and torch.equal(c1, ec)
     batch.close()
+
+
+@pytest.mark.parametrize("per_scheme", [True, False])
+def test_find_best_match_pairs_api(rsfm, per_scheme):
+    """cashash.find_best_match_pairs (all pairs in one call, results in one shared allocation)
+    gives each pair the results of its own find_best_match call, empty images included."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(12))
+    q, t, _ = synth.make_pair(1500, 1200, 0.5, 8.0, seed=121)
+    r, s, _ = synth.make_pair(90, 2500, 0.4, 8.0, seed=122)
+    dq, dt, dr, ds = _dev(q), _dev(t), _dev(r), _dev(s)
+    cas.fit(dq)
+    empty = torch.empty((0, 128), dtype=torch.uint8, device="cuda")
+    imgs = ch.register_ranked_images(cas, [dq, dt, dr, ds, empty])
+    pairs = [(imgs[0], imgs[1]), (imgs[2], imgs[3]), (imgs[4], imgs[1]), (imgs[0], imgs[4]), (imgs[3], imgs[0])]
+    got = ch.find_best_match_pairs(pairs, per_scheme_lists=per_scheme)
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    assert len(got) == len(pairs)
+    for (qi, ti), (bq, bt) in zip(pairs, got):
+        assert bq.numel() == qi.n and bt.numel() == ti.n
+        if qi.n == 0 or ti.n == 0:
+            assert bool((bq == -1).all()) and bool((bt == -1).all())
+            continue
+        (eq, et), = ch.find_best_match([qi], ti, per_scheme_lists=per_scheme)
+        torch.cuda.synchronize()
+        assert torch.equal(bq, eq) and torch.equal(bt, et)
+    assert ch.find_best_match_pairs([]) == []
