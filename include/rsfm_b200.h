@@ -401,6 +401,66 @@ int rsfm_ranked_register_flat(const rsfm_ranked_hasher* hasher, const void* desc
                               uint32_t* bucketEnds, uint32_t* maxBucketSize, uint32_t* buckets, uint32_t* records,
                               cudaStream_t stream);
 
+/* ---------------------------------------------------------------- image registration
+ * The per-image precompute of BruteForceMatcher::registerImage (bruteForceMatcher.cpp:163-203):
+ * one device blob per image, its sections in this order, each padded to a multiple of 128 bytes
+ * (bruteForceMatcher.cpp:56-63):
+ *   [4-bit descriptors, 64 B each     (useFourBit)]
+ *   [squared norms, uint32 x nbDesc   (useSqrNorm)]
+ *   [cascade-hash bucketEnds, uint32 8 x 256 (useCasHash)]
+ *   [cascade-hash bucket lists, uint32 8 x nbDesc (useCasHash)]
+ * Flags as the reference's constructor allows them (bruteForceMatcher.cpp:113-121): useFourBit and
+ * useCasHash each need useSqrNorm, and useCasHash excludes useFourBit. */
+
+/* Byte offsets of the sections in a blob; RSFM_PRECOMP_ABSENT for a section the flags leave out. */
+#define RSFM_PRECOMP_ABSENT ((size_t)-1)
+typedef struct rsfm_precomp_sections {
+    size_t desc4b;
+    size_t sqrNorm;
+    size_t bucketEnds;
+    size_t buckets;
+    size_t total; /* = rsfm_precomp_nb_bytes */
+} rsfm_precomp_sections;
+
+/* Replaces getPreCompNbBytes (bruteForceMatcher.cpp:56-63). */
+size_t rsfm_precomp_nb_bytes(uint32_t nbDesc, int useSqrNorm, int useFourBit, int useCasHash);
+/* The section offsets matchImpl derives from a blob (bruteForceMatcher.cpp:247-263, 296-308). */
+int rsfm_precomp_sections_of(uint32_t nbDesc, int useSqrNorm, int useFourBit, int useCasHash,
+                             rsfm_precomp_sections* out);
+/* Replaces getPreCompDeviceScratchNbBytes and getPreCompPinnedScratchNbBytes
+ * (bruteForceMatcher.cpp:41-55). */
+size_t rsfm_precomp_device_scratch_nb_bytes(uint32_t nbDesc, int useCasHash);
+size_t rsfm_precomp_pinned_scratch_nb_bytes(int useCasHash);
+
+/* Called from a host function on the registration stream with the image's largest cascade-hash
+ * bucket (the reference's maxBucketSizeHandler). Must not call CUDA. */
+typedef void (*rsfm_max_bucket_size_handler)(uint32_t maxBucketSize, void* user);
+
+/* Replaces preCompForMatch (bruteForceMatcher.cpp:64-107). dst: a blob of rsfm_precomp_nb_bytes
+ * bytes, 16-byte aligned; desc: nbDesc 8-bit SIFT descriptors. Sections are written as the
+ * reference writes them, including its choice for useFourBit: the norm section then holds the
+ * norms of the 8-bit descriptors (bruteForceMatcher.cpp:76-78), not of the 4-bit ones
+ * (rsfm_precomp_sift4b_sqr_norm computes those).
+ * Cascade hash (all device memory except accNbDesc and pinnedScratch): acc (128 x uint64) and
+ * *accNbDesc (host) accumulate the descriptors of every image registered so far and the bias is
+ * computed from them, so keys depend on the registration order as in the reference; weights are
+ * 64 x 128 int8 rows (KArray<int32_t, 64, 32>), biasBase 64 int32; deviceScratch has
+ * rsfm_precomp_device_scratch_nb_bytes bytes and pinnedScratch (page-locked host memory)
+ * rsfm_precomp_pinned_scratch_nb_bytes; both are reused by the next call on the same stream.
+ * The image's largest bucket lands in pinnedScratch (as uint32) once the stream reaches it, and
+ * `handler` (optional) is called with it then. Bucket lists are in ascending descriptor order.
+ * Asynchronous on `stream`; the bucket build takes stream-ordered scratch from the library's pool
+ * (as rsfm_cashash_build_buckets). */
+int rsfm_precomp_for_match(void* dst, const void* desc, uint32_t nbDesc, int useSqrNorm, int useFourBit,
+                           int useCasHash, uint64_t* accNbDesc, unsigned long long* acc, const void* casHashWeights,
+                           const int32_t* casHashBiasBase, void* pinnedScratch, void* deviceScratch,
+                           rsfm_max_bucket_size_handler handler, void* user, cudaStream_t stream);
+
+/* The reference matcher's cascade-hash projection (bruteForceMatcher.cpp:120-145): 64 x 128 int8
+ * weights and 64 int32 bias bases from std::default_random_engine{11} and std::normal_distribution
+ * (libstdc++), into host arrays; copy them to the device for rsfm_precomp_for_match. */
+int rsfm_cashash_reference_weights(int8_t* weightsHost, int32_t* biasBaseHost);
+
 /* Triplet trainer for the learned hash. Parameters are one f32 block w1 | b1 | w2 | b2
  * (32768 + 256 + 32768 + 128 floats); the trainer keeps fp32 masters, Adam moments (beta 0.9 /
  * 0.999, eps 1e-8) and the bf16 copies the hash reads. Loss per triplet (anchor, positive,

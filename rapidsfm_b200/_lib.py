@@ -76,6 +76,15 @@ class RankedHasher(ctypes.Structure):
                 ("mlp", ctypes.c_void_p)]
 
 
+class PrecompSections(ctypes.Structure):
+    """rsfm_precomp_sections: byte offsets of a registration blob's sections."""
+    _fields_ = [("desc4b", ctypes.c_size_t), ("sqrNorm", ctypes.c_size_t), ("bucketEnds", ctypes.c_size_t),
+                ("buckets", ctypes.c_size_t), ("total", ctypes.c_size_t)]
+
+
+MAX_BUCKET_SIZE_HANDLER = ctypes.CFUNCTYPE(None, ctypes.c_uint32, ctypes.c_void_p)
+
+
 class RankedImageJob(ctypes.Structure):
     """rsfm_ranked_image_job: one image of rsfm_ranked_register_images."""
     _fields_ = [("desc", ctypes.c_void_p), ("nbDesc", ctypes.c_uint32), ("keys", ctypes.c_void_p),
@@ -171,6 +180,17 @@ SIGNATURES = {
                                                  ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_precomp_nb_bytes": (ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rsfm_precomp_sections_of": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(PrecompSections)]),
+    "rsfm_precomp_device_scratch_nb_bytes": (ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int]),
+    "rsfm_precomp_pinned_scratch_nb_bytes": (ctypes.c_size_t, [ctypes.c_int]),
+    "rsfm_precomp_for_match": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, MAX_BUCKET_SIZE_HANDLER, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
+    "rsfm_cashash_reference_weights": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_pairs": (ctypes.c_int, [ctypes.POINTER(CasHashPair), ctypes.c_uint32,
                                                           ctypes.c_uint32, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,

@@ -21,6 +21,7 @@ SOURCES = [
     "filters.cu",
     "ransac.cu",
     "ranked_register.cpp",
+    "precomp.cpp",
     "bf_autotune.cpp",
     "host_filters.cpp",
     "diag.cu",

@@ -287,15 +287,21 @@ def last_launch_count():
 
 
 class BruteForceMatcher:
-    """Mirror of rsfm::BruteForceMatcher (bruteForceMatcher.h:28-102), brute-force method.
+    """Mirror of rsfm::BruteForceMatcher (bruteForceMatcher.h:28-102).
 
-    register_image() precomputes and keeps per-image squared norms (the reference's precompute
-    blob, bruteForceMatcher.cpp:63-107); match() returns per query image the (fwd, bwd) BestMatch
-    arrays; match_and_filter() applies crossCheckMatches or removeMatchConflicts on the host
-    (bruteForceMatcher.cpp:426-442).
+    method "brute_force": register_image() precomputes and keeps per-image squared norms (4-bit
+    descriptors and their norms with use_sift4b); match() returns per query image the (fwd, bwd)
+    BestMatch arrays of the exact matcher.
+    method "cascade_hash" (Config::Matcher::kCascadeHash): register_image() writes the reference's
+    registration blob (squared norms, bucket ends, bucket lists; precomp.Registrar over
+    rsfm_precomp_for_match, the reference's projection by default, the bias from the descriptors
+    of every image registered so far) and match() runs cashash::findBestMatch on the blobs'
+    sections as matchImpl does (bruteForceMatcher.cpp:283-325).
+    match_and_filter() applies crossCheckMatches or removeMatchConflicts (bruteForceMatcher.cpp:426-442).
     """
 
-    def __init__(self, device="cuda", use_sift4b=False, use_sqr_norm_precomp=True):
+    def __init__(self, device="cuda", use_sift4b=False, use_sqr_norm_precomp=True, method="brute_force",
+                 cas_hash_weights=None, cas_hash_bias_base=None):
         self.device = torch.device(device)
         self._images = {}
         self.stream = torch.cuda.Stream(device=self.device)
@@ -303,9 +309,25 @@ class BruteForceMatcher:
         # dp4a matcher (IDP) runs.
         self.use_sift4b = use_sift4b
         self.use_sqr_norm_precomp = use_sqr_norm_precomp or use_sift4b
+        if method not in ("brute_force", "cascade_hash"):
+            raise ValueError(f"unknown matcher method {method!r}")
+        self.method = method
+        self._registrar = None
+        if method == "cascade_hash":
+            if use_sift4b:  # bruteForceMatcher.cpp:117-121: 4-bit is not implemented for cascade hash
+                raise ValueError("cascade_hash does not support use_sift4b")
+            from .precomp import Registrar
+            self.use_sqr_norm_precomp = True
+            self._registrar = Registrar(use_sqr_norm=True, use_cas_hash=True, weights=cas_hash_weights,
+                                        bias_base=cas_hash_bias_base, device=self.device)
 
     def register_image(self, handle, desc):
         _check_desc(desc)
+        if self._registrar is not None:
+            with torch.cuda.stream(self.stream):
+                blob = self._registrar.register(handle, desc, stream=self.stream)
+            self._images[handle] = (desc, blob)
+            return
         with torch.cuda.stream(self.stream):
             if self.use_sift4b:
                 d4 = sift_desc_8b_to_4b(desc, stream=self.stream)
@@ -321,9 +343,39 @@ class BruteForceMatcher:
         return [BFTask(self._images[q][0], dt, self._images[q][1], st, bits=bits,
                        norms=self.use_sqr_norm_precomp) for q in queries]
 
+    def _match_cascade(self, queries, train):
+        """Both directions' BestMatch tensors (int64, packed) per query image."""
+        lib = _lib.load()
+        # the largest buckets of the registrations (the reference waits on a condition variable)
+        self.stream.synchronize()
+
+        def image(handle):
+            desc, blob = self._images[handle]
+            v = self._registrar.views(blob, desc.shape[0])
+            return _lib.CasHashImage(desc.data_ptr(), v["bucket_ends"].data_ptr(), v["buckets"].data_ptr(),
+                                     v["sqr_norm"].data_ptr()), int(desc.shape[0])
+
+        n = len(queries)
+        qs = [image(h) for h in queries]
+        ti, nt = image(train)
+        outs = [(torch.empty(max(nq, 1), dtype=torch.int64, device=self.device),
+                 torch.empty(max(nt, 1), dtype=torch.int64, device=self.device)) for _, nq in qs]
+        qi = (_lib.CasHashImage * n)(*[c for c, _ in qs])
+        rr = (_lib.CasHashResult * n)(*[_lib.CasHashResult(a.data_ptr(), b.data_ptr()) for a, b in outs])
+        sizes = (ctypes.c_uint32 * n)(*[nq for _, nq in qs])
+        mq = (ctypes.c_uint32 * n)(*[self._registrar.max_bucket_size(h) for h in queries])
+        _lib.check(lib.rsfm_cashash_find_best_match(qi, sizes, ctypes.byref(ti), nt, rr, n, mq,
+                                                    self._registrar.max_bucket_size(train), _stream_ptr(self.stream)),
+                   "rsfm_cashash_find_best_match")
+        return [(a[:nq], b[:nt]) for (a, b), (_, nq) in zip(outs, qs)]
+
     def match(self, queries, train):
         if not queries:
             return []
+        if self._registrar is not None:
+            res = self._match_cascade(queries, train)
+            self.stream.synchronize()
+            return [(np.stack(unpack_best(a), 1), np.stack(unpack_best(b), 1)) for a, b in res]
         run = bf_match_4b if self.use_sift4b else bf_match if self.use_sqr_norm_precomp else bf_match_idp
         with torch.cuda.stream(self.stream):
             tasks = run(self._tasks(queries, train), stream=self.stream)
@@ -340,6 +392,13 @@ class BruteForceMatcher:
             return res
         if not queries:
             return []
+        if self._registrar is not None:
+            res = self._match_cascade(queries, train)
+            with torch.cuda.stream(self.stream):
+                filtered = [filter_matches_device(a, b, nb_train=b.shape[0], cross_check=cross_check,
+                                                  stream=self.stream) for a, b in res]
+            self.stream.synchronize()
+            return [valid_matches_to_host(out, count) for out, count in filtered]
         run = bf_match_4b if self.use_sift4b else bf_match if self.use_sqr_norm_precomp else bf_match_idp
         with torch.cuda.stream(self.stream):
             tasks = run(self._tasks(queries, train), stream=self.stream)
