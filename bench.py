@@ -615,6 +615,26 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
             out["find_best_match_8_schemes"] = {"ms": ms, "recall": int(hit) / max(1, int(tot)),
                                                 "desc_pairs_per_s": pairs / (ms * 1e-3),
                                                 "one_call_per_pair_ms": ms_calls}
+    # registration blobs (the reference's preCompForMatch layout, cascade-hash flags: norms, bias
+    # from the running accumulator, keys with fused histogram, bounds, bucket lists), image by image
+    from rapidsfm_b200 import precomp
+    reg = precomp.Registrar(use_sqr_norm=True, use_cas_hash=True, device=dev)
+    sample = [x for pair in imgs[:100] for x in pair]
+    for k, d in enumerate(sample[:4]):
+        reg.register(("warm-up", k), d, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for k, d in enumerate(sample):
+        reg.register(k, d, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    out["registration_blob"] = {"images": len(sample), "descriptors_per_image": n,
+                                "ms_per_image": ms / len(sample), "wall_ms_per_image": 1e3 * wall / len(sample),
+                                "desc_per_s": len(sample) * n / (ms * 1e-3)}
     if "learned" in out:
         p6 = out["plain"]["tables"]["6"]
         ok = [v for v in out["learned"]["tables"].values() if v["recall"] >= p6["recall"]]

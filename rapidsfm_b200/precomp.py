@@ -7,6 +7,7 @@ lists (use_cas_hash). `Registrar` keeps what the reference matcher keeps across 
 the descriptor accumulator and count that the cascade-hash bias is computed from, the projection
 (the reference's own by default), the scratch buffers and each image's largest bucket.
 """
+import contextlib
 import ctypes
 
 import numpy as np
@@ -65,13 +66,15 @@ class Registrar:
         sq, fb, ch = self.flags
         n = int(desc.shape[0])
         lib = _lib.load()
-        blob = torch.empty(max(nb_bytes(n, sq, fb, ch), 16), dtype=torch.uint8, device=self.device)
+        # allocations belong to the stream the work is enqueued on
+        with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+            blob = torch.empty(max(nb_bytes(n, sq, fb, ch), 16), dtype=torch.uint8, device=self.device)
+            need = int(lib.rsfm_precomp_device_scratch_nb_bytes(n, 1)) if ch else 0
+            if ch and (self._scratch is None or self._scratch.numel() < need):
+                self._scratch = torch.empty(need, dtype=torch.uint8, device=self.device)
         pinned = None
         scratch_ptr = None
         if ch:
-            need = int(lib.rsfm_precomp_device_scratch_nb_bytes(n, 1))
-            if self._scratch is None or self._scratch.numel() < need:
-                self._scratch = torch.empty(need, dtype=torch.uint8, device=self.device)
             scratch_ptr = self._scratch.data_ptr()
             # one pinned word per image, so no host callback is needed to keep each value
             pinned = torch.zeros(1, dtype=torch.int32).pin_memory()
