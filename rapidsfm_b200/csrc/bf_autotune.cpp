@@ -1,8 +1,8 @@
 // Autotuner for batched brute-force plans (no reference counterpart).
 //
 // A batch of uneven pairs is matched by one persistent launch; how fast depends on the unit
-// shape (row tiles x column blocks per unit: fewer column flushes vs. more units to balance),
-// the epilogue warpgroup count and the order in which CTAs take units. The tuner times a pruned
+// shape (row tiles x column blocks per unit: fewer column publishes and unit boundaries vs. more
+// units to balance), the epilogue warpgroup count and the order in which CTAs take units. The tuner times a pruned
 // grid of candidates on the batch itself and keeps the winner in an optional text cache keyed by
 // a coarse signature of the batch, so later batches of the same kind skip the timing.
 #include "../../include/rsfm_b200.h"

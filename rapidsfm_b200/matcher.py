@@ -291,7 +291,9 @@ class BruteForceMatcher:
 
     method "brute_force": register_image() precomputes and keeps per-image squared norms (4-bit
     descriptors and their norms with use_sift4b); match() returns per query image the (fwd, bwd)
-    BestMatch arrays of the exact matcher.
+    BestMatch arrays of the exact matcher. With use_sift4b the norms are the 4-bit descriptors'
+    own (exact 4-bit L2); the reference's registration blob stores the 8-bit norms there
+    (bruteForceMatcher.cpp:76-78), which precomp.Registrar reproduces for callers of that layout.
     method "cascade_hash" (Config::Matcher::kCascadeHash): register_image() writes the reference's
     registration blob (squared norms, bucket ends, bucket lists; precomp.Registrar over
     rsfm_precomp_for_match, the reference's projection by default, the bias from the descriptors
