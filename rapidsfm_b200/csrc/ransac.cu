@@ -34,7 +34,7 @@ namespace rsc {
 
 constexpr uint32_t kCta = 128;
 constexpr uint32_t kMinInliers = 6;
-constexpr uint32_t kStage = 2048;  // neighbourhood matches staged in shared memory (32 KB)
+constexpr uint32_t kStage = 1024;  // neighbourhood matches staged in shared memory (20 KB; more are read from global memory)
 constexpr int kMaxTasks = 64;
 constexpr uint32_t kMaxDraws = 64;  // random draws per 3-sample
 
