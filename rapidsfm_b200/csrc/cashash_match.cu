@@ -537,9 +537,10 @@ __global__ void __launch_bounds__(kThreads) match_subitems_kernel(const PairDev*
 
 using namespace rsfm_b200;
 
-// Resident CTAs per SM for the persistent item kernels: each holds ~28 KB of shared memory and
-// 64 TMEM columns, so eight fit (512 columns); more CTAs hide more of an item's chain of
-// dependent loads (bucket bounds, member lists, rows).
+// CTAs per SM launched for the persistent item kernels: each holds ~28 KB of shared memory, 72
+// registers per thread and 64 TMEM columns, so seven are resident at once and the eighth starts
+// as one of them exits (measured: no slower than launching seven). More CTAs hide more of an
+// item's chain of dependent loads (bucket bounds, member lists, rows).
 #ifndef RSFM_FBM_CTAS_PER_SM
 #define RSFM_FBM_CTAS_PER_SM 8
 #endif
