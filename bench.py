@@ -146,6 +146,44 @@ def cpu_baseline(q, t, rows, threads, min_seconds=0.0):
     return reps * rows * len(t) / dt, dt
 
 
+def cpu_baseline_scalar(q, t, rows):
+    """The reference test's plain loop (one thread, scalar bytes) on `rows` query rows against
+    the whole train set. Returns (pairs/s, seconds)."""
+    from oracle import oracle as orc
+    sub = np.ascontiguousarray(q[:rows])
+    t0 = time.perf_counter()
+    orc.bf_match_scalar(sub, t)
+    dt = time.perf_counter() - t0
+    return rows * len(t) / dt, dt
+
+
+def check_exact(q, t, best_a, best_b, second_a, flags_a, threads):
+    """True when the matcher's outputs (forward and backward BestMatch, second-best distance, flag
+    word; host tensors) equal the oracle's on the whole pair."""
+    from oracle import oracle as orc
+    global _ORACLE_PAIR
+    if _ORACLE_PAIR is None or _ORACLE_PAIR[0] is not q:
+        efwd, ebwd, esec = orc.bf_match(q, t, threads=threads)
+        _ORACLE_PAIR = (q, efwd, ebwd, esec, orc.match_flags(efwd, esec, ebwd))
+    _, efwd, ebwd, esec, eflg = _ORACLE_PAIR
+    u32 = lambda x: x.numpy().view(np.uint32)
+    return bool(np.array_equal(u32(best_a).reshape(-1, 2), efwd) and np.array_equal(u32(best_b).reshape(-1, 2), ebwd)
+                and np.array_equal(u32(second_a), esec) and np.array_equal(u32(flags_a), eflg))
+
+
+_ORACLE_PAIR = None
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def _cpu_sample(q, t, threads, seconds):
     """Rows per run so one run takes about `seconds` (whole pair when faster), and the timing."""
     rate, _ = cpu_baseline(q, t, 256, threads)
@@ -191,7 +229,7 @@ def run_reference(args):
         "data": "synthetic",
         "config": _config(),
         "cpu_baseline": {"value": value, "unit": "desc-pairs/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "desc-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -351,6 +389,12 @@ def run_ours(args):
     e1.record(s_d2h)
     torch.cuda.synchronize()
     e2e_step = e0.elapsed_time(e1) / args.steps
+    e2e_last = sets[(args.steps - 1) % 2][3]  # host outputs of the last pipelined step
+    # copy bandwidth of this box, each direction alone (same pinned buffers, same sizes)
+    h2d_ms = _events_ms(lambda: (dq.copy_(hq, non_blocking=True), dt_.copy_(ht, non_blocking=True)), 10, stream)
+    d2h_ms = _events_ms(lambda: [outs[k].copy_(v, non_blocking=True) for k, v in
+                                 (("fwd", task.bestA), ("bwd", task.bestB), ("sec", task.secondA),
+                                  ("flg", task.flagsA))], 10, stream)
     if ws > 1:
         e2e_step = max_over_ranks(e2e_step, dev)
         e2e_serial_step = max_over_ranks(e2e_serial_step, dev)
@@ -392,9 +436,15 @@ def run_ours(args):
         "ops_per_launch": nops,
     }
 
-    # ---- CPU baseline: oracle port, all host threads, about 10 s of work on the same pair
+    # ---- CPU baseline: oracle port, all host threads, about 10 s of work on the same pair; the
+    # faithful scalar loop on one core beside it (bounded row sample). The oracle's whole-pair
+    # result also checks the timed pair's device outputs and the end-to-end host outputs.
     threads = os.cpu_count() or 1
     rows, (cpu_val, cpu_dt) = _cpu_sample(q, t, threads, 10.0)
+    scalar_rows = 256 if args.size == 0 else max(8, min(256, N_QUERY))
+    scalar_val, scalar_dt = cpu_baseline_scalar(q, t, scalar_rows)
+    exact = check_exact(q, t, task.bestA.cpu(), task.bestB.cpu(), task.secondA.cpu(), task.flagsA.cpu(), threads)
+    exact_e2e = check_exact(q, t, e2e_last["fwd"], e2e_last["bwd"], e2e_last["sec"], e2e_last["flg"], threads)
 
     extras = {}
     if not args.no_extras and ws == 1:  # single-GPU sections; scaling runs time the pair only
@@ -422,11 +472,22 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step,
                 "mode": "pipelined: 2 buffer sets, H2D / match / D2H on 3 streams, every step copies in and out",
                 "serial_ms_per_step": e2e_serial_step,
-                "serial_value": ws * N_QUERY * N_TRAIN / (e2e_serial_step * 1e-3)},
+                "serial_value": ws * N_QUERY * N_TRAIN / (e2e_serial_step * 1e-3),
+                "h2d_ms": h2d_ms, "h2d_GBps": h2d / (h2d_ms * 1e-3) / 1e9,
+                "d2h_ms": d2h_ms, "d2h_GBps": d2h / (d2h_ms * 1e-3) / 1e9,
+                "device_step_ms": ms_per_step,
+                "bound": max((("host-to-device copy", h2d_ms), ("matching on the device", ms_per_step),
+                              ("device-to-host copy", d2h_ms)), key=lambda x: x[1])[0],
+                "exact": exact_e2e},
+        "exact": exact,
         "gpu_launches": int(launches),
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "desc-pairs/s", "cores": threads, "kind": "port",
-                         "sample": f"{rows} query rows x {N_TRAIN} train of the pair, repeated for {cpu_dt:.1f} s"},
+                         "sample": f"{rows} query rows x {N_TRAIN} train of the pair, repeated for {cpu_dt:.1f} s",
+                         "cpu_model": cpu_model(),
+                         "scalar": {"value": scalar_val, "unit": "desc-pairs/s", "cores": 1,
+                                    "sample": f"{scalar_rows} query rows x {N_TRAIN} train, one thread, "
+                                              f"scalar byte loop ({scalar_dt:.1f} s)"}},
         "clocks": clocks,
         "int8_tops_effective": nops / (ms_per_step * 1e-3) / 1e12,
     }
@@ -550,8 +611,11 @@ def run_batched(dev, stream, seed=2):
 def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
     """Configs 3 and 4: n_pairs pairs of n descriptors (40% overlap, noise 8); ranked cascade
     matching (T tables x 8 bits, 128-bit Hamming ranking, top-10 exact re-rank, ratio 0.8) with
-    random projections vs. the learned hash, all pairs in one launch each. Recall = share of the
-    brute-force matches passing ratio test and cross-check that the hash matcher finds."""
+    random projections vs. the learned hash, all pairs in one launch each. The brute-force
+    matches are the brute-force best matches that pass the ratio test and the cross-check.
+    Recall = share of the brute-force matches that the hash matcher finds; precision = share of
+    the hash matcher's reported matches (its ratio test passes; for findBestMatch, its two
+    directions cross-check) that are brute-force matches."""
     import torch
     import rapidsfm_b200 as R
     from rapidsfm_b200 import cashash as ch
@@ -589,10 +653,18 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
             ms = _events_ms(lambda: batch.launch(stream), 3, stream)
             hit = torch.zeros((), dtype=torch.int64, device=dev)
             tot = torch.zeros((), dtype=torch.int64, device=dev)
-            for (ok, gt), (best, _, _, _) in zip(truth, batch.results):
-                hit += (((best & 0xFFFFFFFF) == gt) & ok).sum()
+            rep = torch.zeros((), dtype=torch.int64, device=dev)
+            tp = torch.zeros((), dtype=torch.int64, device=dev)
+            for (ok, gt), (best, _, flg, _) in zip(truth, batch.results):
+                same = (best & 0xFFFFFFFF) == gt
+                hit += (same & ok).sum()
                 tot += ok.sum()
+                # reported matches: the hash matcher's own ratio test passes
+                r = (flg & 1) == 1
+                rep += r.sum()
+                tp += (r & same & ok).sum()
             rows[str(tables)] = {"match_ms": ms, "recall": int(hit) / max(1, int(tot)),
+                                 "precision": int(tp) / max(1, int(rep)), "reported": int(rep),
                                  "desc_pairs_per_s": pairs / (ms * 1e-3)}
             batch.close()
         ok98 = [int(k) for k, v in rows.items() if v["recall"] >= 0.98]
@@ -609,10 +681,22 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
             res = fbp()
             hit = torch.zeros((), dtype=torch.int64, device=dev)
             tot = torch.zeros((), dtype=torch.int64, device=dev)
-            for (ok, gt), (bq, _) in zip(truth, res):
-                hit += (((bq & 0xFFFFFFFF) == gt) & ok).sum()
+            rep = torch.zeros((), dtype=torch.int64, device=dev)
+            tp = torch.zeros((), dtype=torch.int64, device=dev)
+            for (ok, gt), (bq, bt) in zip(truth, res):
+                jq = bq & 0xFFFFFFFF
+                same = jq == gt
+                hit += (same & ok).sum()
                 tot += ok.sum()
+                # reported matches: cross-checked in the two directions (the reference matcher's
+                # use of findBestMatch results, bruteForceMatch.cpp:23-40)
+                valid = jq < bt.numel()
+                back = (bt[jq.clamp(max=bt.numel() - 1)] & 0xFFFFFFFF) == torch.arange(bq.numel(), device=dev)
+                r = valid & back
+                rep += r.sum()
+                tp += (r & same & ok).sum()
             out["find_best_match_8_schemes"] = {"ms": ms, "recall": int(hit) / max(1, int(tot)),
+                                                "precision": int(tp) / max(1, int(rep)), "reported": int(rep),
                                                 "desc_pairs_per_s": pairs / (ms * 1e-3),
                                                 "one_call_per_pair_ms": ms_calls}
     # registration blobs (the reference's preCompForMatch layout, cascade-hash flags: norms, bias

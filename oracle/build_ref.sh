@@ -6,6 +6,8 @@
 # Test infrastructure only. Output goes to oracle/_ref/ (git-ignored; travels with the tree).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# Location of the RapidSFM source tree: RSFM_REFERENCE_DIR, else where this build machine keeps
+# it read-only. This recipe is the only file that reads the reference sources.
 REF="${RSFM_REFERENCE_DIR:-/root/reference}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/bruteForceMatchIMMA.cu" ]; then

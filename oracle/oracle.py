@@ -33,6 +33,7 @@ def load():
     sig = {
         "orc_sqr_norm": (None, [_P, u32, _P]),
         "orc_bf_match": (None, [_P, u32, _P, u32, _P, _P, _P, ctypes.c_int]),
+        "orc_bf_match_scalar": (None, [_P, u32, _P, u32, _P, _P, _P]),
         "orc_match_flags": (None, [_P, _P, u32, _P, u32, u32, u32, _P]),
         "orc_cross_check": (ctypes.c_size_t, [_P, u32, _P, u32, _P]),
         "orc_remove_match_conflicts": (ctypes.c_size_t, [_P, u32, u32, _P]),
@@ -80,6 +81,17 @@ def bf_match(a, b, threads=0):
     bwd = np.empty((len(b), 2), dtype=np.uint32)
     sec = np.empty(len(a), dtype=np.uint32)
     load().orc_bf_match(_c(a), len(a), _c(b), len(b), _c(fwd), _c(bwd), _c(sec), threads)
+    return fwd, bwd, sec
+
+
+def bf_match_scalar(a, b):
+    """bf_match's results from the single-threaded scalar loop (the faithful CPU baseline)."""
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.uint8)
+    fwd = np.empty((len(a), 2), dtype=np.uint32)
+    bwd = np.empty((len(b), 2), dtype=np.uint32)
+    sec = np.empty(len(a), dtype=np.uint32)
+    load().orc_bf_match_scalar(_c(a), len(a), _c(b), len(b), _c(fwd), _c(bwd), _c(sec))
     return fwd, bwd, sec
 
 

@@ -110,6 +110,38 @@ void orc_bf_match(const uint8_t* A, uint32_t nA, const uint8_t* B, uint32_t nB, 
     }
 }
 
+// The same results from the plain scalar loop of the reference's kernel test
+// (test/bruteForceMatchKernelTest.cpp:140-164: for each query, for each train descriptor, the
+// exact squared L2 over 128 bytes, one running minimum): one thread, no vector instructions,
+// byte by byte. It is the faithful single-core CPU baseline beside the vectorised OpenMP one.
+__attribute__((optimize("no-tree-vectorize", "no-tree-slp-vectorize"))) void orc_bf_match_scalar(
+    const uint8_t* A, uint32_t nA, const uint8_t* B, uint32_t nB, OrcBestMatch* fwd, OrcBestMatch* bwd,
+    uint32_t* second) {
+    for (uint32_t j = 0; j < nB; j++) bwd[j] = OrcBestMatch{~0u, ~0u};
+    for (uint32_t i = 0; i < nA; i++) {
+        const uint8_t* a = A + size_t(i) * 128;
+        uint32_t bestD = ~0u, bestJ = ~0u, secD = ~0u;
+        for (uint32_t j = 0; j < nB; j++) {
+            const uint8_t* b = B + size_t(j) * 128;
+            uint32_t d = 0;
+            for (int k = 0; k < 128; k++) {
+                const int32_t t = int32_t(a[k]) - int32_t(b[k]);
+                d += uint32_t(t * t);
+            }
+            if (d < bestD) {
+                secD = bestD;
+                bestD = d;
+                bestJ = j;
+            } else if (d < secD) {
+                secD = d;
+            }
+            if (d < bwd[j].distance) bwd[j] = OrcBestMatch{i, d};  // rows ascend: ties keep the lowest
+        }
+        fwd[i] = OrcBestMatch{bestJ, bestD};
+        if (second) second[i] = secD;
+    }
+}
+
 // Extended per-query flags: bit0 = ratio test pass, bit1 = cross-check pass.
 void orc_match_flags(const OrcBestMatch* fwd, const uint32_t* second, uint32_t nA, const OrcBestMatch* bwd,
                      uint32_t nB, uint32_t ratioNum, uint32_t ratioDen, uint32_t* flags) {

@@ -25,6 +25,7 @@
 // kept in a register across the unit's row tiles and published with one global atomic per B
 // block). The exact row second-best needs per-chunk work only for chunks that can still become
 // the row's best. Row state lives in shared memory per (warpgroup, row).
+#include "bf_internal.h"
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
@@ -37,7 +38,6 @@ namespace bf {
 
 using namespace sm100;
 
-constexpr int kMaxTasksPerLaunch = 16;
 constexpr int kMaxRowTiles = 8;        // A row tiles per unit (p fits 3 bits of the keys)
 constexpr int kTileBytes = 128 * 128;  // 128 descriptors x 128 bytes
 constexpr int kUnitRows = kMaxRowTiles * 128;
@@ -724,8 +724,6 @@ __global__ void plan_flags_kernel(const TaskDev* __restrict__ tasks, uint32_t ra
     }
 }
 
-static int validate(const rsfm_sift_bf_task* tasks, size_t n);
-
 }  // namespace bf
 }  // namespace rsfm_b200
 
@@ -758,7 +756,7 @@ static int plan_enqueue(rsfm_bf_plan* pl, cudaStream_t s) {
     return RSFM_OK;
 }
 
-static int validate(const rsfm_sift_bf_task* tasks, size_t n) {
+int validate(const rsfm_sift_bf_task* tasks, size_t n) {
     if (n > 0 && !tasks) return RSFM_ERR_INVALID_ARG;
     for (size_t t = 0; t < n; ++t) {
         const rsfm_sift_bf_task& T = tasks[t];

@@ -16,21 +16,17 @@
 //    call sets the rows it uses to ~0u before the matcher reads them, so nothing carries over
 //    between calls. Calls whose work overlaps on the GPU (different streams, no ordering between
 //    them) race on the array and their results are undefined: order them on one stream.
+#include "bf_internal.h"
 #include "common.h"
 #include <algorithm>
 #include <mutex>
 #include <vector>
 
 namespace rsfm_b200 {
-namespace bf {
-int launch_chunk(const rsfm_sift_bf_task* tasks, size_t n, uint32_t* const* second, uint32_t* const* flags,
-                 uint32_t ratioNum, uint32_t ratioDen, cudaStream_t stream);
-}  // namespace bf
-
 namespace noalloc {
 
 constexpr size_t kNoAllocMaxRows = size_t(1) << 20;
-constexpr size_t kTasksPerLaunch = 16;  // tasks per matcher launch, as in rsfm_bf_match
+constexpr size_t kTasksPerLaunch = bf::kMaxTasksPerLaunch;  // tasks per matcher launch, as in rsfm_bf_match
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_second_scratch[kNoAllocMaxRows];
@@ -60,22 +56,15 @@ using namespace rsfm_b200;
 
 extern "C" int rsfm_bf_match_noalloc(const rsfm_sift_bf_task* tasks, size_t nbTasks, cudaStream_t stream) {
     launch_count_reset();
-    if (nbTasks > 0 && !tasks) return RSFM_ERR_INVALID_ARG;
+    // The same argument checks as rsfm_bf_match, then the scratch limit on the total query rows.
+    int st = bf::validate(tasks, nbTasks);
+    if (st != RSFM_OK) return st;
     size_t total = 0;
-    for (size_t t = 0; t < nbTasks; ++t) {
-        const rsfm_sift_bf_task& T = tasks[t];
-        if (T.nbDescA > 0 && (!T.descA || !T.bestMatchA || !T.sqrNormDescA)) return RSFM_ERR_INVALID_ARG;
-        if (T.nbDescB > 0 && (!T.descB || !T.bestMatchB || !T.sqrNormDescB)) return RSFM_ERR_INVALID_ARG;
-        if ((reinterpret_cast<uintptr_t>(T.descA) & 15u) || (reinterpret_cast<uintptr_t>(T.descB) & 15u))
-            return RSFM_ERR_INVALID_ARG;
-        if ((reinterpret_cast<uintptr_t>(T.bestMatchA) & 7u) || (reinterpret_cast<uintptr_t>(T.bestMatchB) & 7u))
-            return RSFM_ERR_INVALID_ARG;
-        total += T.nbDescA;
-    }
+    for (size_t t = 0; t < nbTasks; ++t) total += tasks[t].nbDescA;
     if (total > noalloc::kNoAllocMaxRows) return RSFM_ERR_CAPACITY;
     if (nbTasks == 0) return RSFM_OK;
     uint32_t* scratch = nullptr;
-    int st = noalloc::scratch_for_current_device(&scratch);
+    st = noalloc::scratch_for_current_device(&scratch);
     if (st != RSFM_OK) return st;
     uint32_t* second[noalloc::kTasksPerLaunch];
     size_t off = 0;

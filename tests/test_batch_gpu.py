@@ -105,6 +105,35 @@ def test_autotune_and_cache(rsfm, oracle, tmp_path):
     plan.close()
 
 
+def test_plan_batched_workload_sizes(rsfm, oracle):
+    """The batched workload at its own sizes: 64 seeded pairs with N, M ~ U[2000, 16000],
+    overlap ~ U[0.1, 0.7], noise ~ U[4, 12], through the autotuned graph plan; every output of
+    every pair against the oracle (large pairs reach full 8 x 8 units, many units per pair and the
+    largest-first schedule)."""
+    rng = np.random.default_rng(2024)
+    pairs = []
+    for i in range(64):
+        na, nb = int(rng.integers(2000, 16001)), int(rng.integers(2000, 16001))
+        q, t, _ = synth.make_pair(na, nb, float(rng.uniform(0.1, 0.7)), float(rng.uniform(4, 12)), seed=70000 + i)
+        pairs.append((q, t))
+    tasks = [rsfm.BFTask(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in pairs]
+    opts, _ = rsfm.autotune_plan(tasks, reps=1)
+    for schedule in sorted({opts.schedule, 1}):
+        opts.schedule = schedule
+        plan = rsfm.BFPlan(tasks, options=opts)
+        plan.launch()
+        torch.cuda.synchronize()
+        assert rsfm.device_error() == 0
+        for (a, b), t in zip(pairs, tasks):
+            fwd, bwd, sec, flg = _res(rsfm, t)
+            efwd, ebwd, esec = oracle.bf_match(a, b)
+            np.testing.assert_array_equal(fwd, efwd)
+            np.testing.assert_array_equal(bwd, ebwd)
+            np.testing.assert_array_equal(sec, esec)
+            np.testing.assert_array_equal(flg, oracle.match_flags(efwd, esec, ebwd))
+        plan.close()
+
+
 def test_device_generator_distribution(rsfm):
     g = torch.Generator(device="cuda")
     g.manual_seed(3)

@@ -114,18 +114,32 @@ def test_reference_api_matches_ext(rsfm, oracle):
     np.testing.assert_array_equal(np.stack([bi, bd], 1), ebwd)
 
 
-def test_full_size_sampled(rsfm, oracle):
-    # 32768 x 32768 (the dense-contraction workload): check sampled rows and columns exactly
-    # against the oracle restricted to those rows / columns.
+def test_full_size_exact(rsfm, oracle):
+    # The dense-contraction workload itself (32768 x 32768, 50 % overlap, noise 10, seed 1: the
+    # pair bench.py times): every forward match, second-best distance, flag word and backward
+    # match against the oracle's exhaustive loop (test/bruteForceMatchKernelTest.cpp:140-164 with
+    # the (distance, index) tie rule of bruteForceMatch.cuh:110-187).
     q, t, _ = synth.make_pair(32768, 32768, 0.5, 10.0, seed=1)
-    fwd, bwd, sec, flags = _run_ext(rsfm, [(q, t)])[0]
-    rng = np.random.default_rng(7)
-    rows = rng.choice(32768, 192, replace=False)
-    cols = rng.choice(32768, 192, replace=False)
-    efwd, _, esec = oracle.bf_match(q[rows], t)
-    np.testing.assert_array_equal(fwd[rows], efwd)
-    np.testing.assert_array_equal(sec[rows], esec)
-    ebwd, _, _ = oracle.bf_match(t[cols], q)
-    np.testing.assert_array_equal(bwd[cols], ebwd)
-    # flags are a pure function of fwd/bwd/second
-    np.testing.assert_array_equal(flags, oracle.match_flags(fwd, sec, bwd))
+    _check(oracle, q, t, _run_ext(rsfm, [(q, t)])[0])
+
+
+def test_full_size_reference_entry(rsfm, oracle):
+    # Same pair through the reference-shaped entry point (rsfm_bf_match, no extension outputs).
+    q, t, _ = synth.make_pair(32768, 32768, 0.5, 10.0, seed=1)
+    task = rsfm.BFTask(_dev(q), _dev(t))
+    rsfm.bf_match([task])
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    fi, fd = rsfm.unpack_best(task.bestA)
+    bi, bd = rsfm.unpack_best(task.bestB)
+    efwd, ebwd, _ = oracle.bf_match(q, t)
+    np.testing.assert_array_equal(np.stack([fi, fd], 1), efwd)
+    np.testing.assert_array_equal(np.stack([bi, bd], 1), ebwd)
+
+
+def test_uniform_large_exact(rsfm, oracle):
+    # Uniform random bytes (norms spread over a wide range, unlike SIFT-like rows) at a size with
+    # many units per row and column: 12288 x 9000.
+    a = synth.uniform_bytes(12288, 21)
+    b = synth.uniform_bytes(9000, 22)
+    _check(oracle, a, b, _run_ext(rsfm, [(a, b)])[0])

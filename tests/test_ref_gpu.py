@@ -64,6 +64,20 @@ def test_bf_matches_reference_kernels(ref, rsfm, oracle, name, make):
     np.testing.assert_array_equal(np.stack([bi, bd], 1), rb)
 
 
+def test_headline_pair_matches_reference_kernels(ref, rsfm):
+    """The 32768 x 32768 pair that bench.py times (seed 1), through RapidSFM's own launcher and
+    ours: every forward and backward (index, distance) identical."""
+    q, t, _ = synth.make_pair(32768, 32768, 0.5, 10.0, seed=1)
+    rf, rb, _ = _ref_bf(ref, q, t)
+    task = rsfm.BFTask(torch.from_numpy(q).cuda(), torch.from_numpy(t).cuda())
+    rsfm.bf_match([task])
+    torch.cuda.synchronize()
+    fi, fd = rsfm.unpack_best(task.bestA)
+    bi, bd = rsfm.unpack_best(task.bestB)
+    np.testing.assert_array_equal(np.stack([fi, fd], 1), rf)
+    np.testing.assert_array_equal(np.stack([bi, bd], 1), rb)
+
+
 def test_ties_match_reference_kernels(ref, rsfm):
     base = synth.uniform_bytes(40, 3)
     rng = np.random.default_rng(0)

@@ -52,6 +52,30 @@ def test_noalloc_matches_bf_match_two_calls(rsfm):
     assert rsfm.device_error() == 0
 
 
+def test_noalloc_many_tasks_and_empty_sides(rsfm, oracle):
+    """20 small pairs (two matcher launches of up to 16 tasks, so the scratch offset runs across a
+    launch boundary), some with no query or no train rows: equal to rsfm_bf_match on every pair,
+    and to the CPU oracle directly on a few."""
+    pairs = []
+    for k in range(20):
+        na = 0 if k in (3, 17) else 60 + 41 * k
+        nb = 0 if k in (5, 16) else 75 + 29 * k
+        q, t, _ = synth.make_pair(max(na, 1), max(nb, 1), 0.5, 6.0, seed=300 + k)
+        pairs.append((q[:na], t[:nb]))
+    want = _call(rsfm, "rsfm_bf_match", pairs)
+    got = _call(rsfm, "rsfm_bf_match_noalloc", pairs)
+    for (wa, wb), (ga, gb) in zip(want, got):
+        np.testing.assert_array_equal(ga, wa)
+        np.testing.assert_array_equal(gb, wb)
+    for k in (0, 5, 15, 16, 19):
+        a, b = pairs[k]
+        efwd, ebwd, _ = oracle.bf_match(a, b)
+        ga, gb = got[k]
+        np.testing.assert_array_equal(ga.view(np.uint32).reshape(-1, 2), efwd)
+        np.testing.assert_array_equal(gb.view(np.uint32).reshape(-1, 2), ebwd)
+    assert rsfm.device_error() == 0
+
+
 def test_noalloc_rejects_oversize(rsfm):
     lib = rsfm._lib.load()
     d = torch.zeros((16, 128), dtype=torch.uint8, device="cuda")
