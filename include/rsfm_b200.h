@@ -161,7 +161,21 @@ int rsfm_remove_match_conflicts_device(const rsfm_best_match* matches, uint32_t 
  * per image cell, random 3-match affine fits over the 3x3 cell neighbourhood; each cell's best
  * model (or the best of every cell's models, tryOtherSolutions) votes for its inliers when it
  * has >= 6. The reference seeds its generator from clock(); here `seed` makes runs repeatable.
- * A cell whose neighbourhood holds fewer than 9 matches gets the zero model (no votes). */
+ * A cell whose neighbourhood holds fewer than 9 matches gets the zero model (no votes).
+ * tryOtherSolutions / tryOtherAffines:
+ *   RSFM_RANSAC_OWN_MODEL (0)     each cell's own best model votes (kernelComputeVotes);
+ *   RSFM_RANSAC_TRY_OTHER (1)     the best of every cell's models on the neighbourhood, voting as
+ *                                 the reference's kernelTryBestAffineOfOtherCellsAndVote does
+ *                                 (RansacMatchFilter.cu:305-330): each of the 128 threads tests
+ *                                 the 6-inlier gate on its own partial maximum of the CTA tree
+ *                                 (only thread 0 holds the full maximum), so the inliers at
+ *                                 neighbourhood positions i (mod 128) of a thread whose partial
+ *                                 maximum is below 6 get no vote;
+ *   RSFM_RANSAC_TRY_OTHER_ALL (2) the same model, every inlier votes when it has >= 6 inliers
+ *                                 (no reference counterpart). */
+#define RSFM_RANSAC_OWN_MODEL 0
+#define RSFM_RANSAC_TRY_OTHER 1
+#define RSFM_RANSAC_TRY_OTHER_ALL 2
 
 /* rmf::PtPair (RansacMatchFilter.cuh:20-24): left and right point of a match, 16-byte aligned. */
 typedef struct rsfm_pt_pair {
@@ -217,6 +231,15 @@ int rsfm_cashash_accumulate_desc(unsigned long long* acc, int initAcc, const voi
 int rsfm_cashash_compute_bias(int32_t* bias, const void* weights, const int32_t* biasBase,
                               const unsigned long long* acc, unsigned long long nbDesc, int nbChannels,
                               cudaStream_t stream);
+
+/* Replaces cashash::computeBias (cascadeHash.h:33-35, accumulateDesc.cu:136-182) bit for bit:
+ * the reference's own float evaluation (-acc[d] / nbDesc in float; per channel eight partial sums
+ * of sixteen multiply-adds, an xor-shuffle sum, round(), plus biasBase), compiled with the
+ * reference's --use_fast_math. nbChannels is 64 or 192 (channels past 64 follow the same formula).
+ * rsfm_precomp_for_match computes its bias this way, so its keys equal the reference's. */
+int rsfm_cashash_compute_bias_fast_math(int32_t* bias, const void* weights, const int32_t* biasBase,
+                                        const unsigned long long* acc, unsigned long long nbDesc, int nbChannels,
+                                        cudaStream_t stream);
 
 /* Replaces cashash::computeHashForBucketOnly (nbChannels = 64) and computeHashForBucketAndRemap
  * (nbChannels = 192) (cascadeHash.h:43-56, computeHash.cu:474-520). Bit c of descriptor i is
@@ -443,7 +466,8 @@ typedef void (*rsfm_max_bucket_size_handler)(uint32_t maxBucketSize, void* user)
  * (rsfm_precomp_sift4b_sqr_norm computes those).
  * Cascade hash (all device memory except accNbDesc and pinnedScratch): acc (128 x uint64) and
  * *accNbDesc (host) accumulate the descriptors of every image registered so far and the bias is
- * computed from them, so keys depend on the registration order as in the reference; weights are
+ * computed from them (the reference's float evaluation, rsfm_cashash_compute_bias_fast_math), so
+ * keys equal the reference's and depend on the registration order as in the reference; weights are
  * 64 x 128 int8 rows (KArray<int32_t, 64, 32>), biasBase 64 int32; deviceScratch has
  * rsfm_precomp_device_scratch_nb_bytes bytes and pinnedScratch (page-locked host memory)
  * rsfm_precomp_pinned_scratch_nb_bytes; both are reused by the next call on the same stream.

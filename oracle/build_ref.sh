@@ -26,3 +26,16 @@ NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
   "$HERE/ref_wrapper.cu"
 mv "$OUT/librsfm_ref.so.tmp" "$OUT/librsfm_ref.so"
 echo "$OUT/librsfm_ref.so"
+# RANSAC match filter (RansacMatchFilter.cu), twice: with the reference's flags, and with
+# -fmad=false and the shim's arithmetic in the B200 kernel's order (bit-for-bit comparison).
+if [ -f "$REF/RansacMatchFilter.cu" ]; then
+  "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 --use_fast_math -DNDEBUG \
+    --expt-relaxed-constexpr -Xcompiler -fPIC -shared -DRSFM_REF_SEED_HOOK \
+    -I"$HERE/ref_shim" -I"$REF" -o "$OUT/librsfm_ref_ransac.so.tmp" "$HERE/ref_ransac_wrapper.cu"
+  mv "$OUT/librsfm_ref_ransac.so.tmp" "$OUT/librsfm_ref_ransac.so"
+  "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -fmad=false -DNDEBUG \
+    --expt-relaxed-constexpr -Xcompiler -fPIC -shared -DRSFM_REF_SEED_HOOK -DRSFM_SHIM_KMAT_MATCH \
+    -I"$HERE/ref_shim" -I"$REF" -o "$OUT/librsfm_ref_ransac_ieee.so.tmp" "$HERE/ref_ransac_wrapper.cu"
+  mv "$OUT/librsfm_ref_ransac_ieee.so.tmp" "$OUT/librsfm_ref_ransac_ieee.so"
+  echo "$OUT/librsfm_ref_ransac.so $OUT/librsfm_ref_ransac_ieee.so"
+fi

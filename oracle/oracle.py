@@ -331,6 +331,29 @@ def ransac_inlier_mask(width, height, pairs, min_votes=2, n_tests=256, rel_thres
 _ref = None
 
 
+_ref_ransac = {}
+
+
+def ref_ransac_available():
+    return all(os.path.exists(os.path.join(HERE, "_ref", f"librsfm_ref_ransac{k}.so")) for k in ("", "_ieee"))
+
+
+def load_ref_ransac(kind=""):
+    """RapidSFM's RANSAC match filter kernels (RansacMatchFilter.cu) built by oracle/build_ref.sh:
+    kind "" with the reference's flags, "_ieee" with -fmad=false and the shim's arithmetic in
+    the B200 kernel's order. ref_ransac_match_filter(votes, affineScratch, matches, n, bounds,
+    cols, rows, tests, threshold, tryOther, seed, stream)."""
+    if kind in _ref_ransac:
+        return _ref_ransac[kind]
+    lib = ctypes.CDLL(os.path.join(HERE, "_ref", f"librsfm_ref_ransac{kind}.so"))
+    u32 = ctypes.c_uint32
+    fn = lib.ref_ransac_match_filter
+    fn.restype = ctypes.c_int
+    fn.argtypes = [_P, _P, _P, u32, _P, u32, u32, u32, ctypes.c_float, ctypes.c_int, u32, _P]
+    _ref_ransac[kind] = lib
+    return lib
+
+
 def ref_available():
     return os.path.exists(REF_LIB_PATH)
 

@@ -186,7 +186,10 @@ void orc_ransac_models(const float* matches, const uint32_t* bounds, uint32_t co
 }
 
 // Votes (u8 per match) from the models: each cell's own model (tryOther = 0) or the best of all
-// cells' models on its neighbourhood (tryOther = 1); +1 per inlier when >= 6 inliers.
+// cells' models on its neighbourhood (tryOther = 1, 2); +1 per inlier when >= 6 inliers. With
+// tryOther = 1 the gate is the reference's (RansacMatchFilter.cu:305-330): the inlier at
+// neighbourhood position i is voted for by thread i mod 128, which tests its own partial maximum
+// of the CTA tree (n[t] after tree_max; only n[0] is the full maximum).
 void orc_ransac_votes(const float* matches, uint32_t nbMatches, const uint32_t* bounds, uint32_t cols,
                       uint32_t rows, const float* affines, float threshold, int tryOther, uint8_t* votes) {
     const Pt* pts = reinterpret_cast<const Pt*>(matches);
@@ -199,6 +202,7 @@ void orc_ransac_votes(const float* matches, uint32_t nbMatches, const uint32_t* 
             const Hood h(bounds, cols, rows, cy, cx);
             Aff best = models[cell];
             uint32_t bestN = 0;
+            std::vector<uint32_t> gate;  // per thread (tryOther = 1)
             if (tryOther) {
                 std::vector<uint32_t> n(kCta, 0);
                 std::vector<Aff> a(kCta, models[cell]);
@@ -213,12 +217,14 @@ void orc_ransac_votes(const float* matches, uint32_t nbMatches, const uint32_t* 
                 tree_max(n, a);
                 best = a[0];
                 bestN = n[0];
+                if (tryOther == 1) gate = n;
             } else {
                 bestN = h.count(best, pts, threshold);
             }
             if (bestN < kMinInliers) continue;
             const float thr = sqr_threshold(best, threshold);
             for (uint32_t i = 0; i < h.sum; ++i) {
+                if (!gate.empty() && gate[i % kCta] < kMinInliers) continue;
                 const uint32_t m = h.match(i);
                 if (inlier(best, pts[m], thr)) votes[m] = uint8_t(votes[m] + 1);
             }

@@ -38,3 +38,13 @@ void launchKernel(Kernel kernel, dim3 grid, dim3 block, size_t smem, cudaStream_
     cudaCheck(cudaGetLastError());
 }
 #endif
+
+#ifdef RSFM_REF_SEED_HOOK
+// RANSAC reference builds only: the reference seeds each launch from clock()
+// (RansacMatchFilter.cu:216); here clock() reads a seed the test sets, so a run is reproducible
+// and comparable with the B200 kernel's seeded one. This header is the last one the reference
+// file includes, so the macro reaches only that file's own code.
+__device__ uint32_t g_rsfm_ref_seed;
+__device__ __forceinline__ uint32_t rsfm_ref_seed_clock() { return g_rsfm_ref_seed; }
+#define clock() rsfm_ref_seed_clock()
+#endif

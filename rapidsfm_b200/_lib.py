@@ -162,6 +162,9 @@ SIGNATURES = {
                                                     ctypes.c_void_p]),
     "rsfm_cashash_compute_bias": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    "rsfm_cashash_compute_bias_fast_math": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                           ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                                           ctypes.c_void_p]),
     "rsfm_cashash_compute_hash": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p]),

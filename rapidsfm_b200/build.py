@@ -31,6 +31,12 @@ SOURCES = [
     "mlp.cu",
 ]
 
+# Compiled on their own with the reference's --use_fast_math (their float results must equal the
+# reference's kernels', which are built with it), then linked with the rest.
+FAST_MATH_SOURCES = [
+    "cashash_bias_fastmath.cu",
+]
+
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -64,7 +70,19 @@ def build_library(force=False, verbose=False):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES]
+    objs = []
+    for s in FAST_MATH_SOURCES:
+        obj = os.path.join(LIBDIR, os.path.splitext(s)[0] + ".o")
+        flags = [f for f in NVCC_FLAGS if f != "-shared"]
+        cmd = [_nvcc()] + flags + ["--use_fast_math", "-c", "-o", obj, os.path.join(CSRC, s)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError(f"nvcc failed compiling {s}")
+        objs.append(obj)
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + objs
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)

@@ -126,7 +126,7 @@ extern "C" int rsfm_precomp_for_match(void* dst, const void* desc, uint32_t nbDe
             st = step(rsfm_cashash_accumulate_desc(acc, *accNbDesc == 0 ? 1 : 0, desc, nbDesc, stream));
             if (st == RSFM_OK) {
                 *accNbDesc += nbDesc;
-                st = step(rsfm_cashash_compute_bias(S.bias, casHashWeights, casHashBiasBase, acc, *accNbDesc, 64,
+                st = step(rsfm_cashash_compute_bias_fast_math(S.bias, casHashWeights, casHashBiasBase, acc, *accNbDesc, 64,
                                                     stream));
             }
             if (st == RSFM_OK)

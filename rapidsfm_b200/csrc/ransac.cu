@@ -6,8 +6,10 @@
 // every cell, `nbTests` random 3-match affine fits over its 3x3 cell neighbourhood are scored by
 // inlier count (|A l + t - r|^2 < (threshold * min(sqrt(det A), 1))^2, det A in [1/16, 16]);
 // the best model of each cell (or, with tryOther, the best of all cells' models on that
-// neighbourhood) gives +1 vote to each of its inliers when it has at least 6. A match is kept
-// with >= minVotes votes.
+// neighbourhood) gives +1 vote to each of its inliers when it has at least 6 (with tryOther = 1,
+// as the reference does it: thread t of the cell's CTA votes for neighbourhood positions t mod 128
+// only when its own partial maximum of the CTA tree has 6; tryOther = 2 lets every inlier vote).
+// A match is kept with >= minVotes votes.
 //
 // Behaviour kept from the reference: the LCG (glibc constants, :44-49) and per-thread seeding
 // (seed + (128 * cell + thread) * 22695477), test t on thread t % 128, duplicate rejection of
@@ -278,7 +280,9 @@ __global__ void __launch_bounds__(kCta) votes_kernel(const __grid_constant__ Par
         }
         tree_max(R, n, a);
         best = R.a[0];
-        bestN = R.n[0];
+        // The reference gates each thread's votes on its own partial maximum of the tree
+        // (RansacMatchFilter.cu:317-330; thread 0 alone holds the CTA maximum), slot t here.
+        bestN = tryOther == 1 ? R.n[threadIdx.x] : R.n[0];
     } else {
         if (threadIdx.x == 0) total = 0;
         __syncthreads();
@@ -338,6 +342,8 @@ int validate(const rsfm_ransac_task* tasks, size_t n) {
     return RSFM_OK;
 }
 
+bool valid_mode(int tryOther) { return tryOther >= 0 && tryOther <= 2; }
+
 }  // namespace rsc
 }  // namespace rsfm_b200
 
@@ -346,6 +352,7 @@ using namespace rsfm_b200;
 extern "C" int rsfm_ransac_match_filter_batch(const rsfm_ransac_task* tasks, size_t nbTasks, uint32_t nbRansacTests,
                                               int tryOtherSolutions, uint32_t seed, cudaStream_t stream) {
     launch_count_reset();
+    if (!rsc::valid_mode(tryOtherSolutions)) return RSFM_ERR_INVALID_ARG;
     int st = rsc::validate(tasks, nbTasks);
     if (st != RSFM_OK) return st;
     uint32_t launches = 0;
@@ -370,7 +377,8 @@ extern "C" int rsfm_ransac_inlier_mask(int imgWidth, int imgHeight, const rsfm_p
                                        uint32_t cellCols, int tryOtherAffines, uint32_t seed, uint8_t* mask,
                                        cudaStream_t stream) {
     launch_count_reset();
-    if (imgWidth <= 0 || imgHeight <= 0 || cellCols == 0 || (nbMatches > 0 && (!matches || !mask)))
+    if (imgWidth <= 0 || imgHeight <= 0 || cellCols == 0 || (nbMatches > 0 && (!matches || !mask)) ||
+        !rsc::valid_mode(tryOtherAffines))
         return RSFM_ERR_INVALID_ARG;
     if (nbMatches == 0) return RSFM_OK;
     const uint32_t cellWidth = (uint32_t(std::max(imgWidth, imgHeight)) + cellCols - 1) / cellCols;

@@ -7,6 +7,11 @@ Reference interfaces mirrored (paths relative to the RapidSFM source tree):
 
 The reference seeds its random generator from clock(); here every call takes a seed, so results
 are repeatable. Matches are float32 [n, 4] rows (left x, left y, right x, right y).
+
+try_other / try_other_affines: False (0) each cell's own model votes; True (1) the best of every
+cell's models, voting exactly as the reference's kernelTryBestAffineOfOtherCellsAndVote does (each
+CTA thread gates its stride of the neighbourhood on its own partial tree maximum); 2 the same
+model with every inlier voting (no reference counterpart).
 """
 import ctypes
 

@@ -117,6 +117,62 @@ def test_accumulate_and_bias(rsfm, oracle, ref):
         np.testing.assert_array_equal(racc.cpu().numpy().view(np.uint64), eacc)
         # the reference evaluates in float under fast-math; its own test allows +-1
         assert np.abs(rb.cpu().numpy() - got).max() <= 1
+        # the fast-math entry point reproduces the reference's float evaluation bit for bit
+        fm = torch.empty(64, dtype=torch.int32, device="cuda")
+        rsfm._lib.check(lib.rsfm_cashash_compute_bias_fast_math(_ptr(fm), _ptr(dw), _ptr(dbase), _ptr(acc),
+                                                                len(a) + len(b2), 64, None), "bias_fm")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(fm.cpu().numpy(), rb.cpu().numpy())
+
+
+def test_bias_fast_math_equals_reference(rsfm, oracle, ref):
+    """rsfm_cashash_compute_bias_fast_math against RapidSFM's own computeBias kernel
+    (accumulateDesc.cu:136-182) over many accumulators and descriptor counts, with the matcher's
+    weights and with random weights: identical biases. Channels 64..191 of a 192-channel call
+    follow the same formula (first 64 equal the 64-channel call)."""
+    if ref is None:
+        pytest.skip("reference kernels not built")
+    lib = rsfm._lib.load()
+    rng = np.random.default_rng(77)
+    w0, base0 = oracle.cashash_weights()
+    mismatch_exact = 0
+    for trial in range(200):
+        if trial % 2:
+            w = w0
+            base = base0
+        else:
+            w = rng.integers(-128, 128, (64, 128), dtype=np.int8)
+            base = rng.integers(-5000, 5000, 64, dtype=np.int32)
+        n = int(rng.choice([1, 3, 7, 100, 8192, 123457, 1 << 24, int(rng.integers(1, 1 << 30))]))
+        # accumulators of n descriptors: sums of (x >> 1) <= 127 per descriptor
+        mean = rng.uniform(0, 127, 128)
+        acc = np.minimum(np.round(mean * n), 127 * n).astype(np.uint64)
+        dw, db, da = _dev(w), _dev(base), _dev(acc.view(np.int64))
+        rb = torch.empty(64, dtype=torch.int32, device="cuda")
+        fm = torch.empty(64, dtype=torch.int32, device="cuda")
+        assert ref.ref_cashash_compute_bias(_ptr(rb), _ptr(dw), _ptr(db), _ptr(da), n, None) == 0
+        rsfm._lib.check(lib.rsfm_cashash_compute_bias_fast_math(_ptr(fm), _ptr(dw), _ptr(db), _ptr(da), n, 64, None),
+                        "bias_fm")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(fm.cpu().numpy(), rb.cpu().numpy())
+        mismatch_exact += int((fm.cpu().numpy() != oracle.cashash_bias(w, base, acc, n)).sum())
+    # 192 channels: the first 64 rows give the 64-channel result
+    w192 = rng.integers(-128, 128, (192, 128), dtype=np.int8)
+    w192[:64] = w0
+    b192 = rng.integers(-5000, 5000, 192, dtype=np.int32)
+    b192[:64] = base0
+    acc = np.round(rng.uniform(0, 127, 128) * 5000).astype(np.uint64)
+    dw, db, da = _dev(w192), _dev(b192), _dev(acc.view(np.int64))
+    f192 = torch.empty(192, dtype=torch.int32, device="cuda")
+    f64 = torch.empty(64, dtype=torch.int32, device="cuda")
+    rsfm._lib.check(lib.rsfm_cashash_compute_bias_fast_math(_ptr(f192), _ptr(dw), _ptr(db), _ptr(da), 5000, 192, None),
+                    "bias_fm192")
+    rsfm._lib.check(lib.rsfm_cashash_compute_bias_fast_math(_ptr(f64), _ptr(dw), _ptr(db), _ptr(da), 5000, 64, None),
+                    "bias_fm64")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(f192.cpu().numpy()[:64], f64.cpu().numpy())
+    assert np.abs(f192.cpu().numpy() - oracle.cashash_bias(w192, b192, acc, 5000)).max() <= 1
+    print("biases differing from the exact rational rounding:", mismatch_exact, "of", 200 * 64)
 
 
 @pytest.mark.parametrize("n", [1, 164, 897, 20000])
