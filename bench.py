@@ -453,6 +453,7 @@ def run_ours(args):
         extras["cascade"] = run_cascade(dev, stream, n_pairs=args.cascade_pairs)
         extras["hash"] = run_hash(dev, stream, n=1 << args.hash_log2)
         extras["ransac"] = run_ransac(dev, stream)
+        extras["training"] = run_training(dev, stream)
 
     line = {
         "metric": METRIC,
@@ -794,6 +795,67 @@ def run_hash(dev, stream, n=1 << 24):
     return out
 
 
+TRAIN_FLOP_PER_ROW = 5 * 2 * 128 * 256  # five contractions of 128 x 256 per gathered row (3 rows per triplet)
+
+
+def run_training(dev, stream, batch=4096, steps=300, seed=7):
+    """Learned-hash trainer throughput: batch-4096 triplet steps (gather, forward, triplet loss,
+    backward, Adam; the five contractions on the tensor cores) over synthetic SIFT-like pairs with
+    known correspondences; triplet indices drawn on the device every step, as the training loop
+    does. Reports ms per step, the projected time of the 20k-step training run and the
+    contractions' TFLOP/s against the measured bf16 peak."""
+    import torch
+    from rapidsfm_b200 import learned_hash as lh
+    from rapidsfm_b200 import synth
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    n = 8192
+    qs, ts, A, P = [], [], [], []
+    for k in range(8):
+        q, t, truth = synth.make_pair_torch(n, n, 0.4, 8.0, g, dev)
+        pos = torch.nonzero(truth >= 0).flatten()
+        qs.append(q)
+        ts.append(t)
+        A.append(truth[pos] + k * n)
+        P.append(pos + k * n)
+    Q, T, A, P = torch.cat(qs), torch.cat(ts), torch.cat(A), torch.cat(P)
+    tr = lh.Trainer(lh.init_params(seed), batch, lr=1e-3, margin=48.0)
+
+    def one():
+        sel = torch.randint(0, len(A), (batch,), device=dev, generator=g)
+        ip = P[sel].int()
+        inn = ((ip // n) * n + torch.randint(0, n, (batch,), device=dev, generator=g)).int()
+        tr.step(Q, A[sel].int(), T, ip, T, inn, stream=stream)
+
+    with torch.cuda.stream(stream):
+        ms = _events_ms(one, steps, stream)
+        first = float(tr.loss.item())
+        for _ in range(50):
+            one()
+        last = float(tr.loss.item())
+    tr.close()
+    flop = TRAIN_FLOP_PER_ROW * 3 * batch
+    tf = flop / (ms * 1e-3) / 1e12
+    bf16 = _peaks().get("bf16_tflops")
+    return {"batch": batch, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "projected_20k_steps_s": 20000 * ms / 1e3,
+            "contraction_flop_per_step": flop, "TFLOP/s": tf, "frac_of_measured_bf16": tf / bf16 if bf16 else None,
+            "loss_first_last": [first, last], "timed_steps": steps}
+
+
+def run_full_training(dev):
+    """The learned hash's full training run as the package performs it (rapidsfm_b200.learned_hash
+    train_from_brute_force: brute-force correspondences of 200 seeded pairs of 8192, then 20k
+    steps of batch 4096), wall time of each phase."""
+    import torch
+    from rapidsfm_b200 import learned_hash as lh
+    t0 = time.perf_counter()
+    times = {}
+    params = lh.train_from_brute_force(log=lambda m: times.setdefault("log", []).append(m), timings=times)
+    torch.cuda.synchronize()
+    times["total_s"] = time.perf_counter() - t0
+    return params, times
+
+
 def run_ransac(dev, stream, n_pairs=1000, n=4000, seed=6, cpu_pairs=8):
     """RANSAC match filter (the step after matching) on n_pairs image pairs of n matches each
     (1600x1200, 60 % inliers, 16 cell columns, 256 tests, tryOtherAffines as in the reference's
@@ -851,7 +913,22 @@ def main():
     ap.add_argument("--only-ransac", action="store_true", help="run the RANSAC-filter section alone (profiling)")
     ap.add_argument("--ransac-pairs", type=int, default=1000)
     ap.add_argument("--hash-log2", type=int, default=24, help="log2 of the descriptors in the hashing section")
+    ap.add_argument("--only-train", action="store_true", help="run the trainer-throughput section alone")
+    ap.add_argument("--full-training", default="",
+                    help="run the learned hash's whole training (200 pairs, 20k steps), time it and save the "
+                         "parameter block to this path")
     args = ap.parse_args()
+    if args.only_train or args.full_training:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        out = {"training": run_training(dev, torch.cuda.current_stream(dev))}
+        if args.full_training:
+            params, times = run_full_training(dev)
+            np.save(args.full_training, params)
+            out["full_training"] = times
+        print(json.dumps(out), flush=True)
+        return
     if args.only_ransac:
         import torch
         dev = torch.device("cuda", 0)

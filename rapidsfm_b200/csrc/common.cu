@@ -70,6 +70,23 @@ int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows) {
     return r == CUDA_SUCCESS ? RSFM_OK : RSFM_ERR_INVALID_ARG;
 }
 
+int encode_bf16_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint64_t cols, uint64_t pitchElems,
+                     uint32_t boxRows) {
+    auto fn = get_encode_fn();
+    if (!fn) return RSFM_ERR_UNSUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (pitchElems * 2) % 16 != 0 || boxRows == 0 ||
+        boxRows > 256 || pitchElems < cols)
+        return RSFM_ERR_INVALID_ARG;
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {pitchElems * 2};
+    cuuint32_t box[2] = {64, boxRows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? RSFM_OK : RSFM_ERR_INVALID_ARG;
+}
+
 // Stream-ordered scratch comes from a pool of this library (one per device) that keeps its memory
 // between calls: the device's default pool returns freed memory to the system at every
 // synchronisation (release threshold 0), and mapping it again costs tens of microseconds a call.

@@ -35,6 +35,12 @@ int encode_desc_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint32_t
 // 2D uint8 tensor map for one-row gathers (tile::gather4): box = 1 x 128 bytes, no swizzle.
 int encode_desc_tmap_gather(CUtensorMap* out, const void* base, uint64_t rows);
 
+// 2D bf16 tensor map over a row-major [rows][cols] array with a row pitch of pitchElems elements
+// (pitchElems * 2 a multiple of 16), tile = boxRows x 64 elements (128 bytes), 128-byte swizzle
+// (the K-major SW128 layout of the UMMA descriptors). Elements past the array read as zero.
+int encode_bf16_tmap(CUtensorMap* out, const void* base, uint64_t rows, uint64_t cols, uint64_t pitchElems,
+                     uint32_t boxRows);
+
 int sm_count();
 // Raises a kernel's dynamic shared-memory limit on the current device, once per (kernel, device):
 // the attribute belongs to the device's context, so a process using several GPUs sets it on each.

@@ -4,7 +4,8 @@
 //   x = desc / 64;  h = bf16(relu(W1 x + b1));  o = W2 h + b2;  bit c = [o_c > 0]
 // Inference runs on the tensor cores (tcgen05 kind::f16, bf16 x bf16 -> f32 in TMEM) with both
 // layers fused per 128-descriptor tile. Training (triplet loss on tanh(o), Adam on fp32 master
-// weights) uses CUDA-core kernels: a split-K tiled GEMM plus elementwise kernels.
+// weights) runs its five contractions on the tensor cores too (bf16 operands, fp32 accumulation,
+// split-K for the weight gradients) with small elementwise kernels between them.
 #include "common.h"
 #include "sm100.cuh"
 #include <cuda_bf16.h>
@@ -234,72 +235,189 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
     if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
-// ---------------------------------------------------------------- training (CUDA cores)
-// C[m][n] (+)= alpha * sum_k A(m,k) B(k,n), generic strides; split-K over gridDim.z with atomics
-// when `atomic` is set (C must then be zeroed beforehand).
-enum Ty { kF32 = 0, kBF16 = 1, kU8 = 2 };
-__device__ __forceinline__ float ld_any(const void* p, size_t i, int ty) {
-    if (ty == kF32) return static_cast<const float*>(p)[i];
-    if (ty == kBF16) return bf16_to_f(static_cast<const uint16_t*>(p)[i]);
-    return float(static_cast<const uint8_t*>(p)[i]);
-}
-constexpr int kTM = 64, kTN = 64, kTK = 16;
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const void* A, int ta, long sam, long sak,
-                                                   const void* B, int tb, long sbk, long sbn, float* C, long scm,
-                                                   long scn, float alpha, int atomic, int kPerSplit) {
-    __shared__ float As[kTK][kTM + 1];
-    __shared__ float Bs[kTK][kTN + 1];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
-    const int k0 = blockIdx.z * kPerSplit, k1 = min(K, k0 + kPerSplit);
-    float acc[4][4] = {};
-    for (int kb = k0; kb < k1; kb += kTK) {
-        for (int x = threadIdx.x; x < kTK * kTM; x += 256) {
-            const int kk = x / kTM, mm = x % kTM;
-            const int m = m0 + mm, k = kb + kk;
-            As[kk][mm] = (m < M && k < k1) ? ld_any(A, size_t(m) * sam + size_t(k) * sak, ta) : 0.f;
-        }
-        for (int x = threadIdx.x; x < kTK * kTN; x += 256) {
-            const int kk = x / kTN, nn = x % kTN;
-            const int nidx = n0 + nn, k = kb + kk;
-            Bs[kk][nn] = (nidx < N && k < k1) ? ld_any(B, size_t(k) * sbk + size_t(nidx) * sbn, tb) : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kTK; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int m = m0 + ty * 4 + i, nidx = n0 + tx * 4 + j;
-            if (m < M && nidx < N) {
-                float* c = C + size_t(m) * scm + size_t(nidx) * scn;
-                if (atomic) atomicAdd(c, alpha * acc[i][j]);
-                else *c = alpha * acc[i][j];
-            }
-        }
+// ---------------------------------------------------------------- training (tensor cores)
+// Every contraction of the trainer is D[M][N] = A[M][K] . B[N][K]^T on the tensor cores (tcgen05
+// kind::f16, bf16 operands, fp32 accumulator in TMEM). A and B are bf16 arrays in global memory
+// with K contiguous: the kernels that produce the activations also write the transposed copies the
+// weight gradients need, so every operand is K-major. TMA loads 64-element K panels (128-byte
+// swizzle) of A (128 rows) and B (N rows) into a kGStages-deep ring. One 128-row M tile per CTA
+// (blockIdx.x) and one K range per CTA (blockIdx.y: split-K); N (128 or 256) is the whole width.
+// Warp 0 = TMA producer, warp 1 = TMEM allocator and MMA issuer, warps 2-5 = epilogue (TMEM lane
+// quarter warp % 4, one output row per thread, 32 columns per TMEM load).
+constexpr int kGStages = 4;
+constexpr int kGThreads = 192;
+enum GemmEpi : int {
+    kEpiStoreF32 = 0,      // outF[m][n] = d
+    kEpiBiasReluBf16 = 1,  // h = bf16(relu(d + bias[n])) into outB[m][n] and outT[n][m]
+    kEpiReluGrad = 2,      // g = d * [mask[m][n] > 0] into outF[m][n] (fp32) and outT[n][m] (bf16)
+    kEpiAtomicF32 = 3,     // outF[m][n] += d (split-K partial sums into a zeroed outF)
+};
+struct GemmArgs {
+    CUtensorMap tmA, tmB;
+    uint32_t M, N, K, kPerCta;
+    int epi;
+    float* outF;
+    uint16_t* outB;
+    uint16_t* outT;
+    const float* bias;
+    const uint16_t* mask;
+    uint32_t ldF, ldB, ldT, ldMask;
+    uint32_t* err;
+};
+struct GemmSmem {
+    uint8_t a[kGStages][128 * 128];  // 128 rows x 64 bf16
+    uint8_t b[kGStages][256 * 128];  // up to 256 rows x 64 bf16
+    uint64_t full[kGStages], empty[kGStages], done;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float f) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(f);
+    return *reinterpret_cast<const uint16_t*>(&b);
 }
 
-// hpre += b1 ; h = bf16(relu(hpre))
-__global__ void bias_relu_kernel(float* __restrict__ hpre, const float* __restrict__ b1, uint16_t* __restrict__ h,
-                                 size_t total) {
-    for (size_t x = blockIdx.x * size_t(blockDim.x) + threadIdx.x; x < total; x += size_t(gridDim.x) * blockDim.x) {
-        const float v = hpre[x] + b1[x & 255u];
-        hpre[x] = v;
-        const __nv_bfloat16 bv = __float2bfloat16_rn(fmaxf(v, 0.f));
-        h[x] = *reinterpret_cast<const uint16_t*>(&bv);
+__global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(const __grid_constant__ GemmArgs G) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    GemmSmem& S = smem_aligned_1024<GemmSmem>(smem_raw);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t m0 = blockIdx.x * 128u;
+    const uint32_t k0 = blockIdx.y * G.kPerCta;
+    const uint32_t k1 = min(G.K, k0 + G.kPerCta);
+    const uint32_t steps = k1 > k0 ? (k1 - k0 + 63u) / 64u : 0u;
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kGStages; ++st) {
+            mbar_init(&S.full[st], 1);
+            mbar_init(&S.empty[st], 1);
+        }
+        mbar_init(&S.done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&S.tmem, 256);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    if (warp == 0) {
+        if (elect_one()) {
+            const uint32_t bytes = 128u * 128u + G.N * 128u;  // the full boxes, zero-filled past the ends
+            for (uint32_t s = 0; s < steps; ++s) {
+                const uint32_t st = s % kGStages, ph = (s / kGStages) & 1u;
+                mbar_wait(&S.empty[st], ph ^ 1u, G.err, kDevTimeoutTmaEmpty);
+                mbar_arrive_expect_tx(&S.full[st], bytes);
+                const int32_t kx = int32_t(k0 + 64u * s);
+                tma_load_2d(S.a[st], &G.tmA, &S.full[st], kx, int32_t(m0));
+                tma_load_2d(S.b[st], &G.tmB, &S.full[st], kx, 0);
+            }
+        }
+    } else if (warp == 1) {
+        if (elect_one()) {
+            const uint32_t idesc = idesc_bf16_f32(128, int(G.N));
+            for (uint32_t s = 0; s < steps; ++s) {
+                const uint32_t st = s % kGStages, ph = (s / kGStages) & 1u;
+                mbar_wait(&S.full[st], ph, G.err, kDevTimeoutTmaFull);
+                tc_fence_after();
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk)  // K = 16 per UMMA: +32 bytes within the swizzled row
+                    umma_f16(tmem, umma_desc_k_sw128(smem_u32(S.a[st]) + 32u * kk),
+                             umma_desc_k_sw128(smem_u32(S.b[st]) + 32u * kk), idesc, (s | kk) != 0u ? 1u : 0u);
+                umma_commit(&S.empty[st]);
+            }
+            umma_commit(&S.done);
+        }
+    } else if (steps > 0) {
+        const uint32_t q = warp & 3u, m = m0 + 32u * q + lane;
+        mbar_wait(&S.done, 0, G.err, kDevTimeoutAccFull);
+        tc_fence_after();
+        for (uint32_t c0 = 0; c0 < G.N; c0 += 32u) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((32u * q) << 16) + c0, v);
+            tmem_wait_ld();
+            if (m >= G.M) continue;  // (after the warp-collective load)
+            float f[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) f[k] = __uint_as_float(v[k]);
+            if (G.epi == kEpiStoreF32) {
+                float4* o = reinterpret_cast<float4*>(G.outF + size_t(m) * G.ldF + c0);
+#pragma unroll
+                for (int k4 = 0; k4 < 8; ++k4) o[k4] = make_float4(f[4 * k4], f[4 * k4 + 1], f[4 * k4 + 2], f[4 * k4 + 3]);
+            } else if (G.epi == kEpiAtomicF32) {
+                float4* o = reinterpret_cast<float4*>(G.outF + size_t(m) * G.ldF + c0);
+#pragma unroll
+                for (int k4 = 0; k4 < 8; ++k4)
+                    atomicAdd(&o[k4], make_float4(f[4 * k4], f[4 * k4 + 1], f[4 * k4 + 2], f[4 * k4 + 3]));
+            } else {
+                uint16_t hb[32];
+                if (G.epi == kEpiBiasReluBf16) {
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) hb[k] = bf16_bits(fmaxf(f[k] + G.bias[c0 + k], 0.f));
+                    uint4* o = reinterpret_cast<uint4*>(G.outB + size_t(m) * G.ldB + c0);
+                    const uint32_t* w = reinterpret_cast<const uint32_t*>(hb);
+#pragma unroll
+                    for (int k4 = 0; k4 < 4; ++k4) o[k4] = make_uint4(w[4 * k4], w[4 * k4 + 1], w[4 * k4 + 2], w[4 * k4 + 3]);
+                } else {  // kEpiReluGrad
+                    const uint4* mk = reinterpret_cast<const uint4*>(G.mask + size_t(m) * G.ldMask + c0);
+                    uint16_t mb[32];
+#pragma unroll
+                    for (int k4 = 0; k4 < 4; ++k4) *reinterpret_cast<uint4*>(&mb[8 * k4]) = mk[k4];
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) {
+                        if (!(bf16_to_f(mb[k]) > 0.f)) f[k] = 0.f;
+                        hb[k] = bf16_bits(f[k]);
+                    }
+                    float4* o = reinterpret_cast<float4*>(G.outF + size_t(m) * G.ldF + c0);
+#pragma unroll
+                    for (int k4 = 0; k4 < 8; ++k4) o[k4] = make_float4(f[4 * k4], f[4 * k4 + 1], f[4 * k4 + 2], f[4 * k4 + 3]);
+                }
+                // transposed copy: per column, the warp's 32 consecutive rows (64 contiguous bytes)
+#pragma unroll
+                for (int k = 0; k < 32; ++k) G.outT[size_t(c0 + k) * G.ldT + m] = hb[k];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tmem_dealloc(tmem, 256);
+}
+
+// Gathered rows of the three descriptor sets (anchors | positives | negatives, B each) as
+// xb = bf16(x / 64) [R][128] and its transpose xT [128][ldT]. Block: 32 rows; thread (row,
+// 16-byte group).
+__global__ void gather_convert_kernel(const uint8_t* __restrict__ da, const uint32_t* __restrict__ ia,
+                                      const uint8_t* __restrict__ dp, const uint32_t* __restrict__ ip,
+                                      const uint8_t* __restrict__ dn, const uint32_t* __restrict__ in_, uint32_t B,
+                                      uint16_t* __restrict__ xb, uint16_t* __restrict__ xT, uint32_t ldT) {
+    const uint32_t r = blockIdx.x * 32u + (threadIdx.x & 31u), g = threadIdx.x >> 5;  // g: 16-byte group
+    if (r >= 3 * B) return;
+    const uint32_t set = r / B, b = r - set * B;
+    const uint8_t* src = set == 0 ? da + size_t(ia[b]) * 128 : set == 1 ? dp + size_t(ip[b]) * 128 : dn + size_t(in_[b]) * 128;
+    const uint4 raw = reinterpret_cast<const uint4*>(src)[g];
+    const uint8_t* v = reinterpret_cast<const uint8_t*>(&raw);
+    uint16_t o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) o[k] = bf16_bits(float(v[k]) * (1.f / 64));  // exact: x / 64 has <= 8 bits
+    uint4* dst = reinterpret_cast<uint4*>(xb + size_t(r) * 128 + 16 * g);
+    dst[0] = *reinterpret_cast<const uint4*>(&o[0]);
+    dst[1] = *reinterpret_cast<const uint4*>(&o[8]);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) xT[size_t(16 * g + k) * ldT + r] = o[k];
+}
+
+// out[c][r] = bf16(in[r][c]) for in f32 [rows][cols] (32 x 32 tiles through shared memory).
+__global__ void transpose_bf16_kernel(const float* __restrict__ in, uint32_t rows, uint32_t cols,
+                                      uint16_t* __restrict__ out, uint32_t ldOut) {
+    __shared__ float t[32][33];
+    const uint32_t r0 = blockIdx.y * 32u, c0 = blockIdx.x * 32u;
+    for (uint32_t y = threadIdx.y; y < 32u; y += blockDim.y) {
+        const uint32_t r = r0 + y, c = c0 + threadIdx.x;
+        t[y][threadIdx.x] = (r < rows && c < cols) ? in[size_t(r) * cols + c] : 0.f;
+    }
+    __syncthreads();
+    for (uint32_t y = threadIdx.y; y < 32u; y += blockDim.y) {
+        const uint32_t c = c0 + y, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) out[size_t(c) * ldOut + r] = bf16_bits(t[threadIdx.x][y]);
     }
 }
 
@@ -310,7 +428,8 @@ __global__ void bias_relu_kernel(float* __restrict__ hpre, const float* __restri
 //           (channels 8t..8t+7), -log(A_t(a,p) + 1e-6) + lambda * A_t(a,n) with
 //           A_t(u,v) = prod_k max((1 + z_u,k z_v,k) / 2, 1e-4).
 __global__ void triplet_kernel(const float* __restrict__ o, const float* __restrict__ b2, float* __restrict__ dO,
-                               uint32_t B, float margin, int kind, float lambda, float* __restrict__ lossSum) {
+                               uint16_t* __restrict__ dOb, uint32_t B, float margin, int kind, float lambda,
+                               float* __restrict__ lossSum) {
     const uint32_t b = blockIdx.x;
     const uint32_t c = threadIdx.x;
     __shared__ float red[2][4];
@@ -353,26 +472,26 @@ __global__ void triplet_kernel(const float* __restrict__ o, const float* __restr
             if ((c & 7u) == 0) lossKey = -logf(aap + 1e-6f) + lambda * aan;
         }
     }
-    dO[size_t(b) * 128 + c] = ga * inv * (1.f - za * za);
-    dO[size_t(B + b) * 128 + c] = gp * inv * (1.f - zp * zp);
-    dO[size_t(2 * B + b) * 128 + c] = gn * inv * (1.f - zn * zn);
+    const float oa = ga * inv * (1.f - za * za), op = gp * inv * (1.f - zp * zp), on = gn * inv * (1.f - zn * zn);
+    dO[size_t(b) * 128 + c] = oa;
+    dO[size_t(B + b) * 128 + c] = op;
+    dO[size_t(2 * B + b) * 128 + c] = on;
+    dOb[size_t(b) * 128 + c] = bf16_bits(oa);  // the bf16 operand of the gradient GEMM dh = dO W2
+    dOb[size_t(B + b) * 128 + c] = bf16_bits(op);
+    dOb[size_t(2 * B + b) * 128 + c] = bf16_bits(on);
     if (lossKey != 0.f) atomicAdd(lossSum, lossKey * inv);
     if (c == 0 && active) atomicAdd(lossSum, l * inv);
 }
 
-// dh *= [hpre > 0]
-__global__ void relu_grad_kernel(float* __restrict__ dh, const float* __restrict__ hpre, size_t total) {
-    for (size_t x = blockIdx.x * size_t(blockDim.x) + threadIdx.x; x < total; x += size_t(gridDim.x) * blockDim.x)
-        if (!(hpre[x] > 0.f)) dh[x] = 0.f;
-}
-
-// column sums: out[c] = sum_r in[r][c]
+// column sums: out[c] += sum_r in[r][c] (out zeroed beforehand); block = one thread per column,
+// kColRows rows per block, one atomic per column per block.
+constexpr uint32_t kColRows = 128;
 __global__ void colsum_kernel(const float* __restrict__ in, uint32_t rows, uint32_t cols, float* __restrict__ out) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+    const uint32_t c = threadIdx.x;
+    const uint32_t r0 = blockIdx.x * kColRows, r1 = min(rows, r0 + kColRows);
     float s = 0.f;
-    for (uint32_t r = 0; r < rows; ++r) s += in[size_t(r) * cols + c];
-    out[c] = s;
+    for (uint32_t r = r0; r < r1; ++r) s += in[size_t(r) * cols + c];
+    atomicAdd(&out[c], s);
 }
 
 // Adam on fp32 masters; writes the bf16 copy when `bf` is non-null.
@@ -402,27 +521,33 @@ __global__ void f32_to_bf16_kernel(const float* __restrict__ in, uint16_t* __res
     }
 }
 
-// gathers rows of three u8 descriptor sets into one [3B][128] buffer (anchors | positives | negatives)
-__global__ void gather_kernel(const uint8_t* __restrict__ da, const uint32_t* __restrict__ ia,
-                              const uint8_t* __restrict__ dp, const uint32_t* __restrict__ ip,
-                              const uint8_t* __restrict__ dn, const uint32_t* __restrict__ in_, uint32_t B,
-                              uint8_t* __restrict__ x) {
-    const uint32_t r = blockIdx.x;  // 0..3B-1, 8 threads x 16 bytes
-    const uint32_t part = threadIdx.x;
-    const uint32_t set = r / B, b = r % B;
-    const uint8_t* src = set == 0 ? da + size_t(ia[b]) * 128 : set == 1 ? dp + size_t(ip[b]) * 128 : dn + size_t(in_[b]) * 128;
-    reinterpret_cast<uint4*>(x + size_t(r) * 128)[part] = reinterpret_cast<const uint4*>(src)[part];
-}
-
-static int gemm(cudaStream_t s, int M, int N, int K, const void* A, int ta, long sam, long sak, const void* B, int tb,
-                long sbk, long sbn, float* C, long scm, long scn, float alpha, int splits) {
-    const int kPer = ((K + splits - 1) / splits + kTK - 1) / kTK * kTK;
-    const int z = (K + kPer - 1) / kPer;
-    dim3 g((N + kTN - 1) / kTN, (M + kTM - 1) / kTM, z);
-    gemm_kernel<<<g, 256, 0, s>>>(M, N, K, A, ta, sam, sak, B, tb, sbk, sbn, C, scm, scn, alpha, z > 1, kPer);
+static int gemm_tc(cudaStream_t s, const GemmArgs& G) {
+    const size_t smem = sizeof(GemmSmem) + 1024;
+    const int sa = set_max_dynamic_smem(reinterpret_cast<const void*>(gemm_tc_kernel), smem);
+    if (sa != RSFM_OK) return sa;
+    const dim3 grid((G.M + 127u) / 128u, (G.K + G.kPerCta - 1u) / G.kPerCta);
+    gemm_tc_kernel<<<grid, kGThreads, smem, s>>>(G);
     RSFM_CUDA_TRY(cudaGetLastError());
     launch_count_add(1);
     return RSFM_OK;
+}
+
+// The arguments of one trainer GEMM: A [M][K] (pitch lda) and B [N][K] (pitch ldb), bf16,
+// K-major; split-K with K ranges of kPerCta (a multiple of 64).
+static int gemm_args(GemmArgs* G, const uint16_t* A, uint32_t lda, const uint16_t* B, uint32_t ldb, uint32_t M,
+                     uint32_t N, uint32_t K, uint32_t kPerCta, int epi) {
+    memset(G, 0, sizeof(*G));
+    int st = encode_bf16_tmap(&G->tmA, A, M, K, lda, 128);
+    if (st != RSFM_OK) return st;
+    st = encode_bf16_tmap(&G->tmB, B, N, K, ldb, N);
+    if (st != RSFM_OK) return st;
+    G->M = M;
+    G->N = N;
+    G->K = K;
+    G->kPerCta = kPerCta;
+    G->epi = epi;
+    G->err = device_error_word();
+    return G->err ? RSFM_OK : RSFM_ERR_CUDA;
 }
 
 }  // namespace mlp
@@ -432,6 +557,7 @@ using namespace rsfm_b200;
 
 struct rsfm_mlp_trainer {
     uint32_t batch = 0;
+    uint32_t ldR = 0;  // row pitch (elements) of the transposed activations: 3 * batch rounded up to 8
     float margin = 16.f, lr = 1e-3f;
     int kind = 0;        // loss: 0 = triplet hinge, 1 = bucket-key loss + hinge on the code channels
     float lambda = 0.f;  // weight of the negatives' key agreement (kind 1)
@@ -439,11 +565,15 @@ struct rsfm_mlp_trainer {
     rsfm_mlp model{};
     // fp32 masters, Adam moments, gradients
     float *w1 = nullptr, *w2 = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;
-    // activations for 3B rows
-    uint8_t* x = nullptr;
-    float *hpre = nullptr, *o = nullptr, *dO = nullptr, *dh = nullptr, *loss = nullptr;
-    uint16_t* h = nullptr;
+    // activations for R = 3 * batch rows (anchors | positives | negatives); "T": transposed copies,
+    // [columns][ldR], the K-major operands of the weight-gradient GEMMs
+    uint16_t *xb = nullptr, *xT = nullptr;         // bf16 x / 64
+    uint16_t *h = nullptr, *hT = nullptr;          // bf16 relu(x W1^T + b1) [R][256]
+    float *o = nullptr, *dO = nullptr, *dh = nullptr, *loss = nullptr;
+    uint16_t *dOb = nullptr, *dOT = nullptr, *dhT = nullptr;
     uint16_t *bw1 = nullptr, *bw2 = nullptr;  // bf16 copies the hash kernel reads
+    uint16_t* w2T = nullptr;                  // bf16 W2^T [256][128] (the B operand of dh = dO W2)
+    mlp::GemmArgs gemm[5];                    // h, o, dh, dW2, dW1
 };
 
 // parameter block layout (floats): w1 [32768] | b1 [256] | w2 [32768] | b2 [128]
@@ -478,19 +608,24 @@ extern "C" int rsfm_mlp_hash(const rsfm_mlp* m, const void* desc, uint32_t nbDes
 
 extern "C" int rsfm_mlp_trainer_create(const float* initParams, uint32_t batch, float lr, float margin,
                                        rsfm_mlp_trainer** out) {
-    if (!initParams || !out || batch == 0) return RSFM_ERR_INVALID_ARG;
+    if (!initParams || !out || batch == 0 || batch > (1u << 24)) return RSFM_ERR_INVALID_ARG;
     auto* t = new rsfm_mlp_trainer();
     t->batch = batch;
     t->lr = lr;
     t->margin = margin;
     const size_t R = size_t(3) * batch;
+    t->ldR = uint32_t((R + 7) & ~size_t(7));
+    const size_t L = t->ldR;
     bool ok = cudaMalloc(&t->w1, kNP * 4) == cudaSuccess && cudaMalloc(&t->g, kNP * 4) == cudaSuccess &&
               cudaMalloc(&t->m1, kNP * 4) == cudaSuccess && cudaMalloc(&t->m2, kNP * 4) == cudaSuccess &&
-              cudaMalloc(&t->x, R * 128) == cudaSuccess && cudaMalloc(&t->hpre, R * 256 * 4) == cudaSuccess &&
-              cudaMalloc(&t->h, R * 256 * 2) == cudaSuccess && cudaMalloc(&t->o, R * 128 * 4) == cudaSuccess &&
-              cudaMalloc(&t->dO, R * 128 * 4) == cudaSuccess && cudaMalloc(&t->dh, R * 256 * 4) == cudaSuccess &&
-              cudaMalloc(&t->loss, 4) == cudaSuccess;
-    ok = ok && cudaMalloc(&t->bw1, kNW1 * 2) == cudaSuccess && cudaMalloc(&t->bw2, kNW2 * 2) == cudaSuccess;
+              cudaMalloc(&t->xb, R * 128 * 2) == cudaSuccess &&
+              cudaMalloc(&t->xT, 128 * L * 2) == cudaSuccess && cudaMalloc(&t->h, R * 256 * 2) == cudaSuccess &&
+              cudaMalloc(&t->hT, 256 * L * 2) == cudaSuccess && cudaMalloc(&t->o, R * 128 * 4) == cudaSuccess &&
+              cudaMalloc(&t->dO, R * 128 * 4) == cudaSuccess && cudaMalloc(&t->dOb, R * 128 * 2) == cudaSuccess &&
+              cudaMalloc(&t->dOT, 128 * L * 2) == cudaSuccess && cudaMalloc(&t->dh, R * 256 * 4) == cudaSuccess &&
+              cudaMalloc(&t->dhT, 256 * L * 2) == cudaSuccess && cudaMalloc(&t->loss, 4) == cudaSuccess &&
+              cudaMalloc(&t->bw1, kNW1 * 2) == cudaSuccess && cudaMalloc(&t->bw2, kNW2 * 2) == cudaSuccess &&
+              cudaMalloc(&t->w2T, kNW2 * 2) == cudaSuccess;
     if (!ok) {
         rsfm_mlp_trainer_destroy(t);
         return RSFM_ERR_CUDA;
@@ -507,9 +642,52 @@ extern "C" int rsfm_mlp_trainer_create(const float* initParams, uint32_t batch, 
     }
     mlp::f32_to_bf16_kernel<<<(kNW1 + 255) / 256, 256>>>(t->w1, t->bw1, kNW1);
     mlp::f32_to_bf16_kernel<<<(kNW2 + 255) / 256, 256>>>(t->w2, t->bw2, kNW2);
+    mlp::transpose_bf16_kernel<<<dim3(256 / 32, 128 / 32), dim3(32, 8)>>>(t->w2, 128, 256, t->w2T, 128);
     if (cudaDeviceSynchronize() != cudaSuccess) {
         rsfm_mlp_trainer_destroy(t);
         return RSFM_ERR_CUDA;
+    }
+    // The five GEMMs (buffers are fixed, so their tensor maps are encoded once). Split-K for the
+    // weight gradients (K = R): about 32 K ranges of a multiple of 64 rows.
+    using namespace mlp;
+    const uint32_t Ru = uint32_t(R);
+    const uint32_t kSplit = std::max<uint32_t>(64u, ((Ru + 31u) / 32u + 63u) / 64u * 64u);
+    GemmArgs* G = t->gemm;
+    int st = gemm_args(&G[0], t->xb, 128, t->bw1, 128, Ru, 256, 128, 128, kEpiBiasReluBf16);  // h = relu(x W1^T + b1)
+    if (st == RSFM_OK) {
+        G[0].bias = t->model.b1;
+        G[0].outB = t->h;
+        G[0].ldB = 256;
+        G[0].outT = t->hT;
+        G[0].ldT = t->ldR;
+        st = gemm_args(&G[1], t->h, 256, t->bw2, 256, Ru, 128, 256, 256, kEpiStoreF32);  // o = h W2^T
+    }
+    if (st == RSFM_OK) {
+        G[1].outF = t->o;
+        G[1].ldF = 128;
+        st = gemm_args(&G[2], t->dOb, 128, t->w2T, 128, Ru, 256, 128, 128, kEpiReluGrad);  // dh = (dO W2) [h > 0]
+    }
+    if (st == RSFM_OK) {
+        G[2].mask = t->h;
+        G[2].ldMask = 256;
+        G[2].outF = t->dh;
+        G[2].ldF = 256;
+        G[2].outT = t->dhT;
+        G[2].ldT = t->ldR;
+        st = gemm_args(&G[3], t->dOT, t->ldR, t->hT, t->ldR, 128, 256, Ru, kSplit, kEpiAtomicF32);  // dW2 = dO^T h
+    }
+    if (st == RSFM_OK) {
+        G[3].outF = t->g + kNW1 + kNB1;
+        G[3].ldF = 256;
+        st = gemm_args(&G[4], t->dhT, t->ldR, t->xT, t->ldR, 256, 128, Ru, kSplit, kEpiAtomicF32);  // dW1 = dh^T x
+    }
+    if (st == RSFM_OK) {
+        G[4].outF = t->g;
+        G[4].ldF = 128;
+    }
+    if (st != RSFM_OK) {
+        rsfm_mlp_trainer_destroy(t);
+        return st;
     }
     *out = t;
     return RSFM_OK;
@@ -528,42 +706,38 @@ extern "C" int rsfm_mlp_trainer_model(const rsfm_mlp_trainer* t, rsfm_mlp* model
     return RSFM_OK;
 }
 
-// Forward + backward on one triplet batch; gradients land in the trainer's gradient block.
+// Forward + backward on one triplet batch; gradients land in the trainer's gradient block. All five
+// contractions run on the tensor cores (gemm_tc_kernel); bias + ReLU and the ReLU derivative are
+// fused into their epilogues.
 static int trainer_grads(rsfm_mlp_trainer* t, const void* a, const uint32_t* ia, const void* p, const uint32_t* ip,
                          const void* ng, const uint32_t* in_, cudaStream_t s) {
     using namespace mlp;
     const uint32_t B = t->batch;
-    const int R = int(3 * B);
-    gather_kernel<<<R, 8, 0, s>>>(static_cast<const uint8_t*>(a), ia, static_cast<const uint8_t*>(p), ip,
-                                  static_cast<const uint8_t*>(ng), in_, B, t->x);
+    const uint32_t R = 3 * B;
+    gather_convert_kernel<<<(R + 31) / 32, 256, 0, s>>>(static_cast<const uint8_t*>(a), ia,
+                                                        static_cast<const uint8_t*>(p), ip,
+                                                        static_cast<const uint8_t*>(ng), in_, B, t->xb, t->xT,
+                                                        t->ldR);
     RSFM_CUDA_TRY(cudaGetLastError());
     RSFM_CUDA_TRY(cudaMemsetAsync(t->g, 0, kNP * 4, s));
     RSFM_CUDA_TRY(cudaMemsetAsync(t->loss, 0, 4, s));
-    // hpre = x W1^T / 64 ; + b1 ; h = bf16(relu)
-    int st = gemm(s, R, 256, 128, t->x, kU8, 128, 1, t->model.w1, kBF16, 1, 128, t->hpre, 256, 1, 1.f / 64, 1);
-    if (st) return st;
-    bias_relu_kernel<<<1024, 256, 0, s>>>(t->hpre, t->model.b1, t->h, size_t(R) * 256);
-    // o = h W2^T
-    st = gemm(s, R, 128, 256, t->h, kBF16, 256, 1, t->model.w2, kBF16, 1, 256, t->o, 128, 1, 1.f, 1);
-    if (st) return st;
-    triplet_kernel<<<B, 128, 0, s>>>(t->o, t->model.b2, t->dO, B, t->margin, t->kind, t->lambda, t->loss);
-    // dW2 = dO^T h ; db2 = sum dO
-    float* gW1 = t->g;
     float* gB1 = t->g + kNW1;
-    float* gW2 = gB1 + kNB1;
-    float* gB2 = gW2 + kNW2;
-    st = gemm(s, 128, 256, R, t->dO, kF32, 1, 128, t->h, kBF16, 256, 1, gW2, 256, 1, 1.f, 64);
-    if (st) return st;
-    colsum_kernel<<<1, 128, 0, s>>>(t->dO, R, 128, gB2);
-    // dh = dO W2 * [hpre > 0] ; db1 = sum dh ; dW1 = dh^T x / 64
-    st = gemm(s, R, 256, 128, t->dO, kF32, 128, 1, t->model.w2, kBF16, 256, 1, t->dh, 256, 1, 1.f, 1);
-    if (st) return st;
-    relu_grad_kernel<<<1024, 256, 0, s>>>(t->dh, t->hpre, size_t(R) * 256);
-    colsum_kernel<<<1, 256, 0, s>>>(t->dh, R, 256, gB1);
-    st = gemm(s, 256, 128, R, t->dh, kF32, 1, 256, t->x, kU8, 128, 1, gW1, 128, 1, 1.f / 64, 64);
-    if (st) return st;
+    float* gB2 = t->g + kNW1 + kNB1 + kNW2;
+    int st = gemm_tc(s, t->gemm[0]);  // h, h^T = bf16(relu(x W1^T + b1))
+    if (st == RSFM_OK) st = gemm_tc(s, t->gemm[1]);  // o = h W2^T
+    if (st != RSFM_OK) return st;
+    triplet_kernel<<<B, 128, 0, s>>>(t->o, t->model.b2, t->dO, t->dOb, B, t->margin, t->kind, t->lambda, t->loss);
+    transpose_bf16_kernel<<<dim3(128 / 32, (R + 31) / 32), dim3(32, 8), 0, s>>>(t->dO, R, 128, t->dOT, t->ldR);
+    colsum_kernel<<<(R + kColRows - 1) / kColRows, 128, 0, s>>>(t->dO, R, 128, gB2);  // db2 = sum dO
     RSFM_CUDA_TRY(cudaGetLastError());
-    launch_count_add(6);
+    st = gemm_tc(s, t->gemm[2]);  // dh, dh^T = (dO W2) [h > 0]
+    if (st != RSFM_OK) return st;
+    colsum_kernel<<<(R + kColRows - 1) / kColRows, 256, 0, s>>>(t->dh, R, 256, gB1);  // db1 = sum dh
+    RSFM_CUDA_TRY(cudaGetLastError());
+    st = gemm_tc(s, t->gemm[3]);  // dW2 += dO^T h (split-K)
+    if (st == RSFM_OK) st = gemm_tc(s, t->gemm[4]);  // dW1 += dh^T (x / 64) (split-K)
+    if (st != RSFM_OK) return st;
+    launch_count_add(5);
     return RSFM_OK;
 }
 
@@ -599,8 +773,9 @@ extern "C" int rsfm_mlp_trainer_step(rsfm_mlp_trainer* t, const void* a, const u
                                                        t->bw2, kNW2, t->lr, b1c, b2c);
     const size_t o3 = o2 + kNW2;
     adam_kernel<<<1, 128, 0, stream>>>(t->w1 + o3, t->g + o3, t->m1 + o3, t->m2 + o3, nullptr, kNB2, t->lr, b1c, b2c);
+    transpose_bf16_kernel<<<dim3(256 / 32, 128 / 32), dim3(32, 8), 0, stream>>>(t->w2, 128, 256, t->w2T, 128);
     RSFM_CUDA_TRY(cudaGetLastError());
-    launch_count_add(4);
+    launch_count_add(5);
     if (lossDevice) RSFM_CUDA_TRY(cudaMemcpyAsync(lossDevice, t->loss, 4, cudaMemcpyDeviceToDevice, stream));
     return RSFM_OK;
 }
@@ -614,10 +789,12 @@ extern "C" int rsfm_mlp_trainer_params(const rsfm_mlp_trainer* t, float* paramsH
 extern "C" int rsfm_mlp_trainer_destroy(rsfm_mlp_trainer* t) {
     if (!t) return RSFM_OK;
     for (void* p : {static_cast<void*>(t->w1), static_cast<void*>(t->g), static_cast<void*>(t->m1),
-                    static_cast<void*>(t->m2), static_cast<void*>(t->x), static_cast<void*>(t->hpre),
-                    static_cast<void*>(t->h), static_cast<void*>(t->o), static_cast<void*>(t->dO),
-                    static_cast<void*>(t->dh), static_cast<void*>(t->loss), static_cast<void*>(t->bw1),
-                    static_cast<void*>(t->bw2)})
+                    static_cast<void*>(t->m2), static_cast<void*>(t->xb),
+                    static_cast<void*>(t->xT), static_cast<void*>(t->h), static_cast<void*>(t->hT),
+                    static_cast<void*>(t->o), static_cast<void*>(t->dO), static_cast<void*>(t->dOb),
+                    static_cast<void*>(t->dOT), static_cast<void*>(t->dh), static_cast<void*>(t->dhT),
+                    static_cast<void*>(t->loss), static_cast<void*>(t->bw1), static_cast<void*>(t->bw2),
+                    static_cast<void*>(t->w2T)})
         if (p) cudaFree(p);
     delete t;
     return RSFM_OK;

@@ -161,11 +161,14 @@ def default_params_path():
 
 
 def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3, margin=48.0, seed=0,
-                           device="cuda", log=None, loss="triplet", lam=16.0):
+                           device="cuda", log=None, loss="triplet", lam=16.0, timings=None):
     """Trains the learned hash on correspondences the brute-force matcher produces (ratio test and
     cross-check passed) on `n_pairs` seeded synthetic pairs (40% overlap, noise 8); negatives are
-    random train descriptors of the same pair. Returns the f32 parameter block."""
+    random train descriptors of the same pair. Returns the f32 parameter block. `timings` (a dict)
+    receives the wall time of the mining and of the training loop."""
+    import time
     from . import synth
+    t0 = time.perf_counter()
     g = torch.Generator(device=device)
     g.manual_seed(seed + 12345)
     qs, ts, A, P = [], [], [], []
@@ -180,6 +183,8 @@ def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3
     A, P = torch.cat(A), torch.cat(P)
     params = center_output_bias(init_params(seed), lambda p: LearnedHash(p, device=device), Q[:20000])
     tr = Trainer(params, batch, lr=lr, margin=margin, loss=loss, lam=lam)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
     for s in range(steps):
         sel = torch.randint(0, len(A), (batch,), device=device, generator=g)
         ip = P[sel].int()
@@ -189,6 +194,12 @@ def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3
             log(f"step {s} loss {tr.loss.item():.4f}")
     out = tr.params()
     tr.close()
+    if timings is not None:
+        timings["mining_s"] = t1 - t0
+        timings["training_loop_s"] = time.perf_counter() - t1
+        timings["steps"] = steps
+        timings["batch"] = batch
+        timings["correspondences"] = int(len(A))
     return out
 
 
