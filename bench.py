@@ -780,7 +780,17 @@ def run_hash(dev, stream, n=1 << 24):
     out = {"n_desc": n}
     ms = _events_ms(hash_call, 5, stream)
     gbs = n * (128 + 8 + 16) / (ms * 1e-3) / 1e9
-    out["cashash_hash"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None}
+    out["cashash_hash"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None,
+                           "channels": 192}
+
+    def hash64_call():  # computeHashForBucketOnly: the 64 key channels, what the matcher registers
+        lib.rsfm_cashash_compute_hash(p(cas.w), p(cas.bias), 64, p(desc), n, p(keys), None, p(hist),
+                                      ctypes.c_void_p(stream.cuda_stream))
+
+    ms = _events_ms(hash64_call, 5, stream)
+    gbs = n * (128 + 8) / (ms * 1e-3) / 1e9
+    out["cashash_hash_keys_only"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None,
+                                     "channels": 64}
     ms = _events_ms(acc_call, 5, stream)
     gbs = n * 128 / (ms * 1e-3) / 1e9
     out["cashash_accumulate"] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": gbs / hbm if hbm else None}

@@ -77,10 +77,14 @@ __global__ void bias_kernel(int32_t* __restrict__ bias, const int8_t* __restrict
 //   warp 0      TMA producer: raw descriptor tiles into a kHashStages-deep ring
 //   warps 2-5   halve every byte in place ((x & 0xFE) >> 1 fits int8, the reference's transform)
 //   warp 1      TMEM owner and UMMA issuer: s8 x s8 UMMAs (M=128, N=channels, K=128) against the
-//               weights (loaded once) into one of two TMEM accumulators; its commit also frees
-//               the descriptor stage
+//               weights (loaded once) into one of two TMEM accumulators, plus one K = 32 UMMA that
+//               adds the biases (below); its commit also frees the descriptor stage
 //   warps 6-29  epilogue: six warps per TMEM lane quarter, one per 32-channel group, read the
-//               channel sums, add the bias and pack the sign bits
+//               biased channel sums and pack their sign bits
+// The biases enter through the tensor cores: a constant 128-row operand whose every 16-byte chunk
+// is [1, 127 x 15] times per-channel digits d (s8) with sum_k a_k d_k = bias, i.e. d_0 + 127 Q
+// for the 30 digits of weight 127 summing to Q. That covers |bias| <= 127 * 3810 + 127; a channel
+// beyond it keeps the rest as a residual that the epilogue adds (a CTA-uniform slow path).
 // so the HBM stream, the halving, the MMA and the sign packing of different tiles overlap.
 constexpr int kHashStages = 8;
 constexpr int kHashHalvers = 4;
@@ -89,7 +93,10 @@ constexpr int kHashThreads = 32 * (2 + kHashHalvers + kHashEpi);
 struct HashSmem {
     uint8_t desc[kHashStages][128 * 128];
     uint8_t w[192 * 128];
-    int32_t bias[192];
+    uint8_t aOnes[128 * 128];  // bias operand A: every 16-byte chunk [1, 127 x 15]
+    uint8_t wBias[192 * 128];  // bias operand B: row c = channel c's digits in K 0..31 (128-byte swizzle)
+    int32_t bias[192];         // residual beyond the digits' range (usually zero)
+    uint32_t anyResidual;
     uint32_t hist[8][256];
     uint64_t full[kHashStages], halved[kHashStages], empty[kHashStages];
     uint64_t accFull[2], accEmpty[2];
@@ -110,7 +117,38 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t tiles = (n + 127) / 128;
     for (uint32_t x = tid; x < 8 * 256; x += kHashThreads) (&S.hist[0][0])[x] = 0;
-    for (int c = tid; c < channels; c += kHashThreads) S.bias[c] = bias[c];
+    // bias operands: A' constant, B' digits (row c, logical bytes 0..31 at the swizzled 16-byte
+    // positions of chunks 0 and 1, the rest zero), and the residual per channel
+    if (tid == 0) S.anyResidual = 0;
+    for (uint32_t x = tid; x < 128u * 128u / 16u; x += kHashThreads)
+        reinterpret_cast<uint4*>(S.aOnes)[x] = make_uint4(0x7F7F7F01u, 0x7F7F7F7Fu, 0x7F7F7F7Fu, 0x7F7F7F7Fu);
+    for (uint32_t x = tid; x < 192u * 128u / 16u; x += kHashThreads)
+        reinterpret_cast<uint4*>(S.wBias)[x] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    for (int c = tid; c < channels; c += kHashThreads) {
+        const int32_t b = bias[c];
+        const int32_t kQmax = 30 * 127;
+        int32_t Q = (b >= 0 ? b + 63 : b - 63) / 127;  // nearest multiple of 127
+        Q = max(-kQmax, min(kQmax, Q));
+        const int32_t d0 = max(-127, min(127, b - 127 * Q));
+        S.bias[c] = b - (d0 + 127 * Q);
+        if (S.bias[c] != 0) atomicOr(&S.anyResidual, 1u);
+        int8_t dg[32] = {};
+        dg[0] = int8_t(d0);  // weight 1 (dg[16], the other weight-1 slot, stays 0)
+        int32_t rest = Q;
+        for (int k = 1; k < 32; ++k) {
+            if (k == 16) continue;
+            const int32_t v = max(-127, min(127, rest));
+            dg[k] = int8_t(v);
+            rest -= v;
+        }
+        const uint32_t r = uint32_t(c);
+        for (uint32_t ch = 0; ch < 2; ++ch) {
+            const uint32_t off = (r >> 3) * 1024u + (r & 7u) * 128u + (((ch ^ r) & 7u) << 4);
+            *reinterpret_cast<uint4*>(S.wBias + off) = *reinterpret_cast<const uint4*>(&dg[16 * ch]);
+        }
+    }
+    fence_proxy_async_smem();  // generic writes, read by the UMMA (async proxy)
     if (tid == 0) {
         for (int b = 0; b < kHashStages; ++b) {
             mbar_init(&S.full[b], 1);
@@ -161,6 +199,9 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
 #pragma unroll
                 for (uint32_t kk = 0; kk < 4; ++kk)
                     umma_i8(tmem + 256u * b, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(bw + 32u * kk), idesc, kk);
+                // + bias (K = 32: the constant operand times the digits)
+                umma_i8(tmem + 256u * b, umma_desc_k_sw128(smem_u32(S.aOnes)), umma_desc_k_sw128(smem_u32(S.wBias)), idesc,
+                        1u);
                 umma_commit(&S.empty[st]);
                 umma_commit(&S.accFull[b]);
             }
@@ -191,6 +232,7 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
         const uint32_t e = warp - (2 + kHashHalvers);
         const uint32_t q = warp & 3u;
         const int cw = int(e >> 2);
+        const bool residual = S.anyResidual != 0;
         uint32_t k = 0;
         for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
             const uint32_t b = k & 1u;
@@ -201,17 +243,22 @@ hash_kernel(const __grid_constant__ CUtensorMap tmDesc, const __grid_constant__ 
                 uint32_t v[32];
                 tmem_ld32(tmem + 256u * b + ((32u * q) << 16) + 32u * cw, v);
                 tmem_wait_ld();
-                // sign bits of (sum + bias), shifted in from the top channel down: one funnel shift
-                // per channel; bit k = [sum_k + bias_k >= 0] after the final inversion
+                // sign bits of (bias + sum), shifted in from the top channel down: one funnel shift
+                // per channel; bit k = [bias_k + sum_k >= 0] after the final inversion
                 uint32_t neg = 0;
-                const int4* b4 = reinterpret_cast<const int4*>(&S.bias[32 * cw]);
+                if (residual) {  // some channel's bias is beyond the digits' range: add the rest
+                    const int4* b4 = reinterpret_cast<const int4*>(&S.bias[32 * cw]);
 #pragma unroll
-                for (int k4 = 7; k4 >= 0; --k4) {
-                    const int4 bb = b4[k4];
-                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 3]) + bb.w), neg, 1);
-                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 2]) + bb.z), neg, 1);
-                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 1]) + bb.y), neg, 1);
-                    neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 0]) + bb.x), neg, 1);
+                    for (int k4 = 7; k4 >= 0; --k4) {
+                        const int4 bb = b4[k4];
+                        neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 3]) + bb.w), neg, 1);
+                        neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 2]) + bb.z), neg, 1);
+                        neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 1]) + bb.y), neg, 1);
+                        neg = __funnelshift_l(uint32_t(int32_t(v[4 * k4 + 0]) + bb.x), neg, 1);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 31; k >= 0; --k) neg = __funnelshift_l(v[k], neg, 1);
                 }
                 const uint32_t bits = ~neg;
                 if (i < n) {

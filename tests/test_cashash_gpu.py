@@ -85,6 +85,24 @@ def test_matcher_weights_hash(rsfm, oracle):
     np.testing.assert_array_equal(keys, ek)
 
 
+@pytest.mark.parametrize("channels", [64, 192])
+def test_hash_large_biases(rsfm, oracle, channels):
+    """Biases beyond what the kernel's bias operand represents (|bias| > 127 * 3811) next to
+    ordinary ones: the rest is added in the epilogue, keys and codes stay exact."""
+    rng = np.random.default_rng(channels)
+    w = rng.integers(-128, 128, (channels, 128), dtype=np.int8)
+    b = rng.integers(-60000, 60000, channels).astype(np.int32)
+    b[::7] = rng.integers(-2_000_000, 2_000_000, len(b[::7]))
+    b[1] = 484_000
+    b[2] = -484_100
+    d = synth.uniform_bytes(3000, 9)
+    keys, remap, hist = _ours_hash(rsfm, w, b, d)
+    ek, er = oracle.cashash_hash(w, b, d)
+    np.testing.assert_array_equal(keys, ek)
+    if channels == 192:
+        np.testing.assert_array_equal(remap, er)
+
+
 def test_accumulate_and_bias(rsfm, oracle, ref):
     lib = rsfm._lib.load()
     a = synth.uniform_bytes(2000, 1)
