@@ -676,10 +676,14 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
             # pair sharing a bucket, per-scheme bucket lists; one call per pair
             fbm = lambda: [ch.find_best_match([qi], ti, stream=stream) for qi, ti in ranked]
             ms_calls = _events_ms(fbm, 2, stream)
-            # all pairs in one launch (rsfm_cashash_find_best_match_pairs)
+            # all pairs in one call (rsfm_cashash_find_best_match_pairs: builds its work list, one
+            # host synchronization per call) and as a batch built once (rsfm_cashash_fbm_batch_*:
+            # each launch = result init + the matching kernel, no synchronization)
             fbp = lambda: ch.find_best_match_pairs(ranked, stream=stream)
-            ms = _events_ms(fbp, 3, stream)
-            res = fbp()
+            ms_call = _events_ms(fbp, 3, stream)
+            fbb = ch.FindBestMatchBatch(ranked, stream=stream)
+            ms = _events_ms(lambda: fbb.launch(stream), 3, stream)
+            res = fbb.results
             hit = torch.zeros((), dtype=torch.int64, device=dev)
             tot = torch.zeros((), dtype=torch.int64, device=dev)
             rep = torch.zeros((), dtype=torch.int64, device=dev)
@@ -696,8 +700,10 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
                 r = valid & back
                 rep += r.sum()
                 tp += (r & same & ok).sum()
+            fbb.close()
             out["find_best_match_8_schemes"] = {"ms": ms, "recall": int(hit) / max(1, int(tot)),
                                                 "precision": int(tp) / max(1, int(rep)), "reported": int(rep),
+                                                "one_call_all_pairs_ms": ms_call,
                                                 "desc_pairs_per_s": pairs / (ms * 1e-3),
                                                 "one_call_per_pair_ms": ms_calls}
     # registration blobs (the reference's preCompForMatch layout, cascade-hash flags: norms, bias

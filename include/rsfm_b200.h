@@ -319,6 +319,18 @@ typedef struct rsfm_cashash_pair {
 int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
                                        cudaStream_t stream);
 
+/* The same matching for a batch of pairs that is matched repeatedly (no reference counterpart):
+ * _create builds the work list once (it synchronizes `stream` once, to size the list; the images
+ * and result arrays the pairs point to must stay valid while the batch is used); each _launch
+ * re-initialises the results and runs the matching kernel asynchronously on `stream`, with no
+ * allocation and no host synchronization, so it can be captured in a CUDA graph. Launches of one
+ * batch that overlap on the GPU write the same result arrays: order them on one stream. */
+typedef struct rsfm_cashash_fbm_batch rsfm_cashash_fbm_batch;
+int rsfm_cashash_fbm_batch_create(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
+                                  cudaStream_t stream, rsfm_cashash_fbm_batch** out);
+int rsfm_cashash_fbm_batch_launch(const rsfm_cashash_fbm_batch* batch, cudaStream_t stream);
+int rsfm_cashash_fbm_batch_destroy(rsfm_cashash_fbm_batch* batch);
+
 /* Image for ranked cascade-hash matching (no reference counterpart): keys = 8 bucket-key bytes
  * per descriptor and codes = the 128-bit remap code (rsfm_cashash_compute_hash with 192
  * channels, or the learned hash), bucket lists per scheme at buckets[s * nbDesc + lower(s, b)]

@@ -196,6 +196,10 @@ SIGNATURES = {
     "rsfm_cashash_reference_weights": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_pairs": (ctypes.c_int, [ctypes.POINTER(CasHashPair), ctypes.c_uint32,
                                                           ctypes.c_uint32, ctypes.c_void_p]),
+    "rsfm_cashash_fbm_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                                     ctypes.c_void_p]),
+    "rsfm_cashash_fbm_batch_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_cashash_fbm_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_cashash_find_best_match_ex": (ctypes.c_int, [ctypes.POINTER(CasHashImage), ctypes.c_void_p,
                                                        ctypes.POINTER(CasHashImage), ctypes.c_uint32,
                                                        ctypes.POINTER(CasHashResult), ctypes.c_uint32, ctypes.c_uint32,

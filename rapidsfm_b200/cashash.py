@@ -352,6 +352,49 @@ def find_best_match_pairs(pairs, per_scheme_lists=True, stream=None):
     return outs
 
 
+class FindBestMatchBatch:
+    """findBestMatch over a fixed batch of (query, train) RankedImage pairs that is matched
+    repeatedly (rsfm_cashash_fbm_batch_*): the work list is built once, at creation (one stream
+    synchronization); launch() re-initialises the results and matches on `stream` with no
+    allocation and no host synchronization. results: per pair (best int64 [nq], best int64 [nt])."""
+
+    def __init__(self, pairs, per_scheme_lists=True, stream=None):
+        lib = _lib.load()
+        self.pairs = list(pairs)
+
+        def ci(img):
+            return _lib.CasHashImage(img.desc.data_ptr(), img.upper.data_ptr(), img.buckets.data_ptr(),
+                                     img.sqr.data_ptr())
+
+        sizes = [n for q, t in self.pairs for n in (q.n, t.n)]
+        self._flat = torch.empty(sum(sizes), dtype=torch.int64, device=self.pairs[0][0].desc.device)
+        views = torch.split(self._flat, sizes)
+        self.results = list(zip(views[0::2], views[1::2]))
+        arr = (_lib.CasHashPair * len(self.pairs))(*[
+            _lib.CasHashPair(ci(q), ci(t), q.n, t.n, _lib.CasHashResult(a.data_ptr(), b.data_ptr()))
+            for (q, t), (a, b) in zip(self.pairs, self.results)])
+        self._h = ctypes.c_void_p(0)
+        _lib.check(lib.rsfm_cashash_fbm_batch_create(ctypes.cast(arr, ctypes.c_void_p), len(self.pairs),
+                                                     1 if per_scheme_lists else 0, _stream_ptr(stream),
+                                                     ctypes.byref(self._h)), "rsfm_cashash_fbm_batch_create")
+
+    def launch(self, stream=None):
+        _lib.check(_lib.load().rsfm_cashash_fbm_batch_launch(self._h, _stream_ptr(stream)),
+                   "rsfm_cashash_fbm_batch_launch")
+        return self.results
+
+    def close(self):
+        if self._h:
+            _lib.load().rsfm_cashash_fbm_batch_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def find_best_match(queries, train, per_scheme_lists=True, max_bucket_sizes=None, stream=None):
     """cashash::findBestMatch (cascadeHash.h:106-107) over RankedImages: every (query, train)
     descriptor pair sharing a bucket in any of the 8 schemes is scored by exact L2; returns per query

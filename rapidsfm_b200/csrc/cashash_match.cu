@@ -397,6 +397,45 @@ __global__ void __launch_bounds__(1024) subitem_scan_kernel(uint32_t* __restrict
     if (threadIdx.x == 0) counts[n] = carry;
 }
 
+// Exclusive prefix of counts[0..n) in place, three phases for any n: scan_blocks_kernel scans
+// each 1024-item block and leaves the block total in sums[block]; subitem_scan_kernel (one CTA)
+// scans the block totals (the grand total lands in sums[nb]); scan_add_kernel adds each block's
+// offset and writes the total to counts[n].
+__global__ void __launch_bounds__(1024) scan_blocks_kernel(uint32_t* __restrict__ counts, uint32_t n,
+                                                           uint32_t* __restrict__ sums) {
+    __shared__ uint32_t warpSum[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+    const uint32_t v = i < n ? counts[i] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= uint32_t(o)) incl += y;
+    }
+    if (lane == 31) warpSum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warpSum[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= uint32_t(o)) wi += y;
+        }
+        warpSum[lane] = wi - w;  // exclusive prefix of the warp totals
+        if (lane == 31) sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    if (i < n) counts[i] = warpSum[warp] + incl - v;
+}
+__global__ void scan_add_kernel(uint32_t* __restrict__ counts, uint32_t n, const uint32_t* __restrict__ sums,
+                                uint32_t nb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) counts[i] += sums[i >> 10];
+    if (i == 0) counts[n] = sums[nb];
+}
+
 __global__ void subitem_expand_kernel(const PairDev* __restrict__ pairs, uint32_t nItems, uint32_t schemeOffset,
                                       const uint32_t* __restrict__ offsets, SubItem* __restrict__ subs) {
     for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nItems; it += gridDim.x * blockDim.x) {
@@ -626,13 +665,21 @@ extern "C" int rsfm_cashash_find_best_match(const rsfm_cashash_image* queries, c
     return find_best_match_impl(queries, querySize, train, trainSize, results, nbTasks, 0u, stream);
 }
 
-extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
-                                                  cudaStream_t stream) {
-    launch_count_reset();
-    if (nbPairs == 0) return RSFM_OK;
+// The device work of a batch of pairs: the pair table, the sub-item list and its size. Built on
+// `stream` with one read-back of the size (the builder synchronizes the stream once).
+struct FbmWork {
+    chm::PairDev* table = nullptr;
+    uint32_t* counter = nullptr;
+    uint32_t* total = nullptr;  // device: number of sub-items
+    chm::SubItem* subs = nullptr;
+    uint32_t nPairs = 0, nSubs = 0, maxN = 1, schemeOffset = 0;
+};
+
+static int fbm_table(const rsfm_cashash_pair* pairs, uint32_t nbPairs, std::vector<chm::PairDev>& host,
+                     uint32_t& maxN) {
     if (!pairs || nbPairs > 65535u) return RSFM_ERR_INVALID_ARG;
-    std::vector<chm::PairDev> host(nbPairs);
-    uint32_t maxN = 1;
+    host.resize(nbPairs);
+    maxN = 1;
     auto bad = [](const rsfm_cashash_image& m) {
         return !m.desc || !m.bucketEnds || !m.buckets || !m.sqrNormDesc || (reinterpret_cast<uintptr_t>(m.desc) & 15u);
     };
@@ -649,63 +696,153 @@ extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs
         d.nT = in.trainSize;
         maxN = std::max(maxN, std::max(d.nQ, d.nT));
     }
-    cudaMemPool_t pool = nullptr;
-    const int ps = scratch_pool(&pool);
-    if (ps != RSFM_OK) return ps;
-    uint8_t* scratch = nullptr;
-    const size_t tableBytes = sizeof(chm::PairDev) * nbPairs;
-    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), 256 + tableBytes, pool, stream));
-    auto* counter = reinterpret_cast<uint32_t*>(scratch);
-    auto* table = reinterpret_cast<chm::PairDev*>(scratch + 256);
-    int st = RSFM_OK;
-    // pageable source: the copy is staged before the call returns, so `host` may go out of scope
-    if (cudaMemcpyAsync(table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) st = RSFM_ERR_CUDA;
-    const uint32_t schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
-    const uint32_t nItems = nbPairs * 2048u;
-    uint32_t* offsets = nullptr;
-    chm::SubItem* subs = nullptr;
-    uint32_t nSubs = 0;
+    return RSFM_OK;
+}
+
+// Counts, scans (offsets: nItems + 1 entries, sums: nItems / 1024 + 2), reads back the size and
+// expands the sub-item list into `subs` (allocated by `alloc` once the size is known).
+template <typename Alloc>
+static int fbm_build(FbmWork& W, uint32_t* offsets, uint32_t* sums, cudaStream_t stream, Alloc&& alloc) {
+    const uint32_t nItems = W.nPairs * 2048u;
+    const uint32_t g = std::min<uint32_t>((nItems + 255) / 256, uint32_t(8 * sm_count()));
+    chm::subitem_count_kernel<<<g, 256, 0, stream>>>(W.table, nItems, W.schemeOffset, offsets);
+    const uint32_t nb = (nItems + 1023) / 1024;
+    chm::scan_blocks_kernel<<<nb, 1024, 0, stream>>>(offsets, nItems, sums);
+    chm::subitem_scan_kernel<<<1, 1024, 0, stream>>>(sums, nb);
+    chm::scan_add_kernel<<<(nItems + 255) / 256, 256, 0, stream>>>(offsets, nItems, sums, nb);
+    launch_count_add(4);
+    // the sub-item list is sized from its count: one read-back (synchronizes the stream)
+    RSFM_CUDA_TRY(cudaGetLastError());
+    RSFM_CUDA_TRY(cudaMemcpyAsync(&W.nSubs, offsets + nItems, 4, cudaMemcpyDeviceToHost, stream));
+    RSFM_CUDA_TRY(cudaStreamSynchronize(stream));
+    W.total = offsets + nItems;
+    if (W.nSubs == 0) return RSFM_OK;
+    const int st = alloc(reinterpret_cast<void**>(&W.subs), size_t(W.nSubs) * sizeof(chm::SubItem));
+    if (st != RSFM_OK) return st;
+    chm::subitem_expand_kernel<<<g, 256, 0, stream>>>(W.table, nItems, W.schemeOffset, offsets, W.subs);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+// Result init + the matching kernel (no allocation, no host synchronization).
+static int fbm_launch(const FbmWork& W, cudaStream_t stream) {
     const size_t smem = sizeof(chm::SubSmem) + 1024;
-    if (st == RSFM_OK) st = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_subitems_kernel), smem);
-    if (st == RSFM_OK && cudaMallocFromPoolAsync(reinterpret_cast<void**>(&offsets), (size_t(nItems) + 1) * 4, pool,
-                                                 stream) != cudaSuccess)
+    int st = set_max_dynamic_smem(reinterpret_cast<const void*>(chm::match_subitems_kernel), smem);
+    if (st != RSFM_OK) return st;
+    chm::pairs_init_kernel<<<dim3(std::min<uint32_t>((W.maxN + 255) / 256, 64u), W.nPairs), 256, 0, stream>>>(
+        W.table, W.counter);
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    if (W.nSubs == 0) return RSFM_OK;
+    const uint32_t units = (W.nSubs + 3u) / 4u;
+    const uint32_t grid = std::min<uint32_t>(units, uint32_t(4 * sm_count()));  // 4 x 128 TMEM columns
+    void* tok = nullptr;
+    const bool prof = profile_begin(stream, &tok);
+    chm::match_subitems_kernel<<<grid, chm::kThreads, smem, stream>>>(W.table, W.subs, W.total, W.schemeOffset,
+                                                                       device_error_word());
+    RSFM_CUDA_TRY(cudaGetLastError());
+    if (prof) profile_end(stream, tok);
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
+                                                  cudaStream_t stream) {
+    launch_count_reset();
+    if (nbPairs == 0) return RSFM_OK;
+    std::vector<chm::PairDev> host;
+    FbmWork W;
+    int st = fbm_table(pairs, nbPairs, host, W.maxN);
+    if (st != RSFM_OK) return st;
+    W.nPairs = nbPairs;
+    W.schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+    cudaMemPool_t pool = nullptr;
+    st = scratch_pool(&pool);
+    if (st != RSFM_OK) return st;
+    const uint32_t nItems = nbPairs * 2048u;
+    const size_t tableBytes = sizeof(chm::PairDev) * nbPairs;
+    const size_t offBytes = (size_t(nItems) + 1) * 4, sumBytes = (size_t(nItems) / 1024 + 2) * 4;
+    uint8_t* scratch = nullptr;
+    RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch),
+                                          256 + tableBytes + offBytes + sumBytes + 256, pool, stream));
+    W.counter = reinterpret_cast<uint32_t*>(scratch);
+    W.table = reinterpret_cast<chm::PairDev*>(scratch + 256);
+    auto* offsets = reinterpret_cast<uint32_t*>(scratch + 256 + ((tableBytes + 255) & ~size_t(255)));
+    auto* sums = offsets + nItems + 1;
+    // pageable source: the copy is staged before the call returns, so `host` may go out of scope
+    if (cudaMemcpyAsync(W.table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess)
         st = RSFM_ERR_CUDA;
-    if (st == RSFM_OK) {
-        chm::pairs_init_kernel<<<dim3(std::min<uint32_t>((maxN + 255) / 256, 64u), nbPairs), 256, 0, stream>>>(table,
-                                                                                                          counter);
-        const uint32_t g = std::min<uint32_t>((nItems + 255) / 256, uint32_t(8 * sm_count()));
-        chm::subitem_count_kernel<<<g, 256, 0, stream>>>(table, nItems, schemeOffset, offsets);
-        chm::subitem_scan_kernel<<<1, 1024, 0, stream>>>(offsets, nItems);
-        launch_count_add(3);
-        // the sub-item list is sized from its count: one read-back (the call synchronizes the stream)
-        if (cudaGetLastError() != cudaSuccess ||
-            cudaMemcpyAsync(&nSubs, offsets + nItems, 4, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess)
-            st = RSFM_ERR_CUDA;
-    }
-    if (st == RSFM_OK && nSubs > 0) {
-        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&subs), size_t(nSubs) * sizeof(chm::SubItem), pool,
-                                    stream) != cudaSuccess)
-            st = RSFM_ERR_CUDA;
-        if (st == RSFM_OK) {
-            const uint32_t g = std::min<uint32_t>((nItems + 255) / 256, uint32_t(8 * sm_count()));
-            chm::subitem_expand_kernel<<<g, 256, 0, stream>>>(table, nItems, schemeOffset, offsets, subs);
-            const uint32_t units = (nSubs + 3u) / 4u;
-            const uint32_t grid = std::min<uint32_t>(units, uint32_t(4 * sm_count()));  // 4 x 128 TMEM columns
-            void* tok = nullptr;
-            const bool prof = profile_begin(stream, &tok);
-            chm::match_subitems_kernel<<<grid, chm::kThreads, smem, stream>>>(table, subs, offsets + nItems,
-                                                                               schemeOffset, device_error_word());
-            if (cudaGetLastError() != cudaSuccess) st = RSFM_ERR_CUDA;
-            if (prof) profile_end(stream, tok);
-            launch_count_add(2);
-        }
-    }
-    if (subs) cudaFreeAsync(subs, stream);
-    if (offsets) cudaFreeAsync(offsets, stream);
+    if (st == RSFM_OK)
+        st = fbm_build(W, offsets, sums, stream, [&](void** ptr, size_t bytes) {
+            return cudaMallocFromPoolAsync(ptr, bytes, pool, stream) == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA;
+        });
+    if (st == RSFM_OK) st = fbm_launch(W, stream);
+    if (W.subs) cudaFreeAsync(W.subs, stream);
     const cudaError_t e = cudaFreeAsync(scratch, stream);
     if (st == RSFM_OK && e != cudaSuccess) st = RSFM_ERR_CUDA;
     return st;
+}
+
+struct rsfm_cashash_fbm_batch {
+    FbmWork W;
+    void* mem = nullptr;  // table, counter, offsets, sums
+};
+
+extern "C" int rsfm_cashash_fbm_batch_create(const rsfm_cashash_pair* pairs, uint32_t nbPairs, uint32_t flags,
+                                             cudaStream_t stream, rsfm_cashash_fbm_batch** out) {
+    launch_count_reset();
+    if (!out || nbPairs == 0) return RSFM_ERR_INVALID_ARG;
+    std::vector<chm::PairDev> host;
+    auto* b = new rsfm_cashash_fbm_batch();
+    FbmWork& W = b->W;
+    int st = fbm_table(pairs, nbPairs, host, W.maxN);
+    if (st != RSFM_OK) {
+        delete b;
+        return st;
+    }
+    W.nPairs = nbPairs;
+    W.schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+    const uint32_t nItems = nbPairs * 2048u;
+    const size_t tableBytes = (sizeof(chm::PairDev) * nbPairs + 255) & ~size_t(255);
+    const size_t offBytes = (size_t(nItems) + 1) * 4, sumBytes = (size_t(nItems) / 1024 + 2) * 4;
+    if (cudaMalloc(&b->mem, 256 + tableBytes + offBytes + sumBytes) != cudaSuccess) {
+        delete b;
+        return RSFM_ERR_CUDA;
+    }
+    auto* base = static_cast<uint8_t*>(b->mem);
+    W.counter = reinterpret_cast<uint32_t*>(base);
+    W.table = reinterpret_cast<chm::PairDev*>(base + 256);
+    auto* offsets = reinterpret_cast<uint32_t*>(base + 256 + tableBytes);
+    auto* sums = offsets + nItems + 1;
+    if (cudaMemcpyAsync(W.table, host.data(), sizeof(chm::PairDev) * nbPairs, cudaMemcpyHostToDevice, stream) !=
+        cudaSuccess)
+        st = RSFM_ERR_CUDA;
+    if (st == RSFM_OK)
+        st = fbm_build(W, offsets, sums, stream, [](void** ptr, size_t bytes) {
+            return cudaMalloc(ptr, bytes) == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA;
+        });
+    if (st == RSFM_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = RSFM_ERR_CUDA;
+    if (st != RSFM_OK) {
+        rsfm_cashash_fbm_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_cashash_fbm_batch_launch(const rsfm_cashash_fbm_batch* b, cudaStream_t stream) {
+    launch_count_reset();
+    if (!b) return RSFM_ERR_INVALID_ARG;
+    return fbm_launch(b->W, stream);
+}
+
+extern "C" int rsfm_cashash_fbm_batch_destroy(rsfm_cashash_fbm_batch* b) {
+    if (!b) return RSFM_OK;
+    if (b->W.subs) cudaFree(b->W.subs);
+    if (b->mem) cudaFree(b->mem);
+    delete b;
+    return RSFM_OK;
 }
 
 extern "C" int rsfm_cashash_find_best_match_ex(const rsfm_cashash_image* queries, const uint32_t* querySize,

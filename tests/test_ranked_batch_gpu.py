@@ -140,3 +140,44 @@ def test_find_best_match_pairs_api(rsfm, per_scheme):
         torch.cuda.synchronize()
         assert torch.equal(bq, eq) and torch.equal(bt, et)
     assert ch.find_best_match_pairs([]) == []
+
+
+def test_find_best_match_batch_repeated_and_many_pairs(rsfm, oracle):
+    """FindBestMatchBatch (work list built once, launches without host synchronization) against
+    find_best_match_pairs and the oracle: 600 pairs of small images (1.2 M bucket items, so the
+    work-list scan spans many blocks), launched twice with the results scribbled over between
+    launches, plus the pairs with an empty image."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(14))
+    rng = np.random.default_rng(14)
+    hosts = [synth.make_pair(int(rng.integers(40, 400)), int(rng.integers(40, 400)), 0.5, 8.0, seed=1400 + k)[:2]
+             for k in range(600)]
+    devs = [(_dev(q), _dev(t)) for q, t in hosts]
+    for q, t in devs:
+        cas.fit(q)
+    empty = torch.empty((0, 128), dtype=torch.uint8, device="cuda")
+    imgs = ch.register_ranked_images(cas, [x for p in devs for x in p] + [empty])
+    pairs = list(zip(imgs[0:1200:2], imgs[1:1200:2])) + [(imgs[1200], imgs[1]), (imgs[0], imgs[1200])]
+    batch = ch.FindBestMatchBatch(pairs)
+    want = ch.find_best_match_pairs(pairs)
+    for rep in range(2):
+        for bq, bt in batch.results:
+            bq.fill_(7)
+            bt.fill_(7)
+        got = batch.launch()
+        torch.cuda.synchronize()
+        assert rsfm.device_error() == 0
+        for (bq, bt), (wq, wt) in zip(got, want):
+            assert torch.equal(bq, wq) and torch.equal(bt, wt)
+    # a few pairs against the oracle directly (per-scheme bucket lists, as the batch reads them)
+    for k in (0, 17, 599):
+        q, t = hosts[k]
+        qi, ti = pairs[k]
+        eq, et = oracle.cashash_find_best_match(q, qi.upper.cpu().numpy().view(np.uint32),
+                                                qi.buckets.cpu().numpy().view(np.uint32), t,
+                                                ti.upper.cpu().numpy().view(np.uint32),
+                                                ti.buckets.cpu().numpy().view(np.uint32), per_scheme=True)
+        bq, bt = batch.results[k]
+        np.testing.assert_array_equal(bq.cpu().numpy().view(np.uint32).reshape(-1, 2), eq)
+        np.testing.assert_array_equal(bt.cpu().numpy().view(np.uint32).reshape(-1, 2), et)
+    batch.close()
