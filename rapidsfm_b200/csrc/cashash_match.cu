@@ -73,6 +73,9 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool va
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
 
 // Ascending sort of one value per lane (bitonic network over the warp).
 __device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
@@ -324,18 +327,50 @@ __global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* c
 // products, and warp w reads only its diagonal 32 x 32 block of the accumulator. Row and column
 // minima are merged across sub-items by the same 64-bit atomicMin as everywhere else.
 struct SubItem {
-    uint32_t item;  // pair * 2048 + bucket * 8 + scheme
-    uint32_t seg;   // query segment << 16 | train segment
+    const uint32_t* qList;  // first query member of the segment (bucket list of the query image)
+    const uint32_t* tList;  // first train member of the segment
+    uint32_t pair;
+    uint32_t counts;        // query members in the segment | train members << 16 (each 1..32)
 };
 
-struct SubSmem {
+// Warp-specialised persistent kernel (one CTA per SM): producer warps gather the rows of a unit
+// (four sub-items) into a ring of shared-memory stages with cp.async, one thread issues the UMMAs
+// (the products and their transpose) into one of two TMEM buffers, and two groups of four
+// epilogue warps (one warp per sub-item and TMEM lane quarter) reduce the diagonal blocks of
+// alternate units: query minima from the products, train minima from the transpose, both
+// thread-local. A producer's time per
+// sub-item is a chain of dependent loads (record, member lists, then norms and rows), so four
+// producer warps per sub-item slot take every fourth unit and pipeline the chain across their
+// units; norms and rows signal their arrival on the stage barrier by themselves
+// (cp.async.mbarrier.arrive), so a producer never waits for its own copies.
+constexpr int kSubStages = 6;
+constexpr int kSubEpi = 8;
+constexpr int kSubProducers = 16;
+constexpr int kSubMmaWarp = kSubEpi;
+constexpr int kSubThreads = 32 * (kSubEpi + 1 + kSubProducers);  // epilogue 0-7, MMA 8, producers 9..
+
+struct alignas(1024) SubStage {
     uint8_t a[128 * 128];
     uint8_t b[128 * 128];
     uint32_t rowQ[128], rowNA[128];
     uint32_t colT[128], colNB[128];
-    uint64_t mma;
+    unsigned long long* qBest[4];
+    unsigned long long* tBest[4];
+};
+
+struct SubSmem {
+    SubStage st[kSubStages];
+    uint64_t full[kSubStages], empty[kSubStages];
+    uint64_t accFull[2], accEmpty[2];
     uint32_t tmem;
 };
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Arrives on `bar` once all of this thread's earlier cp.async copies have landed (the barrier's
+// expected count includes this arrival).
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 
 __device__ __forceinline__ void item_ranges(const PairDev& P, uint32_t local, uint32_t schemeOffset, uint32_t& qb,
                                             uint32_t& nQ, uint32_t& tb, uint32_t& nT, uint32_t& s) {
@@ -445,130 +480,204 @@ __global__ void subitem_expand_kernel(const PairDev* __restrict__ pairs, uint32_
         uint32_t qb, nQ, tb, nT, s;
         item_ranges(P, it & 2047u, schemeOffset, qb, nQ, tb, nT, s);
         const uint32_t segT = (nT + 31u) / 32u;
-        for (uint32_t x = 0; x < c; ++x) subs[o + x] = SubItem{it, ((x / segT) << 16) | (x % segT)};
+        for (uint32_t x = 0; x < c; ++x) {
+            const uint32_t m0 = (x / segT) * 32u, c0 = (x % segT) * 32u;
+            subs[o + x] = SubItem{P.q.buckets + qb + m0, P.t.buckets + tb + c0, it >> 11,
+                                  min(nQ - m0, 32u) | (min(nT - c0, 32u) << 16)};
+        }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) match_subitems_kernel(const PairDev* __restrict__ pairs,
-                                                                  const SubItem* __restrict__ subs,
-                                                                  const uint32_t* __restrict__ total,
-                                                                  uint32_t schemeOffset, uint32_t* err) {
+__global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const PairDev* __restrict__ pairs,
+                                                                      const SubItem* __restrict__ subs,
+                                                                      const uint32_t* __restrict__ total,
+                                                                      uint32_t schemeOffset, uint32_t* err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     SubSmem& S = smem_aligned_1024<SubSmem>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     if (tid == 0) {
-        mbar_init(&S.mma, 1);
+        for (int s = 0; s < kSubStages; ++s) {
+            // every thread of the unit's four producer warps, twice: once after writing the row and
+            // column records, once (asynchronously) when its rows have landed
+            mbar_init(&S.full[s], 2 * 32 * 4);
+            mbar_init(&S.empty[s], 4);  // the four epilogue warps of the unit's group
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&S.accFull[b], 1);
+            mbar_init(&S.accEmpty[b], 4);
+        }
         fence_mbar_init();
     }
-    if (warp == 0) {
-        tmem_alloc(&S.tmem, 128);
+    if (warp == kSubMmaWarp) {
+        tmem_alloc(&S.tmem, 512);
         tmem_relinquish();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem;
-    const uint32_t idesc = idesc_u8u8_s32(128, 128);
-    uint32_t mmaPhase = 0;
     const uint32_t nSubs = *total;
-    // Everything a warp needs for one sub-item, fetched one unit ahead (its chain of dependent
-    // loads - sub-item, bucket bounds, member lists, norms - overlaps the current unit's MMA).
-    struct Fetched {
-        uint32_t q, t, nA, nB;
-        const uint8_t* qd;
-        const uint8_t* td;
-        unsigned long long* qBest;
-        unsigned long long* tBest;
-    };
-    const uint8_t* dummy = reinterpret_cast<const uint8_t*>(subs);  // zero-byte cp.async source
-    auto fetch = [&](uint32_t si) {
-        Fetched f{kNoRow, kNoRow, kBigNorm, kBigNorm, dummy, dummy, nullptr, nullptr};
-        const bool have = si < nSubs;
-        const SubItem sub = have ? subs[si] : SubItem{0u, 0u};
-        const PairDev& P = pairs[sub.item >> 11];
-        uint32_t qb = 0, nQ = 0, tb = 0, nT = 0, s = 0;
-        if (have) item_ranges(P, sub.item & 2047u, schemeOffset, qb, nQ, tb, nT, s);
-        const uint32_t m = (sub.seg >> 16) * 32u + lane, c = (sub.seg & 0xFFFFu) * 32u + lane;
-        f.q = warp_sort(have && m < nQ ? __ldg(&P.q.buckets[qb + m]) : kNoRow, lane);
-        f.t = warp_sort(have && c < nT ? __ldg(&P.t.buckets[tb + c]) : kNoRow, lane);
-        if (f.q != kNoRow) {
-            f.nA = __ldg(&P.q.sqr[f.q]);
-            f.qd = P.q.desc + size_t(f.q) * 128;
-        }
-        if (f.t != kNoRow) {
-            f.nB = __ldg(&P.t.sqr[f.t]);
-            f.td = P.t.desc + size_t(f.t) * 128;
-        }
-        if (have) {
-            f.qBest = P.qBest;
-            f.tBest = P.tBest;
-        }
-        return f;
-    };
-    Fetched cur = fetch(4u * blockIdx.x + warp);
-    for (uint32_t unit = blockIdx.x; 4u * unit < nSubs; unit += gridDim.x) {
-        // ---- warp w: sub-item 4 unit + w (rows and columns sorted by index)
-        const uint32_t row = 32u * warp + lane;
-        S.rowQ[row] = cur.q;
-        S.rowNA[row] = cur.nA;
-        S.colT[row] = cur.t;
-        S.colNB[row] = cur.nB;
-#pragma unroll
-        for (uint32_t ch = 0; ch < 8; ++ch) {
-            cp_async16(S.a + sw128(row, ch), cur.qd + (cur.q != kNoRow ? 16 * ch : 0), cur.q != kNoRow);
-            cp_async16(S.b + sw128(row, ch), cur.td + (cur.t != kNoRow ? 16 * ch : 0), cur.t != kNoRow);
-        }
-        cp_async_wait_all();
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t a = smem_u32(S.a), b = smem_u32(S.b);
-#pragma unroll
-            for (uint32_t kk = 0; kk < 4; ++kk)
-                umma_i8(tmem, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk), idesc, kk);
-            umma_commit(&S.mma);
-        }
-        const Fetched nxt = fetch(4u * (unit + gridDim.x) + warp);
-        __syncwarp();
-        mbar_wait(&S.mma, mmaPhase, err, kDevTimeoutAccFull);
-        mmaPhase ^= 1u;
-        tc_fence_after();
-        // ---- epilogue: warp w's diagonal block (TMEM lanes 32w.., columns 32w..)
-        uint32_t x[32];
-        tmem_ld32(tmem + ((32u * warp) << 16) + 32u * warp, x);
-        tmem_wait_ld();
-        const uint32_t nA = S.rowNA[row];
-        const bool rowValid = cur.q != kNoRow;
-        uint32_t rmin = 0xFFFFFFFFu;
-#pragma unroll
-        for (uint32_t k = 0; k < 32; ++k) {
-            const uint32_t d = nA + S.colNB[32 * warp + k] - 2u * x[k];
-            x[k] = d;
-            rmin = min(rmin, (d << 5) | k);  // ties -> lowest column = lowest train index (sorted)
-        }
-        const uint32_t cd = rmin >> 5;
-        if (rowValid && cd < kValidD)
-            atomicMin(&cur.qBest[cur.q], (static_cast<unsigned long long>(cd) << 32) | S.colT[32 * warp + (rmin & 31u)]);
-        if (cur.tBest) {
-            uint32_t mine = 0xFFFFFFFFu;
-#pragma unroll
-            for (uint32_t k = 0; k < 32; ++k) {
-                const uint32_t key = rowValid && x[k] < kValidD ? ((x[k] << 5) | lane) : 0xFFFFFFFFu;
-                const uint32_t mk = __reduce_min_sync(0xffffffffu, key);
-                mine = (lane == k) ? mk : mine;
+    const uint32_t nUnits = (nSubs + 3u) / 4u;
+    // this CTA's units: blockIdx.x + i * gridDim.x, i < nLocal
+    const uint32_t nLocal = blockIdx.x < nUnits ? (nUnits - blockIdx.x + gridDim.x - 1u) / gridDim.x : 0u;
+
+    if (warp > kSubMmaWarp) {
+        // ------------------------------------------------------------ producers
+        // Warp pw fills slot j = pw % 4 (sub-item 4 unit + j, rows 32 j..) of the units i with
+        // i % 4 = pw / 4. Members are sorted by index, so the lowest position wins ties.
+        const uint32_t pw = warp - (kSubMmaWarp + 1u), j = pw & 3u;
+        constexpr uint32_t kStep = kSubProducers / 4;
+        const uint8_t* dummy = reinterpret_cast<const uint8_t*>(subs);  // zero-byte cp.async source
+        const SubItem none{nullptr, nullptr, 0u, 0u};
+        auto record = [&](uint32_t i) {
+            const uint32_t si = 4u * (blockIdx.x + i * gridDim.x) + j;
+            return i < nLocal && si < nSubs ? subs[si] : none;
+        };
+        // One sub-item's members (unsorted, one per lane) and its pair's pointers.
+        struct Members {
+            uint32_t q, t;
+            const uint8_t* qd;
+            const uint8_t* td;
+            const uint32_t* qs;
+            const uint32_t* ts;
+            unsigned long long* qb;
+            unsigned long long* tb;
+        };
+        auto members = [&](const SubItem& r) {
+            const PairDev& P = pairs[r.pair];
+            Members m;
+            m.q = lane < (r.counts & 0xFFFFu) ? __ldg(&r.qList[lane]) : kNoRow;
+            m.t = lane < (r.counts >> 16) ? __ldg(&r.tList[lane]) : kNoRow;
+            m.qd = P.q.desc;
+            m.td = P.t.desc;
+            m.qs = P.q.sqr;
+            m.ts = P.t.sqr;
+            m.qb = r.counts ? P.qBest : nullptr;
+            m.tb = r.counts ? P.tBest : nullptr;
+            return m;
+        };
+        // Software pipeline over this warp's units: records are loaded two units ahead and member
+        // lists one unit ahead; norms and rows go straight to shared memory by cp.async. A stage is
+        // taken only when its unit's members are known.
+        uint32_t i = pw >> 2;
+        SubItem r1 = record(i + kStep);
+        Members cur = members(record(i));
+        for (; i < nLocal; i += kStep) {
+            const SubItem r2 = record(i + 2 * kStep);
+            const Members nxt = members(r1);
+            const uint32_t q = warp_sort(cur.q, lane), t = warp_sort(cur.t, lane);
+            const uint32_t stg = i % kSubStages;
+            mbar_wait_backoff(&S.empty[stg], ((i / kSubStages) & 1u) ^ 1u, err, kDevTimeoutTmaEmpty, 256u);
+            SubStage& T = S.st[stg];
+            const uint32_t row = 32u * j + lane;
+            T.rowQ[row] = q;
+            T.colT[row] = t;
+            if (q != kNoRow) cp_async4(&T.rowNA[row], cur.qs + q); else T.rowNA[row] = kBigNorm;
+            if (t != kNoRow) cp_async4(&T.colNB[row], cur.ts + t); else T.colNB[row] = kBigNorm;
+            if (lane == 0) {
+                T.qBest[j] = cur.qb;
+                T.tBest[j] = cur.tb;
             }
-            if (mine != 0xFFFFFFFFu && cur.t != kNoRow)
-                atomicMin(&cur.tBest[cur.t], (static_cast<unsigned long long>(mine >> 5) << 32) |
-                                                 S.rowQ[32 * warp + (mine & 31u)]);
+            // rows: eight lanes copy the eight 16-byte chunks of one row, four rows per
+            // instruction (four cache lines per instruction instead of 32)
+#pragma unroll
+            for (uint32_t ii = 0; ii < 8; ++ii) {
+                const uint32_t r = 4u * ii + (lane >> 3), ch = lane & 7u;
+                const uint32_t qr = __shfl_sync(0xffffffffu, q, r), tr = __shfl_sync(0xffffffffu, t, r);
+                cp_async16(T.a + sw128(32u * j + r, ch), qr != kNoRow ? cur.qd + size_t(qr) * 128 + 16 * ch : dummy,
+                           qr != kNoRow);
+                cp_async16(T.b + sw128(32u * j + r, ch), tr != kNoRow ? cur.td + size_t(tr) * 128 + 16 * ch : dummy,
+                           tr != kNoRow);
+            }
+            mbar_arrive(&S.full[stg]);                // the records above (release)
+            cp_async_mbar_arrive_noinc(&S.full[stg]);  // rows and norms, when they have landed
+            cur = nxt;
+            r1 = r2;
         }
-        tc_fence_before();
-        __syncthreads();  // tiles and TMEM are reused by the next unit
-        cur = nxt;
+    } else if (warp == kSubMmaWarp) {
+        // ------------------------------------------------------------ UMMA issuer
+        if (elect_one()) {
+            const uint32_t idesc = idesc_u8u8_s32(128, 128);
+            for (uint32_t i = 0; i < nLocal; ++i) {
+                const uint32_t stg = i % kSubStages, buf = i & 1u;
+                mbar_wait_backoff(&S.full[stg], (i / kSubStages) & 1u, err, kDevTimeoutTmaFull, 32u);
+                mbar_wait_backoff(&S.accEmpty[buf], ((i >> 1) & 1u) ^ 1u, err, kDevTimeoutAccEmpty, 32u);
+                // the rows were written by cp.async (generic proxy); the UMMA reads them through
+                // the async proxy
+                fence_proxy_async_smem();
+                tc_fence_after();
+                const uint32_t a = smem_u32(S.st[stg].a), b = smem_u32(S.st[stg].b);
+                // the products (lane = query row, column = train row) and their transpose (lane =
+                // train row, column = query row), side by side in the unit's buffer
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    umma_i8(tmem + buf * 256u, umma_desc_k_sw128(a + 32u * kk), umma_desc_k_sw128(b + 32u * kk),
+                            idesc, kk);
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    umma_i8(tmem + buf * 256u + 128u, umma_desc_k_sw128(b + 32u * kk),
+                            umma_desc_k_sw128(a + 32u * kk), idesc, kk);
+                umma_commit(&S.accFull[buf]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------ epilogue
+        // Group e = warp / 4 takes the units i with i % 2 = e (TMEM buffer e); its warp w = warp % 4
+        // reduces sub-item w's diagonal block (TMEM lanes 32w.., columns 32w..).
+        const uint32_t e = warp >> 2, w = warp & 3u;
+        const uint32_t row = 32u * w + lane;
+        for (uint32_t i = e; i < nLocal; i += 2) {
+            const uint32_t stg = i % kSubStages, buf = i & 1u;
+            mbar_wait_backoff(&S.accFull[buf], (i >> 1) & 1u, err, kDevTimeoutAccFull, 32u);
+            // (complete already; acquires the producers' row and column records)
+            mbar_wait(&S.full[stg], (i / kSubStages) & 1u, err, kDevTimeoutTmaFull);
+            tc_fence_after();
+            // diagonal blocks of sub-item w: x = products of query row 32w + lane with the
+            // sub-item's 32 train rows, then y = products of train row 32w + lane with its 32
+            // query rows (one block in registers at a time)
+            const SubStage& T = S.st[stg];
+            uint32_t x[32];
+            tmem_ld32(tmem + ((32u * w) << 16) + buf * 256u + 32u * w, x);
+            tmem_wait_ld();
+            // Keys (d << 5 | position): positions follow the sorted member indices, so the smallest
+            // key is the smallest distance with ties to the lowest index. Padding rows and columns
+            // have norm kBigNorm and zero data, so their distances are >= kValidD.
+            {   // query member 32w + lane: minimum over the train members
+                const uint32_t nA = T.rowNA[row];
+                uint32_t m4[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+#pragma unroll
+                for (uint32_t k = 0; k < 32; ++k)
+                    m4[k & 3u] = min(m4[k & 3u], ((nA + T.colNB[32 * w + k] - 2u * x[k]) << 5) | k);
+                const uint32_t key = min(min(m4[0], m4[1]), min(m4[2], m4[3]));
+                if ((key >> 5) < kValidD)
+                    atomicMin(&T.qBest[w][T.rowQ[row]],
+                              (static_cast<unsigned long long>(key >> 5) << 32) | T.colT[32 * w + (key & 31u)]);
+            }
+            uint32_t y[32];
+            tmem_ld32(tmem + ((32u * w) << 16) + buf * 256u + 128u + 32u * w, y);
+            tmem_wait_ld();
+            tc_fence_before();
+            if (lane == 0) mbar_arrive(&S.accEmpty[buf]);
+            unsigned long long* tBest = T.tBest[w];
+            if (tBest) {  // train member 32w + lane: minimum over the query members
+                const uint32_t nB = T.colNB[row];
+                uint32_t m4[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+#pragma unroll
+                for (uint32_t k = 0; k < 32; ++k)
+                    m4[k & 3u] = min(m4[k & 3u], ((nB + T.rowNA[32 * w + k] - 2u * y[k]) << 5) | k);
+                const uint32_t key = min(min(m4[0], m4[1]), min(m4[2], m4[3]));
+                if ((key >> 5) < kValidD)
+                    atomicMin(&tBest[T.colT[row]],
+                              (static_cast<unsigned long long>(key >> 5) << 32) | T.rowQ[32 * w + (key & 31u)]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&S.empty[stg]);
+        }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 128);
+    if (threadIdx.x >> 5 == uint32_t(kSubMmaWarp)) tmem_dealloc(tmem, 512);
 }
 
 }  // namespace chm
@@ -736,10 +845,10 @@ static int fbm_launch(const FbmWork& W, cudaStream_t stream) {
     launch_count_add(1);
     if (W.nSubs == 0) return RSFM_OK;
     const uint32_t units = (W.nSubs + 3u) / 4u;
-    const uint32_t grid = std::min<uint32_t>(units, uint32_t(4 * sm_count()));  // 4 x 128 TMEM columns
+    const uint32_t grid = std::min<uint32_t>(units, uint32_t(sm_count()));  // persistent, one CTA per SM
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
-    chm::match_subitems_kernel<<<grid, chm::kThreads, smem, stream>>>(W.table, W.subs, W.total, W.schemeOffset,
+    chm::match_subitems_kernel<<<grid, chm::kSubThreads, smem, stream>>>(W.table, W.subs, W.total, W.schemeOffset,
                                                                        device_error_word());
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);

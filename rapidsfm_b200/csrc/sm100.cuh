@@ -106,6 +106,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+// The same bounded wait for warps that can afford to wake up late: between polls the warp sleeps
+// (__nanosleep, doubling from `ns0` up to 2 us) instead of polling again at once, so it leaves the
+// issue slots to the warps that do the work.
+__device__ __forceinline__ bool mbar_wait_backoff(uint64_t* bar, uint32_t parity, uint32_t* err, uint32_t code,
+                                                  uint32_t ns0) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    uint32_t ns = ns0;
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+        __nanosleep(ns);
+        if (mbar_try_wait(bar, parity)) return true;
+        ns = min(2u * ns, 2000u);
+        if ((i & 15u) == 15u) {
+            if (*reinterpret_cast<volatile uint32_t*>(err) != 0u) return false;
+            if (global_ns() - t0 > kWaitLimitNs) break;
+        }
+    }
+    atomicCAS(err, 0u, code);
+    return false;
+}
+
 // ---------------------------------------------------------------- TMA
 __device__ __forceinline__ void tma_prefetch_desc(const void* tmap) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
