@@ -46,6 +46,13 @@ __global__ void pack_kernel(const uint2* __restrict__ keys, const uint4* __restr
 
 // True when any of the first s key bytes of t equals q's (bytes 0-3 in .x, 4-7 in .y): the
 // candidate was already found in an earlier table. __vcmpeq4 sets 0xFF per equal byte.
+// Alignment the kernels' vector loads rely on: descriptors, codes and bucket lists 16 bytes,
+// keys 8, packed records 32.
+inline bool aligned(const Img& I) {
+    auto a = [](const void* p, uintptr_t m) { return (reinterpret_cast<uintptr_t>(p) & (m - 1)) == 0; };
+    return a(I.desc, 16) && a(I.keys, 8) && a(I.codes, 16) && a(I.buckets, 16) && a(I.rec, 32);
+}
+
 __device__ __forceinline__ bool collides_before(uint2 t, uint2 q, uint32_t s) {
     const uint32_t lo = s >= 4 ? 0xFFFFFFFFu : (1u << (8 * s)) - 1u;
     const uint32_t hi = s <= 4 ? 0u : (1u << (8 * (s - 4))) - 1u;
@@ -339,6 +346,15 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
 // descriptor as eight 16-byte loads. Results are identical to the warp kernel: same keys, same
 // set of the topK smallest, same exact re-rank rule.
 constexpr int kThreadTopK = 12;
+
+// One 32-byte record in one load (256-bit, read-only path): each thread of a warp reads a
+// different record, so the instruction costs one L1 wavefront per thread either way, and one
+// load instead of two halves them. `p` must be 32-byte aligned (records are).
+__device__ __forceinline__ void ldg_record(const uint4* p, uint4& a, uint4& b) {
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p));
+}
 constexpr int kThreadBlock = 128;
 constexpr int kThreadMinBlocks = 7;  // 72 registers, 28 warps per SM (6: 80 registers, 2 % slower)
 
@@ -363,14 +379,31 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
     };
     if (nt) open_table(0);
     for (;;) {
+        // Up to four candidates of the current list per step, from the 16-byte block of the
+        // (16-byte aligned) bucket array that holds the cursor: one load instead of four. A block
+        // that would reach past the lists of the tables in use is read one entry at a time.
+        while (x == hi && s + 1 < nt) open_table(++s);
+        if (x >= hi) break;
+        const size_t e = size_t(s) * T.n + x;
+        uint32_t off = 0, cnt = 1;
+        uint4 w;
+        if ((e | 3u) < size_t(nt) * T.n) {
+            off = uint32_t(e) & 3u;
+            w = __ldg(reinterpret_cast<const uint4*>(T.buckets + (e - off)));
+            cnt = min(4u - off, hi - x);
+        } else {
+            w.x = __ldg(&T.buckets[e]);
+            w.y = w.z = w.w = 0xFFFFFFFFu;
+        }
+        x += cnt;
         uint32_t j[4], su[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            while (x == hi && s + 1 < nt) open_table(++s);
+            const uint32_t pos = off + uint32_t(u);
+            const uint32_t v = pos == 0 ? w.x : pos == 1 ? w.y : pos == 2 ? w.z : w.w;
             su[u] = s;
-            j[u] = x < hi ? __ldg(&T.buckets[size_t(s) * T.n + x++]) : 0xFFFFFFFFu;
+            j[u] = uint32_t(u) < cnt ? v : 0xFFFFFFFFu;
         }
-        if (j[0] == 0xFFFFFFFFu) break;
         uint2 tk[4];
         uint4 tc[4];
 #pragma unroll
@@ -379,7 +412,8 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
                 tk[u] = make_uint2(0, 0);
                 tc[u] = make_uint4(0, 0, 0, 0);
             } else if (T.rec) {
-                const uint4 r0 = __ldg(&T.rec[2 * size_t(j[u])]), r1 = __ldg(&T.rec[2 * size_t(j[u]) + 1]);
+                uint4 r0, r1;
+                ldg_record(&T.rec[2 * size_t(j[u])], r0, r1);
                 tk[u] = make_uint2(r0.x, r0.y);
                 tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
             } else {
@@ -514,6 +548,7 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     if (!Q.desc || !Q.keys || !Q.codes || !Q.sqr) return RSFM_ERR_INVALID_ARG;
     if (train->nbDesc && (!T.desc || !T.keys || !T.codes || !T.ends || !T.buckets || !T.sqr))
         return RSFM_ERR_INVALID_ARG;
+    if (!chr::aligned(Q) || !chr::aligned(T)) return RSFM_ERR_INVALID_ARG;
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
     const chr::Out O{reinterpret_cast<unsigned long long*>(best), secondDist, flags, nbCandidates};
@@ -578,6 +613,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
             return RSFM_ERR_INVALID_ARG;
         host[p].q = mk(q);
         host[p].t = mk(t);
+        if (!chr::aligned(host[p].q) || !chr::aligned(host[p].t)) return RSFM_ERR_INVALID_ARG;
         host[p].o = chr::Out{reinterpret_cast<unsigned long long*>(in.best), in.secondDist, in.flags, in.nbCandidates};
         begin[p] = uint32_t(total);
         total += q->nbDesc;

@@ -94,3 +94,26 @@ def test_new_entry_points_validate_without_gpu(rsfm):
     assert lib.rsfm_ransac_match_filter(None, None, None, 0, None, 16, 12, 256, 15.0, 1, 0, None) == 0
     assert lib.rsfm_ransac_inlier_mask(0, 1200, None, 0, 2, 256, 0.15, 16, 1, 0, None, None) == 1
     assert lib.rsfm_ransac_inlier_mask(1600, 1200, None, 0, 2, 256, 0.15, 16, 1, 0, None, None) == 0
+
+
+def test_ranked_alignment_checked_without_gpu(rsfm):
+    """The ranked matcher's vector loads need aligned arrays (descriptors, codes and bucket lists
+    16 bytes, keys 8, records 32); a misaligned array is rejected before any CUDA call."""
+    lib = rsfm._lib.load()
+    R = rsfm._lib.RankedImage
+
+    def img(**over):
+        f = dict(desc=0x10000, keys=0x20000, codes=0x30000, bucketEnds=0x40000, buckets=0x50000,
+                 sqrNormDesc=0x60000, nbDesc=100, records=0x70000)
+        f.update(over)
+        return R(**f)
+
+    for bad in (dict(buckets=0x50004), dict(records=0x70010), dict(codes=0x30008), dict(keys=0x20004),
+                dict(desc=0x10008)):
+        q, t = img(), img(**bad)
+        assert lib.rsfm_cashash_match_ranked(ctypes.byref(q), ctypes.byref(t), 6, 10, 4, 5,
+                                             0x80000, 0x90000, 0xA0000, None, None) == 1
+        pair = rsfm._lib.RankedPair(ctypes.pointer(q), ctypes.pointer(t), 0x80000, 0x90000, 0xA0000, None)
+        h = ctypes.c_void_p(0)
+        assert lib.rsfm_ranked_batch_create(ctypes.byref(pair), 1, 6, 10, 4, 5, ctypes.byref(h)) == 1
+        assert not h.value
