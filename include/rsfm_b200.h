@@ -345,8 +345,8 @@ typedef struct rsfm_ranked_image {
     uint32_t nbDesc;
     const uint32_t* records;  /* optional (32-byte aligned): rsfm_ranked_pack_records output */
 } rsfm_ranked_image;
-/* Alignment (checked; RSFM_ERR_INVALID_ARG otherwise): desc, codes and buckets 16 bytes, keys 8,
- * records 32. Bucket lists are read in aligned 16-byte blocks within the lists of the tables in
+/* Alignment (checked; RSFM_ERR_INVALID_ARG otherwise): desc and records 32 bytes, codes and
+ * buckets 16, keys 8. Bucket lists are read in aligned 16-byte blocks within the lists of the tables in
  * use. */
 
 /* Packs keys, codes and squared norms into one 32-byte record per descriptor (8 x uint32:

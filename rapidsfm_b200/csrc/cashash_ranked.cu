@@ -46,11 +46,11 @@ __global__ void pack_kernel(const uint2* __restrict__ keys, const uint4* __restr
 
 // True when any of the first s key bytes of t equals q's (bytes 0-3 in .x, 4-7 in .y): the
 // candidate was already found in an earlier table. __vcmpeq4 sets 0xFF per equal byte.
-// Alignment the kernels' vector loads rely on: descriptors, codes and bucket lists 16 bytes,
-// keys 8, packed records 32.
+// Alignment the kernels' vector loads rely on: descriptors and packed records 32 bytes, codes
+// and bucket lists 16, keys 8.
 inline bool aligned(const Img& I) {
     auto a = [](const void* p, uintptr_t m) { return (reinterpret_cast<uintptr_t>(p) & (m - 1)) == 0; };
-    return a(I.desc, 16) && a(I.keys, 8) && a(I.codes, 16) && a(I.buckets, 16) && a(I.rec, 32);
+    return a(I.desc, 32) && a(I.keys, 8) && a(I.codes, 16) && a(I.buckets, 16) && a(I.rec, 32);
 }
 
 __device__ __forceinline__ bool collides_before(uint2 t, uint2 q, uint32_t s) {
@@ -347,9 +347,9 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
 // set of the topK smallest, same exact re-rank rule.
 constexpr int kThreadTopK = 12;
 
-// One 32-byte record in one load (256-bit, read-only path): each thread of a warp reads a
-// different record, so the instruction costs one L1 wavefront per thread either way, and one
-// load instead of two halves them. `p` must be 32-byte aligned (records are).
+// 32 bytes in one load (256-bit, read-only path): each thread of a warp reads a different
+// record or row, so an instruction costs one L1 wavefront per thread either way, and one load
+// instead of two halves them. `p` must be 32-byte aligned (records and rows are).
 __device__ __forceinline__ void ldg_record(const uint4* p, uint4& a, uint4& b) {
     asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
@@ -442,7 +442,7 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
     const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
     uint4 qr[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) qr[k] = __ldg(&qd[k]);
+    for (int k = 0; k < 4; ++k) ldg_record(&qd[2 * k], qr[2 * k], qr[2 * k + 1]);
     const uint32_t nq = __ldg(&Q.sqr[i]);
     uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
 #pragma unroll
@@ -452,12 +452,18 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
         const uint4* td = reinterpret_cast<const uint4*>(T.desc + size_t(jr) * 128);
         uint32_t dot = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint4 t = __ldg(&td[k]), q = qr[k];
-            dot = __dp4a(q.x, t.x, dot);
-            dot = __dp4a(q.y, t.y, dot);
-            dot = __dp4a(q.z, t.z, dot);
-            dot = __dp4a(q.w, t.w, dot);
+        for (int k = 0; k < 4; ++k) {
+            uint4 t0, t1;
+            ldg_record(&td[2 * k], t0, t1);  // 32 bytes of the row per load
+            const uint4 q0 = qr[2 * k], q1 = qr[2 * k + 1];
+            dot = __dp4a(q0.x, t0.x, dot);
+            dot = __dp4a(q0.y, t0.y, dot);
+            dot = __dp4a(q0.z, t0.z, dot);
+            dot = __dp4a(q0.w, t0.w, dot);
+            dot = __dp4a(q1.x, t1.x, dot);
+            dot = __dp4a(q1.y, t1.y, dot);
+            dot = __dp4a(q1.z, t1.z, dot);
+            dot = __dp4a(q1.w, t1.w, dot);
         }
         const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
         const uint32_t d = nq + ns - 2u * dot;

@@ -97,8 +97,8 @@ def test_new_entry_points_validate_without_gpu(rsfm):
 
 
 def test_ranked_alignment_checked_without_gpu(rsfm):
-    """The ranked matcher's vector loads need aligned arrays (descriptors, codes and bucket lists
-    16 bytes, keys 8, records 32); a misaligned array is rejected before any CUDA call."""
+    """The ranked matcher's vector loads need aligned arrays (descriptors and records 32 bytes,
+    codes and bucket lists 16, keys 8); a misaligned array is rejected before any CUDA call."""
     lib = rsfm._lib.load()
     R = rsfm._lib.RankedImage
 
@@ -109,7 +109,7 @@ def test_ranked_alignment_checked_without_gpu(rsfm):
         return R(**f)
 
     for bad in (dict(buckets=0x50004), dict(records=0x70010), dict(codes=0x30008), dict(keys=0x20004),
-                dict(desc=0x10008)):
+                dict(desc=0x10010)):
         q, t = img(), img(**bad)
         assert lib.rsfm_cashash_match_ranked(ctypes.byref(q), ctypes.byref(t), 6, 10, 4, 5,
                                              0x80000, 0x90000, 0xA0000, None, None) == 1
