@@ -395,8 +395,9 @@ typedef struct rsfm_mlp {
 } rsfm_mlp;
 
 /* Hashes nbDesc descriptors (16-byte aligned): codes = 4 x uint32 per descriptor (required, 16-byte
- * aligned), keys = the first 8 code bytes per descriptor (the 8 bucket keys; optional), outputs =
- * the 128 pre-sign values as f32 (optional, for tests). Tensor cores, fp32 accumulation. */
+ * aligned), keys = the first 8 code bytes per descriptor (the 8 bucket keys; optional, 8-byte
+ * aligned), outputs = the 128 pre-sign values as f32 (optional, for tests; 16-byte aligned).
+ * Tensor cores, fp32 accumulation. */
 int rsfm_mlp_hash(const rsfm_mlp* model, const void* desc, uint32_t nbDesc, uint8_t* keys, uint32_t* codes,
                   float* outputs, cudaStream_t stream);
 

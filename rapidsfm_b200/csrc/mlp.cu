@@ -17,11 +17,13 @@ namespace mlp {
 
 using namespace sm100;
 
-__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
 __device__ __forceinline__ float bf16_to_f(uint16_t u) { return __uint_as_float(uint32_t(u) << 16); }
+// bf16x2 of (max(a, 0), max(b, 0)), round to nearest even (negative inputs give zero).
+__device__ __forceinline__ uint32_t pack_bf16x2_relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
 
 // byte offset of 16-byte chunk c (0..7) of row r in a K-major panel with the 128-byte swizzle
 __device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
@@ -43,10 +45,11 @@ __device__ __forceinline__ void umma_f16(uint32_t d, uint64_t a, uint64_t b, uin
 // ---------------------------------------------------------------- inference
 // Persistent, one CTA per SM, 256 threads. Per 128-descriptor tile: X (u8 -> bf16, x/64 exact)
 // into smem; layer 1 = 8 UMMAs (M=128, N=256, K=16) into TMEM columns 0-255; bias + ReLU -> bf16
-// H back to smem; layer 2 = 16 UMMAs (N=128) into columns 256-383; sign bits out. Two tiles are in
-// flight: the next tile's X conversion overlaps this tile's layer 2, and this tile's layer-2
-// epilogue overlaps the next tile's layer 1.
-constexpr int kInfThreads = 256;
+// H back to smem one 64-unit K panel at a time, each panel's four layer-2 UMMAs (N=128) issued into
+// columns 256-383 as soon as it is written; sign bits out. Two tiles are in flight: the next
+// tile's X conversion overlaps this tile's layer 2, and this tile's layer-2 epilogue overlaps the
+// next tile's layer 1.
+constexpr int kInfThreads = 512;
 struct InfSmem {
     uint8_t w1[2][256 * 128];  // K panels of W1 (256 rows = outputs, 64 inputs per panel)
     uint8_t w2[4][128 * 128];  // K panels of W2 (128 rows, 64 hidden per panel)
@@ -90,22 +93,22 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem;
-    const uint32_t q = warp & 3u, half = warp >> 2;
+    // warp (q, part): TMEM lane quarter q (rows 32q..), part = which quarter of the columns
+    const uint32_t q = warp & 3u, part = warp >> 2;
     const uint32_t laneBase = (32u * q) << 16;
     const uint32_t row = 32u * q + lane;
 
-    // Thread t converts half t%2 of row t/2 (64 bytes -> 64 bf16 = one panel row). The raw bytes of
-    // a tile are loaded into registers one tile ahead (fetch_x), so their DRAM latency overlaps
-    // the previous tile's work instead of sitting between the two layers' MMAs.
-    uint4 raw[4];
+    // Thread t converts quarter t%4 of row t/4 (32 bytes -> 32 bf16, half a panel row). The raw
+    // bytes of a tile are loaded into registers one tile ahead (fetch_x), so their DRAM latency
+    // overlaps the previous tile's work instead of sitting between the two layers' MMAs.
+    uint4 raw[2];
     auto fetch_x = [&](uint32_t tile) {
-        const uint32_t i = tile * 128u + (tid >> 1);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) raw[k] = make_uint4(0, 0, 0, 0);
+        const uint32_t i = tile * 128u + (tid >> 2);
+        raw[0] = raw[1] = make_uint4(0, 0, 0, 0);
         if (i < n) {
-            const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 64 * (tid & 1u));
-#pragma unroll
-            for (int k = 0; k < 4; ++k) raw[k] = __ldg(&src[k]);
+            const uint4* src = reinterpret_cast<const uint4*>(desc + size_t(i) * 128 + 32 * (tid & 3u));
+            raw[0] = __ldg(&src[0]);
+            raw[1] = __ldg(&src[1]);
         }
     };
     // x / 64 in bf16, exact for x in 0..255: the float with bits 0x4B0000xx is 2^23 + x, so
@@ -116,16 +119,16 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
         return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632u);
     };
     auto convert_x = [&]() {
-        const uint32_t r = tid >> 1, hh = tid & 1u;
+        const uint32_t r = tid >> 2, qq = tid & 3u;  // input dims [32 qq, +32): panel qq / 2
         const uint32_t* w = reinterpret_cast<const uint32_t*>(raw);
 #pragma unroll
-        for (uint32_t c = 0; c < 8; ++c) {
+        for (uint32_t c = 0; c < 4; ++c) {
             uint4 o;
             o.x = bf16x2_of_bytes(w[2 * c], 0, 1);
             o.y = bf16x2_of_bytes(w[2 * c], 2, 3);
             o.z = bf16x2_of_bytes(w[2 * c + 1], 0, 1);
             o.w = bf16x2_of_bytes(w[2 * c + 1], 2, 3);
-            *reinterpret_cast<uint4*>(S.x[hh] + sw128(r, c)) = o;
+            *reinterpret_cast<uint4*>(S.x[qq >> 1] + sw128(r, 4u * (qq & 1u) + c)) = o;
         }
         fence_proxy_async_smem();
     };
@@ -139,18 +142,6 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
                 umma_f16(tmem, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 256), s);
             }
             umma_commit(&S.mma1);
-        }
-    };
-    auto issue_layer2 = [&]() {
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll
-            for (uint32_t s = 0; s < 16; ++s) {
-                const uint32_t pa = smem_u32(S.h[s >> 2]) + 32u * (s & 3u);
-                const uint32_t pb = smem_u32(S.w2[s >> 2]) + 32u * (s & 3u);
-                umma_f16(tmem + 256u, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 128), s);
-            }
-            umma_commit(&S.mma2);
         }
     };
 
@@ -169,31 +160,46 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
         mbar_wait(&S.mma1, ph1, err, kDevTimeoutAccFull);
         ph1 ^= 1u;
         tc_fence_after();
-        // ---- layer-1 epilogue: warp (q, half) handles rows 32q.. and hidden [128 half, +128)
+        // ---- layer-1 epilogue, two K panels (128 hidden units) of H at a time: warp (q, part)
+        // handles rows 32q.. and hidden units [128 g + 32 part, +32) (panel 2g + part / 2). As
+        // soon as a pair of panels is complete its eight layer-2 UMMAs are issued, so layer 2 runs
+        // during the rest of this epilogue instead of after it.
 #pragma unroll 1
-        for (uint32_t ch = 0; ch < 4; ++ch) {
-            const uint32_t col = 128u * half + 32u * ch;
+        for (uint32_t g = 0; g < 2; ++g) {
+            const uint32_t col = 128u * g + 32u * part;
             uint32_t v[32];
             tmem_ld32(tmem + laneBase + col, v);
             tmem_wait_ld();
 #pragma unroll
             for (uint32_t c8 = 0; c8 < 4; ++c8) {
+                const float4 ba = *reinterpret_cast<const float4*>(&S.b1[col + 8 * c8]);
+                const float4 bb = *reinterpret_cast<const float4*>(&S.b1[col + 8 * c8 + 4]);
+                const float bs[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
                 float f[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) f[k] = fmaxf(__uint_as_float(v[8 * c8 + k]) + S.b1[col + 8 * c8 + k], 0.f);
-                uint4 o;
-                o.x = pack_bf16x2(f[0], f[1]);
-                o.y = pack_bf16x2(f[2], f[3]);
-                o.z = pack_bf16x2(f[4], f[5]);
-                o.w = pack_bf16x2(f[6], f[7]);
+                for (int k = 0; k < 8; ++k) f[k] = __uint_as_float(v[8 * c8 + k]) + bs[k];
+                uint4 o;  // bias + ReLU, rounded to bf16
+                o.x = pack_bf16x2_relu(f[0], f[1]);
+                o.y = pack_bf16x2_relu(f[2], f[3]);
+                o.z = pack_bf16x2_relu(f[4], f[5]);
+                o.w = pack_bf16x2_relu(f[6], f[7]);
                 const uint32_t k0 = col + 8 * c8;  // hidden index of the chunk
                 *reinterpret_cast<uint4*>(S.h[k0 >> 6] + sw128(row, (k0 >> 3) & 7u)) = o;
             }
+            tc_fence_before();
+            fence_proxy_async_smem();
+            __syncthreads();  // panels 2g, 2g+1 of H complete (after g = 1: TMEM 0-255 read, X free)
+            if (tid == 0) {
+                tc_fence_after();
+#pragma unroll
+                for (uint32_t s = 8 * g; s < 8 * g + 8; ++s) {
+                    const uint32_t pa = smem_u32(S.h[s >> 2]) + 32u * (s & 3u);
+                    const uint32_t pb = smem_u32(S.w2[s >> 2]) + 32u * (s & 3u);
+                    umma_f16(tmem + 256u, umma_desc_k_sw128(pa), umma_desc_k_sw128(pb), idesc_bf16_f32(128, 128), s);
+                }
+                if (g == 1) umma_commit(&S.mma2);
+            }
         }
-        tc_fence_before();
-        fence_proxy_async_smem();
-        __syncthreads();  // H complete; TMEM columns 0-255 read; X free (layer 1 done)
-        issue_layer2();
         if (hasNext) {
             convert_x();  // tile `next`, fetched one tile ago
             if (next + gridDim.x < (n + 127u) / 128u) fetch_x(next + gridDim.x);
@@ -205,27 +211,34 @@ infer_kernel(const uint16_t* __restrict__ w1, const float* __restrict__ b1, cons
         mbar_wait(&S.mma2, ph2, err, kDevTimeoutAccFull);
         ph2 ^= 1u;
         tc_fence_after();
-        // ---- layer-2 epilogue: outputs [64 half, +64) -> 64 sign bits
+        // ---- layer-2 epilogue: outputs [32 part, +32) -> 32 sign bits
         const uint32_t i = tile * 128u + row;
-        uint32_t bits[2];
-#pragma unroll
-        for (uint32_t ch = 0; ch < 2; ++ch) {
-            const uint32_t col = 64u * half + 32u * ch;
+        {
+            const uint32_t col = 32u * part;
             uint32_t v[32];
             tmem_ld32(tmem + laneBase + 256u + col, v);
             tmem_wait_ld();
+            // t = -(acc + b2) in one rounding (round to nearest is symmetric, and an exact zero
+            // sum is +0), so the sign bit of t is exactly [o > 0]; funnel shifts collect the 32
+            // sign bits, output 31 first.
             uint32_t w = 0;
 #pragma unroll
-            for (int k = 0; k < 32; ++k) {
-                const float o = __uint_as_float(v[k]) + S.b2[col + k];
-                w |= (o > 0.f ? 1u : 0u) << k;
-                if (out && i < n) out[size_t(i) * 128 + col + k] = o;
+            for (int k = 31; k >= 0; --k) {
+                const float t = __fsub_rn(-__uint_as_float(v[k]), S.b2[col + k]);
+                w = __funnelshift_l(__float_as_uint(t), w, 1);
+                v[k] = __float_as_uint(-t);
             }
-            bits[ch] = w;
-        }
-        if (i < n) {
-            *reinterpret_cast<uint2*>(codes + size_t(i) * 4 + 2 * half) = make_uint2(bits[0], bits[1]);
-            if (half == 0 && keys) *reinterpret_cast<uint2*>(keys + size_t(i) * 8) = make_uint2(bits[0], bits[1]);
+            if (i < n) {
+                codes[size_t(i) * 4 + part] = w;
+                if (part < 2 && keys) reinterpret_cast<uint32_t*>(keys + size_t(i) * 8)[part] = w;
+                if (out) {
+                    float4* dst = reinterpret_cast<float4*>(out + size_t(i) * 128 + col);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        dst[k] = make_float4(__uint_as_float(v[4 * k]), __uint_as_float(v[4 * k + 1]),
+                                             __uint_as_float(v[4 * k + 2]), __uint_as_float(v[4 * k + 3]));
+                }
+            }
         }
         tc_fence_before();
         __syncthreads();  // TMEM columns 256-383 read; H may be overwritten (layer 2 done)
@@ -586,7 +599,7 @@ extern "C" int rsfm_mlp_hash(const rsfm_mlp* m, const void* desc, uint32_t nbDes
     if (!m || !m->w1 || !m->b1 || !m->w2 || !m->b2) return RSFM_ERR_INVALID_ARG;
     if (nbDesc == 0) return RSFM_OK;
     if (!desc || !codes || (reinterpret_cast<uintptr_t>(desc) & 15u) || (reinterpret_cast<uintptr_t>(codes) & 15u) ||
-        (reinterpret_cast<uintptr_t>(keys) & 7u))
+        (reinterpret_cast<uintptr_t>(keys) & 7u) || (reinterpret_cast<uintptr_t>(outputs) & 15u))
         return RSFM_ERR_INVALID_ARG;
     const size_t smem = sizeof(mlp::InfSmem) + 1024;
     {
