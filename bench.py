@@ -841,19 +841,25 @@ def run_training(dev, stream, batch=4096, steps=300, seed=7):
         sel = torch.randint(0, len(A), (batch,), device=dev, generator=g)
         ip = P[sel].int()
         inn = ((ip // n) * n + torch.randint(0, n, (batch,), device=dev, generator=g)).int()
-        tr.step(Q, A[sel].int(), T, ip, T, inn, stream=stream)
+        tr.step(Q, A[sel].int(), T, ip, T, inn)
 
+    # as the training loop runs it: a few eager steps, then one step (sampling included) replayed
+    # from a CUDA graph; also the eager step for comparison
     with torch.cuda.stream(stream):
-        ms = _events_ms(one, steps, stream)
+        ms_eager = _events_ms(one, 50, stream)
+        graph = lh.StepGraph(one, generators=(g,))
+        ms = _events_ms(graph.replay, steps, stream)
         first = float(tr.loss.item())
         for _ in range(50):
-            one()
+            graph.replay()
         last = float(tr.loss.item())
+    del graph
     tr.close()
     flop = TRAIN_FLOP_PER_ROW * 3 * batch
     tf = flop / (ms * 1e-3) / 1e12
     bf16 = _peaks().get("bf16_tflops")
-    return {"batch": batch, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "projected_20k_steps_s": 20000 * ms / 1e3,
+    return {"batch": batch, "ms_per_step": ms, "ms_per_step_eager": ms_eager, "steps_per_s": 1e3 / ms,
+            "projected_20k_steps_s": 20000 * ms / 1e3,
             "contraction_flop_per_step": flop, "TFLOP/s": tf, "frac_of_measured_bf16": tf / bf16 if bf16 else None,
             "loss_first_last": [first, last], "timed_steps": steps}
 

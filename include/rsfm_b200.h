@@ -507,7 +507,9 @@ int rsfm_cashash_reference_weights(int8_t* weightsHost, int32_t* biasBaseHost);
  * negative), z = tanh(o): max(0, margin + |z_a - z_p|^2/4 - |z_a - z_n|^2/4), averaged over the
  * batch; gradients pass the bf16 rounding of h as the identity. A step gathers rows ia/ip/in of
  * the descriptor sets a/p/n (device arrays of `batch` indices), computes the gradients and applies
- * Adam, all enqueued on `stream` (no host synchronization). */
+ * Adam, all enqueued on `stream` (no host synchronization, no allocation, and no per-step host
+ * arguments: the Adam step count lives on the device, so a step captured in a CUDA graph can be
+ * replayed; pass the same index buffers, refilled between replays). */
 typedef struct rsfm_mlp_trainer rsfm_mlp_trainer;
 int rsfm_mlp_trainer_create(const float* initParamsHost, uint32_t batch, float lr, float margin,
                             rsfm_mlp_trainer** trainer);

@@ -508,11 +508,17 @@ __global__ void colsum_kernel(const float* __restrict__ in, uint32_t rows, uint3
 }
 
 // Adam on fp32 masters; writes the bf16 copy when `bf` is non-null.
-__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m1,
-                            float* __restrict__ m2, uint16_t* __restrict__ bf, uint32_t n, float lr, float b1c,
-                            float b2c) {
+// All four parameter groups in one launch (w1 | b1 | w2 | b2, the parameter block's layout), with
+// the bias corrections 1 - beta^t of step t = *step + 1 computed on the device, so a step needs
+// no per-step host arguments (it can be replayed from a CUDA graph). bf16 copies of w1 and w2.
+__global__ void adam_all_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m1,
+                                float* __restrict__ m2, uint16_t* __restrict__ bw1, uint16_t* __restrict__ bw2,
+                                uint32_t nW1, uint32_t nB1, uint32_t nW2, uint32_t nB2, float lr,
+                                const uint32_t* __restrict__ step) {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n) return;
+    if (x >= nW1 + nB1 + nW2 + nB2) return;
+    const float t = float(*step + 1u);
+    const float b1c = 1.f - powf(0.9f, t), b2c = 1.f - powf(0.999f, t);
     const float gi = g[x];
     const float a = 0.9f * m1[x] + 0.1f * gi;
     const float b = 0.999f * m2[x] + 0.001f * gi * gi;
@@ -520,11 +526,13 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
     m2[x] = b;
     const float v = w[x] - lr * (a / b1c) / (sqrtf(b / b2c) + 1e-8f);
     w[x] = v;
-    if (bf) {
-        const __nv_bfloat16 bv = __float2bfloat16_rn(v);
-        bf[x] = *reinterpret_cast<const uint16_t*>(&bv);
-    }
+    const __nv_bfloat16 bv = __float2bfloat16_rn(v);
+    if (x < nW1) bw1[x] = *reinterpret_cast<const uint16_t*>(&bv);
+    const uint32_t o2 = nW1 + nB1;
+    if (x >= o2 && x < o2 + nW2) bw2[x - o2] = *reinterpret_cast<const uint16_t*>(&bv);
 }
+
+__global__ void step_increment_kernel(uint32_t* step) { *step += 1u; }
 
 __global__ void f32_to_bf16_kernel(const float* __restrict__ in, uint16_t* __restrict__ out, uint32_t n) {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -575,6 +583,7 @@ struct rsfm_mlp_trainer {
     int kind = 0;        // loss: 0 = triplet hinge, 1 = bucket-key loss + hinge on the code channels
     float lambda = 0.f;  // weight of the negatives' key agreement (kind 1)
     uint32_t step = 0;
+    uint32_t* stepDev = nullptr;  // steps taken, on the device (read by the Adam kernel)
     rsfm_mlp model{};
     // fp32 masters, Adam moments, gradients
     float *w1 = nullptr, *w2 = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;
@@ -638,7 +647,7 @@ extern "C" int rsfm_mlp_trainer_create(const float* initParams, uint32_t batch, 
               cudaMalloc(&t->dOT, 128 * L * 2) == cudaSuccess && cudaMalloc(&t->dh, R * 256 * 4) == cudaSuccess &&
               cudaMalloc(&t->dhT, 256 * L * 2) == cudaSuccess && cudaMalloc(&t->loss, 4) == cudaSuccess &&
               cudaMalloc(&t->bw1, kNW1 * 2) == cudaSuccess && cudaMalloc(&t->bw2, kNW2 * 2) == cudaSuccess &&
-              cudaMalloc(&t->w2T, kNW2 * 2) == cudaSuccess;
+              cudaMalloc(&t->w2T, kNW2 * 2) == cudaSuccess && cudaMalloc(&t->stepDev, 4) == cudaSuccess;
     if (!ok) {
         rsfm_mlp_trainer_destroy(t);
         return RSFM_ERR_CUDA;
@@ -649,7 +658,8 @@ extern "C" int rsfm_mlp_trainer_create(const float* initParams, uint32_t batch, 
     t->model.w2 = t->bw2;
     t->model.b2 = t->w2 + kNW2;
     if (cudaMemcpy(t->w1, initParams, kNP * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(t->m1, 0, kNP * 4) != cudaSuccess || cudaMemset(t->m2, 0, kNP * 4) != cudaSuccess) {
+        cudaMemset(t->m1, 0, kNP * 4) != cudaSuccess || cudaMemset(t->m2, 0, kNP * 4) != cudaSuccess ||
+        cudaMemset(t->stepDev, 0, 4) != cudaSuccess) {
         rsfm_mlp_trainer_destroy(t);
         return RSFM_ERR_CUDA;
     }
@@ -775,20 +785,13 @@ extern "C" int rsfm_mlp_trainer_step(rsfm_mlp_trainer* t, const void* a, const u
     int st = trainer_grads(t, a, ia, p, ip, n, in_, stream);
     if (st) return st;
     t->step += 1;
-    const float b1c = 1.f - powf(0.9f, float(t->step)), b2c = 1.f - powf(0.999f, float(t->step));
     using namespace mlp;
-    adam_kernel<<<(kNW1 + 255) / 256, 256, 0, stream>>>(t->w1, t->g, t->m1, t->m2, t->bw1,
-                                                       kNW1, t->lr, b1c, b2c);
-    adam_kernel<<<1, 256, 0, stream>>>(t->w1 + kNW1, t->g + kNW1, t->m1 + kNW1, t->m2 + kNW1, nullptr, kNB1, t->lr,
-                                       b1c, b2c);
-    const size_t o2 = kNW1 + kNB1;
-    adam_kernel<<<(kNW2 + 255) / 256, 256, 0, stream>>>(t->w1 + o2, t->g + o2, t->m1 + o2, t->m2 + o2,
-                                                       t->bw2, kNW2, t->lr, b1c, b2c);
-    const size_t o3 = o2 + kNW2;
-    adam_kernel<<<1, 128, 0, stream>>>(t->w1 + o3, t->g + o3, t->m1 + o3, t->m2 + o3, nullptr, kNB2, t->lr, b1c, b2c);
+    adam_all_kernel<<<(kNP + 255) / 256, 256, 0, stream>>>(t->w1, t->g, t->m1, t->m2, t->bw1, t->bw2, kNW1, kNB1,
+                                                          kNW2, kNB2, t->lr, t->stepDev);
+    step_increment_kernel<<<1, 1, 0, stream>>>(t->stepDev);
     transpose_bf16_kernel<<<dim3(256 / 32, 128 / 32), dim3(32, 8), 0, stream>>>(t->w2, 128, 256, t->w2T, 128);
     RSFM_CUDA_TRY(cudaGetLastError());
-    launch_count_add(5);
+    launch_count_add(3);
     if (lossDevice) RSFM_CUDA_TRY(cudaMemcpyAsync(lossDevice, t->loss, 4, cudaMemcpyDeviceToDevice, stream));
     return RSFM_OK;
 }
@@ -807,7 +810,7 @@ extern "C" int rsfm_mlp_trainer_destroy(rsfm_mlp_trainer* t) {
                     static_cast<void*>(t->o), static_cast<void*>(t->dO), static_cast<void*>(t->dOb),
                     static_cast<void*>(t->dOT), static_cast<void*>(t->dh), static_cast<void*>(t->dhT),
                     static_cast<void*>(t->loss), static_cast<void*>(t->bw1), static_cast<void*>(t->bw2),
-                    static_cast<void*>(t->w2T)})
+                    static_cast<void*>(t->w2T), static_cast<void*>(t->stepDev)})
         if (p) cudaFree(p);
     delete t;
     return RSFM_OK;

@@ -128,6 +128,30 @@ class Trainer:
             pass
 
 
+class StepGraph:
+    """`body` (one trainer step, including the caller's sampling of its index tensors on the
+    device) captured once in a CUDA graph and replayed: one launch per step instead of one per
+    kernel. `generators`: torch generators that `body` draws from (their state advances on every
+    replay). `body` runs `warmup` times eagerly first (lazy initialisation happens outside the
+    capture); tensors it allocates during the capture keep their addresses on every replay."""
+
+    def __init__(self, body, generators=(), warmup=3):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                body()
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        for g in generators:
+            self.graph.register_generator_state(g)
+        with torch.cuda.graph(self.graph):
+            body()
+
+    def replay(self):
+        self.graph.replay()
+
+
 def center_output_bias(params, hasher_factory, sample_desc):
     """Sets b2 so every output bit splits `sample_desc` in half (median of o before the bias)."""
     p = np.array(params, dtype=np.float32, copy=True)
@@ -185,13 +209,23 @@ def train_from_brute_force(n_pairs=200, n=8192, steps=20000, batch=4096, lr=1e-3
     tr = Trainer(params, batch, lr=lr, margin=margin, loss=loss, lam=lam)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    for s in range(steps):
+    def one():
         sel = torch.randint(0, len(A), (batch,), device=device, generator=g)
         ip = P[sel].int()
         inn = ((ip // n) * n + torch.randint(0, n, (batch,), device=device, generator=g)).int()
         tr.step(Q, A[sel].int(), T, ip, T, inn)
-        if log and (s % 1000 == 0 or s == steps - 1):
-            log(f"step {s} loss {tr.loss.item():.4f}")
+
+    # the first steps run eagerly (warm-up), the rest from a CUDA graph of one step
+    warm = 3
+    if steps > warm:
+        graph = StepGraph(one, generators=(g,), warmup=warm)
+        for s in range(warm, steps):
+            graph.replay()
+            if log and (s % 1000 == 0 or s == steps - 1):
+                log(f"step {s} loss {tr.loss.item():.4f}")
+    else:
+        for _ in range(steps):
+            one()
     out = tr.params()
     tr.close()
     if timings is not None:

@@ -95,3 +95,31 @@ def test_trainer_reduces_loss(rsfm):
     torch.cuda.synchronize()
     assert keys.shape == (4096, 8)
     tr.close()
+
+
+def test_trainer_step_replayed_from_graph_matches_eager(rsfm):
+    """rsfm_mlp_trainer_step keeps no per-step host arguments (the Adam step count is on the
+    device), so a step captured in a CUDA graph and replayed gives the parameters of eager steps on
+    the same batches (up to the order of the split-K gradient atomics)."""
+    from rapidsfm_b200 import learned_hash as lh
+    B = 256
+    q, t, truth = synth.make_pair(2000, 2000, 0.6, 8.0, seed=5)
+    pos = np.nonzero(truth >= 0)[0][:B]
+    Q, T = _dev(q), _dev(t)
+    ia = _dev(truth[pos].astype(np.int32))
+    ip = _dev(pos.astype(np.int32))
+    inn = _dev(np.random.default_rng(3).integers(0, len(t), B).astype(np.int32))
+    p0 = _params(7)
+    eager = lh.Trainer(p0, B, margin=8.0)
+    graphed = lh.Trainer(p0, B, margin=8.0)
+    for _ in range(7):
+        eager.step(Q, ia, T, ip, T, inn)
+    sg = lh.StepGraph(lambda: graphed.step(Q, ia, T, ip, T, inn), warmup=3)  # 3 eager steps
+    for _ in range(4):
+        sg.replay()
+    torch.cuda.synchronize()
+    pe, pg = eager.params(), graphed.params()
+    assert not np.array_equal(pe, p0)
+    np.testing.assert_allclose(pg, pe, rtol=1e-4, atol=1e-6)
+    eager.close()
+    graphed.close()
