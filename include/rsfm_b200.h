@@ -321,7 +321,9 @@ int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs, uint32_t 
 
 /* The same matching for a batch of pairs that is matched repeatedly (no reference counterpart):
  * _create builds the work list once (it synchronizes `stream` once, to size the list; the images
- * and result arrays the pairs point to must stay valid while the batch is used); each _launch
+ * and result arrays the pairs point to must stay valid while the batch is used, and _create keeps
+ * a copy of the images' squared norms in bucket-list order, so their bucket lists and norms must
+ * not change afterwards); each _launch
  * re-initialises the results and runs the matching kernel asynchronously on `stream`, with no
  * allocation and no host synchronization, so it can be captured in a CUDA graph. Launches of one
  * batch that overlap on the GPU write the same result arrays: order them on one stream. */

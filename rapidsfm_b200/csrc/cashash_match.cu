@@ -19,6 +19,7 @@
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
+#include <unordered_map>
 #include <vector>
 
 namespace rsfm_b200 {
@@ -73,9 +74,6 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool va
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
 
 // Ascending sort of one value per lane (bitonic network over the warp).
 __device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
@@ -90,6 +88,27 @@ __device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
         }
     }
     return v;
+}
+
+// Ascending order of one (key, value) per lane by key, unless the keys already are ascending.
+__device__ __forceinline__ void sort_if_needed(uint32_t& key, uint32_t& val, uint32_t lane) {
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (__all_sync(0xffffffffu, lane == 0 || prev <= key)) return;
+#pragma unroll
+    for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint32_t ok = __shfl_xor_sync(0xffffffffu, key, stride);
+            const uint32_t ov = __shfl_xor_sync(0xffffffffu, val, stride);
+            const bool up = ((lane & size) == 0);
+            const bool lower = ((lane & stride) == 0);
+            const bool takeOther = (lower == up) ? (ok < key) : (ok > key);
+            if (takeOther) {
+                key = ok;
+                val = ov;
+            }
+        }
+    }
 }
 
 __global__ void init_kernel(const __grid_constant__ Params P, uint32_t nTrain, uint32_t maxQ,
@@ -308,6 +327,10 @@ struct PairDev {
     unsigned long long* qBest;
     unsigned long long* tBest;
     uint32_t nQ, nT;
+    // the images' squared norms in bucket-list order: qNorms[e] = q.sqr[q.buckets[e]] for every
+    // list position e (filled by norm_lists_kernel), so a segment's norms are one coalesced load
+    const uint32_t* qNorms;
+    const uint32_t* tNorms;
 };
 
 __global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* counter) {
@@ -329,9 +352,26 @@ __global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* c
 struct SubItem {
     const uint32_t* qList;  // first query member of the segment (bucket list of the query image)
     const uint32_t* tList;  // first train member of the segment
+    const uint32_t* qNorm;  // their squared norms, same positions
+    const uint32_t* tNorm;
     uint32_t pair;
     uint32_t counts;        // query members in the segment | train members << 16 (each 1..32)
 };
+
+// One image's norm list: out[e] = sqr[buckets[e]] for e < count (member indices checked).
+struct NormListJob {
+    const uint32_t* buckets;
+    const uint32_t* sqr;
+    uint32_t* out;
+    uint32_t count, n;
+};
+__global__ void norm_lists_kernel(const NormListJob* __restrict__ jobs) {
+    const NormListJob J = jobs[blockIdx.y];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < J.count; e += gridDim.x * blockDim.x) {
+        const uint32_t m = J.buckets[e];
+        J.out[e] = m < J.n ? J.sqr[m] : kBigNorm;
+    }
+}
 
 // Warp-specialised persistent kernel (one CTA per SM): producer warps gather the rows of a unit
 // (four sub-items) into a ring of shared-memory stages with cp.async, one thread issues the UMMAs
@@ -482,8 +522,8 @@ __global__ void subitem_expand_kernel(const PairDev* __restrict__ pairs, uint32_
         const uint32_t segT = (nT + 31u) / 32u;
         for (uint32_t x = 0; x < c; ++x) {
             const uint32_t m0 = (x / segT) * 32u, c0 = (x % segT) * 32u;
-            subs[o + x] = SubItem{P.q.buckets + qb + m0, P.t.buckets + tb + c0, it >> 11,
-                                  min(nQ - m0, 32u) | (min(nT - c0, 32u) << 16)};
+            subs[o + x] = SubItem{P.q.buckets + qb + m0, P.t.buckets + tb + c0, P.qNorms + qb + m0,
+                                  P.tNorms + tb + c0, it >> 11, min(nQ - m0, 32u) | (min(nT - c0, 32u) << 16)};
         }
     }
 }
@@ -528,30 +568,30 @@ __global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const Pa
         const uint32_t pw = warp - (kSubMmaWarp + 1u), j = pw & 3u;
         constexpr uint32_t kStep = kSubProducers / 4;
         const uint8_t* dummy = reinterpret_cast<const uint8_t*>(subs);  // zero-byte cp.async source
-        const SubItem none{nullptr, nullptr, 0u, 0u};
+        const SubItem none{nullptr, nullptr, nullptr, nullptr, 0u, 0u};
         auto record = [&](uint32_t i) {
             const uint32_t si = 4u * (blockIdx.x + i * gridDim.x) + j;
             return i < nLocal && si < nSubs ? subs[si] : none;
         };
-        // One sub-item's members (unsorted, one per lane) and its pair's pointers.
+        // One sub-item's members and their norms (list order, one per lane) and its pair's
+        // pointers.
         struct Members {
-            uint32_t q, t;
+            uint32_t q, t, nq, nt;
             const uint8_t* qd;
             const uint8_t* td;
-            const uint32_t* qs;
-            const uint32_t* ts;
             unsigned long long* qb;
             unsigned long long* tb;
         };
         auto members = [&](const SubItem& r) {
             const PairDev& P = pairs[r.pair];
             Members m;
-            m.q = lane < (r.counts & 0xFFFFu) ? __ldg(&r.qList[lane]) : kNoRow;
-            m.t = lane < (r.counts >> 16) ? __ldg(&r.tList[lane]) : kNoRow;
+            const bool hq = lane < (r.counts & 0xFFFFu), ht = lane < (r.counts >> 16);
+            m.q = hq ? __ldg(&r.qList[lane]) : kNoRow;
+            m.t = ht ? __ldg(&r.tList[lane]) : kNoRow;
+            m.nq = hq ? __ldg(&r.qNorm[lane]) : kBigNorm;
+            m.nt = ht ? __ldg(&r.tNorm[lane]) : kBigNorm;
             m.qd = P.q.desc;
             m.td = P.t.desc;
-            m.qs = P.q.sqr;
-            m.ts = P.t.sqr;
             m.qb = r.counts ? P.qBest : nullptr;
             m.tb = r.counts ? P.tBest : nullptr;
             return m;
@@ -565,15 +605,19 @@ __global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const Pa
         for (; i < nLocal; i += kStep) {
             const SubItem r2 = record(i + 2 * kStep);
             const Members nxt = members(r1);
-            const uint32_t q = warp_sort(cur.q, lane), t = warp_sort(cur.t, lane);
+            // rows in ascending member order (ties resolve by position); lists built by this
+            // library already are, others are sorted here with their norms
+            uint32_t q = cur.q, t = cur.t, nq = cur.nq, nt = cur.nt;
+            sort_if_needed(q, nq, lane);
+            sort_if_needed(t, nt, lane);
             const uint32_t stg = i % kSubStages;
             mbar_wait_backoff(&S.empty[stg], ((i / kSubStages) & 1u) ^ 1u, err, kDevTimeoutTmaEmpty, 256u);
             SubStage& T = S.st[stg];
             const uint32_t row = 32u * j + lane;
             T.rowQ[row] = q;
             T.colT[row] = t;
-            if (q != kNoRow) cp_async4(&T.rowNA[row], cur.qs + q); else T.rowNA[row] = kBigNorm;
-            if (t != kNoRow) cp_async4(&T.colNB[row], cur.ts + t); else T.colNB[row] = kBigNorm;
+            T.rowNA[row] = nq;
+            T.colNB[row] = nt;
             if (lane == 0) {
                 T.qBest[j] = cur.qb;
                 T.tBest[j] = cur.tb;
@@ -590,7 +634,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const Pa
                            tr != kNoRow);
             }
             mbar_arrive(&S.full[stg]);                // the records above (release)
-            cp_async_mbar_arrive_noinc(&S.full[stg]);  // rows and norms, when they have landed
+            cp_async_mbar_arrive_noinc(&S.full[stg]);  // the rows, when they have landed
             cur = nxt;
             r1 = r2;
         }
@@ -778,6 +822,7 @@ extern "C" int rsfm_cashash_find_best_match(const rsfm_cashash_image* queries, c
 // `stream` with one read-back of the size (the builder synchronizes the stream once).
 struct FbmWork {
     chm::PairDev* table = nullptr;
+    uint32_t* norms = nullptr;  // the images' norm lists (see PairDev)
     uint32_t* counter = nullptr;
     uint32_t* total = nullptr;  // device: number of sub-items
     chm::SubItem* subs = nullptr;
@@ -804,6 +849,54 @@ static int fbm_table(const rsfm_cashash_pair* pairs, uint32_t nbPairs, std::vect
         d.nQ = in.querySize;
         d.nT = in.trainSize;
         maxN = std::max(maxN, std::max(d.nQ, d.nT));
+    }
+    return RSFM_OK;
+}
+
+// The distinct images of the pairs (by bucket array) and their norm lists: sets the pairs' qNorms /
+// tNorms to base + offset once `base` is known. Lists are read at positions below 8 n with
+// per-scheme lists and below n with the reference's indexing.
+static void fbm_norm_jobs(std::vector<chm::PairDev>& host, uint32_t schemeOffset, std::vector<chm::NormListJob>& jobs,
+                          std::vector<std::pair<uint32_t, size_t>>& slots, size_t& entries) {
+    std::unordered_map<const uint32_t*, size_t> seen;  // bucket array -> job
+    jobs.clear();
+    slots.assign(host.size(), {0u, 0u});
+    entries = 0;
+    auto job_of = [&](const chm::ImageDev& m, uint32_t n) -> size_t {
+        const auto it = seen.find(m.buckets);
+        if (it != seen.end()) return it->second;
+        const uint32_t count = schemeOffset ? 8u * n : n;
+        jobs.push_back(chm::NormListJob{m.buckets, m.sqr, reinterpret_cast<uint32_t*>(entries * 4), count, n});
+        entries += (size_t(count) + 63) & ~size_t(63);
+        seen.emplace(m.buckets, jobs.size() - 1);
+        return jobs.size() - 1;
+    };
+    for (size_t p = 0; p < host.size(); ++p) {
+        chm::PairDev& d = host[p];
+        d.qNorms = d.tNorms = nullptr;
+        if (!d.nQ || !d.nT) continue;
+        slots[p] = {uint32_t(job_of(d.q, d.nQ)) + 1u, job_of(d.t, d.nT) + 1u};
+    }
+}
+// Points the jobs and the pairs at the norm buffer `base`.
+static void fbm_norm_bind(std::vector<chm::PairDev>& host, std::vector<chm::NormListJob>& jobs,
+                          const std::vector<std::pair<uint32_t, size_t>>& slots, uint32_t* base) {
+    for (auto& j : jobs) j.out = base + reinterpret_cast<uintptr_t>(j.out) / 4;
+    for (size_t p = 0; p < host.size(); ++p) {
+        if (!slots[p].first) continue;
+        host[p].qNorms = jobs[slots[p].first - 1].out;
+        host[p].tNorms = jobs[slots[p].second - 1].out;
+    }
+}
+static int fbm_norm_fill(const chm::NormListJob* dJobs, const std::vector<chm::NormListJob>& jobs, cudaStream_t stream) {
+    uint32_t maxCount = 0;
+    for (const auto& j : jobs) maxCount = std::max(maxCount, j.count);
+    const uint32_t bx = std::min<uint32_t>((maxCount + 255) / 256, 64u);
+    for (size_t j0 = 0; j0 < jobs.size(); j0 += 65535) {
+        const uint32_t ny = uint32_t(std::min<size_t>(65535, jobs.size() - j0));
+        chm::norm_lists_kernel<<<dim3(bx, ny), 256, 0, stream>>>(dJobs + j0);
+        RSFM_CUDA_TRY(cudaGetLastError());
+        launch_count_add(1);
     }
     return RSFM_OK;
 }
@@ -866,22 +959,37 @@ extern "C" int rsfm_cashash_find_best_match_pairs(const rsfm_cashash_pair* pairs
     if (st != RSFM_OK) return st;
     W.nPairs = nbPairs;
     W.schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+    std::vector<chm::NormListJob> jobs;
+    std::vector<std::pair<uint32_t, size_t>> slots;
+    size_t entries = 0;
+    fbm_norm_jobs(host, W.schemeOffset, jobs, slots, entries);
     cudaMemPool_t pool = nullptr;
     st = scratch_pool(&pool);
     if (st != RSFM_OK) return st;
     const uint32_t nItems = nbPairs * 2048u;
-    const size_t tableBytes = sizeof(chm::PairDev) * nbPairs;
+    const size_t tableBytes = (sizeof(chm::PairDev) * nbPairs + 255) & ~size_t(255);
+    const size_t jobBytes = (sizeof(chm::NormListJob) * jobs.size() + 255) & ~size_t(255);
+    const size_t normBytes = entries * 4;
     const size_t offBytes = (size_t(nItems) + 1) * 4, sumBytes = (size_t(nItems) / 1024 + 2) * 4;
     uint8_t* scratch = nullptr;
     RSFM_CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch),
-                                          256 + tableBytes + offBytes + sumBytes + 256, pool, stream));
+                                          256 + tableBytes + jobBytes + normBytes + offBytes + sumBytes + 256, pool,
+                                          stream));
     W.counter = reinterpret_cast<uint32_t*>(scratch);
     W.table = reinterpret_cast<chm::PairDev*>(scratch + 256);
-    auto* offsets = reinterpret_cast<uint32_t*>(scratch + 256 + ((tableBytes + 255) & ~size_t(255)));
+    auto* dJobs = reinterpret_cast<chm::NormListJob*>(scratch + 256 + tableBytes);
+    W.norms = reinterpret_cast<uint32_t*>(scratch + 256 + tableBytes + jobBytes);
+    auto* offsets = reinterpret_cast<uint32_t*>(scratch + 256 + tableBytes + jobBytes + normBytes);
     auto* sums = offsets + nItems + 1;
-    // pageable source: the copy is staged before the call returns, so `host` may go out of scope
-    if (cudaMemcpyAsync(W.table, host.data(), tableBytes, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    fbm_norm_bind(host, jobs, slots, W.norms);
+    // pageable sources: the copies are staged before the call returns, so `host` and `jobs` may go
+    // out of scope
+    if (cudaMemcpyAsync(W.table, host.data(), sizeof(chm::PairDev) * nbPairs, cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        (!jobs.empty() && cudaMemcpyAsync(dJobs, jobs.data(), sizeof(chm::NormListJob) * jobs.size(),
+                                          cudaMemcpyHostToDevice, stream) != cudaSuccess))
         st = RSFM_ERR_CUDA;
+    if (st == RSFM_OK) st = fbm_norm_fill(dJobs, jobs, stream);
     if (st == RSFM_OK)
         st = fbm_build(W, offsets, sums, stream, [&](void** ptr, size_t bytes) {
             return cudaMallocFromPoolAsync(ptr, bytes, pool, stream) == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA;
@@ -912,21 +1020,33 @@ extern "C" int rsfm_cashash_fbm_batch_create(const rsfm_cashash_pair* pairs, uin
     }
     W.nPairs = nbPairs;
     W.schemeOffset = (flags & RSFM_CASHASH_PER_SCHEME_LISTS) ? 1u : 0u;
+    std::vector<chm::NormListJob> jobs;
+    std::vector<std::pair<uint32_t, size_t>> slots;
+    size_t entries = 0;
+    fbm_norm_jobs(host, W.schemeOffset, jobs, slots, entries);
     const uint32_t nItems = nbPairs * 2048u;
     const size_t tableBytes = (sizeof(chm::PairDev) * nbPairs + 255) & ~size_t(255);
+    const size_t jobBytes = (sizeof(chm::NormListJob) * jobs.size() + 255) & ~size_t(255);
+    const size_t normBytes = entries * 4;
     const size_t offBytes = (size_t(nItems) + 1) * 4, sumBytes = (size_t(nItems) / 1024 + 2) * 4;
-    if (cudaMalloc(&b->mem, 256 + tableBytes + offBytes + sumBytes) != cudaSuccess) {
+    if (cudaMalloc(&b->mem, 256 + tableBytes + jobBytes + normBytes + offBytes + sumBytes) != cudaSuccess) {
         delete b;
         return RSFM_ERR_CUDA;
     }
     auto* base = static_cast<uint8_t*>(b->mem);
     W.counter = reinterpret_cast<uint32_t*>(base);
     W.table = reinterpret_cast<chm::PairDev*>(base + 256);
-    auto* offsets = reinterpret_cast<uint32_t*>(base + 256 + tableBytes);
+    auto* dJobs = reinterpret_cast<chm::NormListJob*>(base + 256 + tableBytes);
+    W.norms = reinterpret_cast<uint32_t*>(base + 256 + tableBytes + jobBytes);
+    auto* offsets = reinterpret_cast<uint32_t*>(base + 256 + tableBytes + jobBytes + normBytes);
     auto* sums = offsets + nItems + 1;
+    fbm_norm_bind(host, jobs, slots, W.norms);
     if (cudaMemcpyAsync(W.table, host.data(), sizeof(chm::PairDev) * nbPairs, cudaMemcpyHostToDevice, stream) !=
-        cudaSuccess)
+            cudaSuccess ||
+        (!jobs.empty() && cudaMemcpyAsync(dJobs, jobs.data(), sizeof(chm::NormListJob) * jobs.size(),
+                                          cudaMemcpyHostToDevice, stream) != cudaSuccess))
         st = RSFM_ERR_CUDA;
+    if (st == RSFM_OK) st = fbm_norm_fill(dJobs, jobs, stream);
     if (st == RSFM_OK)
         st = fbm_build(W, offsets, sums, stream, [](void** ptr, size_t bytes) {
             return cudaMalloc(ptr, bytes) == cudaSuccess ? RSFM_OK : RSFM_ERR_CUDA;
