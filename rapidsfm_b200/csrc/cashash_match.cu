@@ -90,6 +90,11 @@ __device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
     return v;
 }
 
+// 64-bit atomic minimum without a returned value (a reduction: no response traffic).
+__device__ __forceinline__ void red_min_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 // Ascending order of one (key, value) per lane by key, unless the keys already are ascending.
 __device__ __forceinline__ void sort_if_needed(uint32_t& key, uint32_t& val, uint32_t lane) {
     const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -695,7 +700,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const Pa
                     m4[k & 3u] = min(m4[k & 3u], ((nA + T.colNB[32 * w + k] - 2u * x[k]) << 5) | k);
                 const uint32_t key = min(min(m4[0], m4[1]), min(m4[2], m4[3]));
                 if ((key >> 5) < kValidD)
-                    atomicMin(&T.qBest[w][T.rowQ[row]],
+                    red_min_u64(&T.qBest[w][T.rowQ[row]],
                               (static_cast<unsigned long long>(key >> 5) << 32) | T.colT[32 * w + (key & 31u)]);
             }
             uint32_t y[32];
@@ -712,7 +717,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) match_subitems_kernel(const Pa
                     m4[k & 3u] = min(m4[k & 3u], ((nB + T.rowNA[32 * w + k] - 2u * y[k]) << 5) | k);
                 const uint32_t key = min(min(m4[0], m4[1]), min(m4[2], m4[3]));
                 if ((key >> 5) < kValidD)
-                    atomicMin(&tBest[T.colT[row]],
+                    red_min_u64(&tBest[T.colT[row]],
                               (static_cast<unsigned long long>(key >> 5) << 32) | T.rowQ[32 * w + (key & 31u)]);
             }
             __syncwarp();
