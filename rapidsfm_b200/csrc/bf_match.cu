@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                         const uint32_t i = U.r0 + rr;
                         if (i < T.nA) {
                             const uint32_t d = nbj - uint32_t(colBest[cc] >> 8);
-                            atomicMin(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
+                            red_min_u64(&T.bestB[j], (static_cast<unsigned long long>(d) << 32) | i);
                         }
                     }
                 }
@@ -478,9 +478,9 @@ __global__ void __launch_bounds__(Cfg<kWG>::kThreads, 1) bf_match_kernel(const _
                 }
                 if (bst != ~0ull) {
                     const unsigned long long old = atomicMin(&T.bestA[i], bst);
-                    atomicMin(&T.secondA[i], max(uint32_t(old >> 32), uint32_t(bst >> 32)));
+                    red_min_u32(&T.secondA[i], max(uint32_t(old >> 32), uint32_t(bst >> 32)));
                 }
-                if (sec != ~0u) atomicMin(&T.secondA[i], sec);
+                if (sec != ~0u) red_min_u32(&T.secondA[i], sec);
             }
             named_bar(1, 32 * kEpiWarps);
         }

@@ -90,11 +90,6 @@ __device__ __forceinline__ uint32_t warp_sort(uint32_t v, uint32_t lane) {
     return v;
 }
 
-// 64-bit atomic minimum without a returned value (a reduction: no response traffic).
-__device__ __forceinline__ void red_min_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("red.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
 // Ascending order of one (key, value) per lane by key, unless the keys already are ascending.
 __device__ __forceinline__ void sort_if_needed(uint32_t& key, uint32_t& val, uint32_t lane) {
     const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -270,7 +265,7 @@ __device__ __forceinline__ void process_item(Smem& S, const ItemCtx& C, uint32_t
                     const uint32_t tIdx = S.colT[32 * ch + lane];
                     if (mine != 0xFFFFFFFFu && tIdx != kNoRow) {
                         const uint32_t qIdx = S.rowQ[32 * warp + (mine & 31u)];
-                        atomicMin(&C.tBest[rowTask][tIdx], (static_cast<unsigned long long>(mine >> 5) << 32) | qIdx);
+                        red_min_u64(&C.tBest[rowTask][tIdx], (static_cast<unsigned long long>(mine >> 5) << 32) | qIdx);
                     }
                 }
             }
@@ -278,7 +273,7 @@ __device__ __forceinline__ void process_item(Smem& S, const ItemCtx& C, uint32_t
             __syncthreads();  // TMEM and the B block are reused by the next block / tile
         }
         if (rowValid && bestD != 0xFFFFFFFFu)
-            atomicMin(&C.qBest[rowTask][q], (static_cast<unsigned long long>(bestD) << 32) | bestT);
+            red_min_u64(&C.qBest[rowTask][q], (static_cast<unsigned long long>(bestD) << 32) | bestT);
         __syncthreads();  // the A tile is reused by the next tile
     }
 }

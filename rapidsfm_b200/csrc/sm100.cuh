@@ -127,6 +127,14 @@ __device__ __forceinline__ bool mbar_wait_backoff(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// Atomic minimum whose old value is not needed: a reduction (`red`), no response traffic.
+__device__ __forceinline__ void red_min_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_min_u32(uint32_t* p, uint32_t v) {
+    asm volatile("red.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // ---------------------------------------------------------------- TMA
 __device__ __forceinline__ void tma_prefetch_desc(const void* tmap) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
