@@ -175,10 +175,15 @@ __device__ __forceinline__ void process_item(Smem& S, const ItemCtx& C, uint32_t
         const uint32_t row = 32u * warp + lane;
         S.rowQ[row] = q;
         S.rowNA[row] = q != kNoRow ? C.q[task].sqr[q] : kBigNorm;
-        {
-            const uint8_t* src = q != kNoRow ? C.q[task].desc + size_t(q) * 128 : C.q[0].desc;
+        {   // eight lanes copy the eight 16-byte chunks of one row, four rows per instruction
+            const uint8_t* base = C.q[task].desc;
 #pragma unroll
-            for (uint32_t c = 0; c < 8; ++c) cp_async16(S.a + sw128(row, c), src + 16 * c, q != kNoRow);
+            for (uint32_t ii = 0; ii < 8; ++ii) {
+                const uint32_t r = 4u * ii + (lane >> 3), ch = lane & 7u;
+                const uint32_t qr = __shfl_sync(0xffffffffu, q, r);
+                cp_async16(S.a + sw128(32u * warp + r, ch), qr != kNoRow ? base + size_t(qr) * 128 + 16 * ch : C.q[0].desc,
+                           qr != kNoRow);
+            }
         }
         const uint32_t rowTask = task;
         const bool rowValid = q != kNoRow;
