@@ -15,7 +15,7 @@
 // tile gathered with cp.async into the 128-byte-swizzled layout; the train members form 64-column
 // B blocks (sorted by index). One thread issues the u8 x u8 UMMA (M=128, N=64, K=128) into TMEM;
 // each warp reads its segment's 32 TMEM lanes: row minima are thread-local, column minima use a
-// warp reduction per column; results go out with 64-bit atomicMin as in the reference.
+// warp reduction per column; results go out as 64-bit atomic minima, as in the reference.
 #include "common.h"
 #include "sm100.cuh"
 #include <algorithm>
@@ -353,7 +353,7 @@ __global__ void pairs_init_kernel(const PairDev* __restrict__ pairs, uint32_t* c
 // members; a CTA takes four sub-items at once: warp w gathers sub-item w's 32 query rows into A
 // rows 32w.. and its 32 train rows into B rows 32w.., one UMMA (M = N = 128) computes all 128 x 128
 // products, and warp w reads only its diagonal 32 x 32 block of the accumulator. Row and column
-// minima are merged across sub-items by the same 64-bit atomicMin as everywhere else.
+// minima are merged across sub-items by the same 64-bit atomic minimum as everywhere else.
 struct SubItem {
     const uint32_t* qList;  // first query member of the segment (bucket list of the query image)
     const uint32_t* tList;  // first train member of the segment
@@ -410,7 +410,6 @@ struct SubSmem {
     uint32_t tmem;
 };
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Arrives on `bar` once all of this thread's earlier cp.async copies have landed (the barrier's
 // expected count includes this arrival).
 __device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t* bar) {

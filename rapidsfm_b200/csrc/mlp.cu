@@ -43,10 +43,10 @@ __device__ __forceinline__ void umma_f16(uint32_t d, uint64_t a, uint64_t b, uin
 }
 
 // ---------------------------------------------------------------- inference
-// Persistent, one CTA per SM, 256 threads. Per 128-descriptor tile: X (u8 -> bf16, x/64 exact)
+// Persistent, one CTA per SM, 512 threads. Per 128-descriptor tile: X (u8 -> bf16, x/64 exact)
 // into smem; layer 1 = 8 UMMAs (M=128, N=256, K=16) into TMEM columns 0-255; bias + ReLU -> bf16
-// H back to smem one 64-unit K panel at a time, each panel's four layer-2 UMMAs (N=128) issued into
-// columns 256-383 as soon as it is written; sign bits out. Two tiles are in flight: the next
+// H back to smem two 64-unit K panels at a time, each pair's eight layer-2 UMMAs (N=128) issued
+// into columns 256-383 as soon as it is written; sign bits out. Two tiles are in flight: the next
 // tile's X conversion overlaps this tile's layer 2, and this tile's layer-2 epilogue overlaps the
 // next tile's layer 1.
 constexpr int kInfThreads = 512;
