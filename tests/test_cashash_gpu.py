@@ -380,3 +380,71 @@ def test_find_best_match_pairs(rsfm, oracle, flags):
                                                 ti["host_buckets"], per_scheme=bool(flags))
         np.testing.assert_array_equal(got_q, eq)
         np.testing.assert_array_equal(got_t, et)
+
+
+@pytest.mark.parametrize("flags", [0, 1])
+def test_find_best_match_pairs_unsorted_lists(rsfm, oracle, flags):
+    """Bucket lists in any member order (as the reference's atomic bucket fill leaves them): the
+    pairs call and the reusable batch sort each 32-member segment with its norms and give the
+    oracle's results, whose ties go to the lowest index whatever the order."""
+    rng = np.random.default_rng(91 + flags)
+
+    def shuffled(img):
+        b = np.array(img["host_buckets"], dtype=np.uint32, copy=True)
+        n = img["n"]
+        up = np.asarray(img["upper"], dtype=np.int64).reshape(8, 256)
+        for s in range(8):
+            lo = 0
+            for k in range(256):
+                hi = int(up[s, k])
+                seg = b[s * n + lo:s * n + hi]
+                rng.shuffle(seg)
+                lo = hi
+        out = dict(img)
+        out["host_buckets"] = b
+        out["buckets"] = _dev(b.view(np.int32))
+        return out
+
+    sizes = [(1500, 1700), (700, 2000), (2000, 900)]
+    data = []
+    for nq, nt in sizes:
+        qd = rng.integers(0, 256, size=(nq, 128), dtype=np.int64).astype(np.uint8)
+        td = rng.integers(0, 256, size=(nt, 128), dtype=np.int64).astype(np.uint8)
+        # few distinct keys per byte: large buckets, several 32-member segments each
+        qk = rng.integers(0, 24, size=(nq, 8), dtype=np.int64).astype(np.uint8)
+        tk = rng.integers(0, 24, size=(nt, 8), dtype=np.int64).astype(np.uint8)
+        data.append((qd, shuffled(_image(oracle, qd, qk)), td, shuffled(_image(oracle, td, tk))))
+    lib = rsfm._lib.load()
+
+    def pairs_array():
+        res, arr = [], []
+        for qd, qi, td, ti in data:
+            a = torch.empty(len(qd), dtype=torch.int64, device="cuda")
+            b = torch.empty(len(td), dtype=torch.int64, device="cuda")
+            res.append((a, b))
+            arr.append(rsfm._lib.CasHashPair(_ci(rsfm, qi), _ci(rsfm, ti), len(qd), len(td),
+                                             rsfm._lib.CasHashResult(a.data_ptr(), b.data_ptr())))
+        return res, (rsfm._lib.CasHashPair * len(arr))(*arr)
+
+    def check(res):
+        torch.cuda.synchronize()
+        assert rsfm.device_error() == 0
+        for (qd, qi, td, ti), (a, b) in zip(data, res):
+            eq, et = oracle.cashash_find_best_match(qd, qi["upper"], qi["host_buckets"], td, ti["upper"],
+                                                    ti["host_buckets"], per_scheme=bool(flags))
+            np.testing.assert_array_equal(a.cpu().numpy().view(np.uint32).reshape(-1, 2), eq)
+            np.testing.assert_array_equal(b.cpu().numpy().view(np.uint32).reshape(-1, 2), et)
+
+    res, c = pairs_array()
+    rsfm._lib.check(lib.rsfm_cashash_find_best_match_pairs(c, len(data), flags, None), "pairs")
+    check(res)
+    res, c = pairs_array()
+    h = ctypes.c_void_p(0)
+    rsfm._lib.check(lib.rsfm_cashash_fbm_batch_create(ctypes.cast(c, ctypes.c_void_p), len(data), flags, None,
+                                                      ctypes.byref(h)), "create")
+    try:
+        for _ in range(2):
+            rsfm._lib.check(lib.rsfm_cashash_fbm_batch_launch(h, None), "launch")
+            check(res)
+    finally:
+        lib.rsfm_cashash_fbm_batch_destroy(h)
