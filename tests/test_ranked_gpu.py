@@ -45,8 +45,10 @@ def _ranked_image(rsfm, img, keep, records=False):
 
 @pytest.mark.parametrize("records", [False, True])
 # topK <= 12 runs one thread per query, larger topK one warp per query: 12 and 13 sit either side.
+# tables x n not a multiple of 4 (1001 x 3, 999 x 5): the last 16-byte block of the bucket lists
+# would pass their end and is read one entry at a time.
 @pytest.mark.parametrize("n,tables,topk", [(8192, 6, 10), (3000, 6, 10), (1000, 8, 32), (500, 1, 1),
-                                           (2000, 4, 12), (2000, 4, 13)])
+                                           (2000, 4, 12), (2000, 4, 13), (1001, 3, 10), (999, 5, 12)])
 def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, records):
     q, t, _ = synth.make_pair(n, n, 0.4, 8.0, seed=n + tables)
     w = _gauss_weights(7)
