@@ -15,6 +15,7 @@ its kernel tests (test/bruteForceMatchKernelTest.cpp:140-164), restated in oracl
 the host cores (all threads) on a bounded row sample of the same workload.
 """
 import argparse
+import copy
 import ctypes
 import json
 import os
@@ -647,11 +648,30 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
         flat = ch.register_ranked_images(h, [x for pair in imgs for x in pair], stream=stream)
         torch.cuda.synchronize()
         hash_s = time.perf_counter() - t0
+        # train images' records in each table's bucket-list order (table records): a candidate is
+        # then one load at its list position; the same images without them read a bucket entry,
+        # then the record (same results, checked below)
+        t0 = time.perf_counter()
+        for t in flat[1::2]:
+            t.pack_table_records(stream=stream)
+        torch.cuda.synchronize()
+        trec_s = time.perf_counter() - t0
         ranked = list(zip(flat[0::2], flat[1::2]))
+        bare = []
+        for t in flat[1::2]:
+            b = copy.copy(t)
+            b.table_records = None
+            bare.append(b)
+        ranked_bare = list(zip(flat[0::2], bare))
         rows = {}
         for tables in (2, 3, 4, 6, 8):
+            bb = ch.RankedBatch(ranked_bare, tables, 10)
+            ms_bare = _events_ms(lambda: bb.launch(stream), 3, stream)
             batch = ch.RankedBatch(ranked, tables, 10)
             ms = _events_ms(lambda: batch.launch(stream), 3, stream)
+            equal = all(torch.equal(x[0], y[0]) and torch.equal(x[1], y[1]) and torch.equal(x[2], y[2])
+                       for x, y in zip(batch.results, bb.results))
+            bb.close()
             hit = torch.zeros((), dtype=torch.int64, device=dev)
             tot = torch.zeros((), dtype=torch.int64, device=dev)
             rep = torch.zeros((), dtype=torch.int64, device=dev)
@@ -664,12 +684,13 @@ def run_cascade(dev, stream, n_pairs=1000, n=8192, seed=3):
                 r = (flg & 1) == 1
                 rep += r.sum()
                 tp += (r & same & ok).sum()
-            rows[str(tables)] = {"match_ms": ms, "recall": int(hit) / max(1, int(tot)),
+            rows[str(tables)] = {"match_ms": ms, "match_ms_thread_per_query": ms_bare,
+                                 "results_equal_thread_per_query": equal, "recall": int(hit) / max(1, int(tot)),
                                  "precision": int(tp) / max(1, int(rep)), "reported": int(rep),
                                  "desc_pairs_per_s": pairs / (ms * 1e-3)}
             batch.close()
         ok98 = [int(k) for k, v in rows.items() if v["recall"] >= 0.98]
-        out[name] = {"tables": rows, "hash_and_buckets_host_s": hash_s,
+        out[name] = {"tables": rows, "hash_and_buckets_host_s": hash_s, "table_records_host_s": trec_s,
                      "fewest_tables_at_98pct_recall": min(ok98) if ok98 else None}
         if name == "plain":
             # reference mode (cashash::findBestMatch): all 8 schemes, exact L2 over every descriptor

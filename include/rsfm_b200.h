@@ -346,9 +346,10 @@ typedef struct rsfm_ranked_image {
     const uint32_t* sqrNormDesc;
     uint32_t nbDesc;
     const uint32_t* records;  /* optional (32-byte aligned): rsfm_ranked_pack_records output */
+    const uint32_t* tableRecords;  /* optional (32-byte aligned): rsfm_ranked_pack_table_records output */
 } rsfm_ranked_image;
-/* Alignment (checked; RSFM_ERR_INVALID_ARG otherwise): desc and records 32 bytes, codes and
- * buckets 16, keys 8. Bucket lists are read in aligned 16-byte blocks within the lists of the tables in
+/* Alignment (checked; RSFM_ERR_INVALID_ARG otherwise): desc, records and tableRecords 32 bytes,
+ * codes and buckets 16, keys 8. Bucket lists are read in aligned 16-byte blocks within the lists of the tables in
  * use. */
 
 /* Packs keys, codes and squared norms into one 32-byte record per descriptor (8 x uint32:
@@ -356,6 +357,15 @@ typedef struct rsfm_ranked_image {
  * ranked matching instead of two (no reference counterpart). records: nbDesc x 32 bytes. */
 int rsfm_ranked_pack_records(const uint8_t* keys, const uint32_t* codes, const uint32_t* sqrNormDesc,
                              uint32_t nbDesc, uint32_t* records, cudaStream_t stream);
+
+/* Copies the packed records into each table's bucket-list order (no reference counterpart):
+ * tableRecords[s][pos] = records[buckets[s * nbDesc + pos]] with word 7 set to that descriptor index,
+ * for all 8 tables (tableRecords: 8 x nbDesc x 32 bytes). When a train image has them, ranked
+ * matching with topK <= 12 reads a candidate with one load at its list position instead of a
+ * bucket-entry load and a record load (same results); they must be re-packed whenever the records
+ * or bucket lists change. nbDesc < 2^24. */
+int rsfm_ranked_pack_table_records(const uint32_t* records, const uint32_t* buckets, uint32_t nbDesc,
+                                   uint32_t* tableRecords, cudaStream_t stream);
 
 /* Ranked cascade-hash matching (no reference counterpart): for every query descriptor, the
  * candidates are the train descriptors sharing one of the first nbTables bucket keys; they are

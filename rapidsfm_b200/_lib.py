@@ -101,7 +101,7 @@ class CasHashPair(ctypes.Structure):
 class RankedImage(ctypes.Structure):
     _fields_ = [("desc", ctypes.c_void_p), ("keys", ctypes.c_void_p), ("codes", ctypes.c_void_p),
                 ("bucketEnds", ctypes.c_void_p), ("buckets", ctypes.c_void_p), ("sqrNormDesc", ctypes.c_void_p),
-                ("nbDesc", ctypes.c_uint32), ("records", ctypes.c_void_p)]
+                ("nbDesc", ctypes.c_uint32), ("records", ctypes.c_void_p), ("tableRecords", ctypes.c_void_p)]
 
 
 class RankedPair(ctypes.Structure):
@@ -224,6 +224,8 @@ SIGNATURES = {
     "rsfm_ranked_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_ranked_pack_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                                 ctypes.c_void_p, ctypes.c_void_p]),
+    "rsfm_ranked_pack_table_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                      ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rsfm_bf_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rsfm_mlp_hash": (ctypes.c_int, [ctypes.POINTER(MLP), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,

@@ -55,6 +55,7 @@ class RankedImage:
         self.records = torch.empty((max(n, 1), 8), dtype=torch.int32, device=dev)
         _lib.check(lib.rsfm_ranked_pack_records(_p(keys), _p(codes), _p(self.sqr), n, _p(self.records), s),
                    "rsfm_ranked_pack_records")
+        self.table_records = None
         self.n = n
 
     @classmethod
@@ -63,7 +64,21 @@ class RankedImage:
         self = cls.__new__(cls)
         self.desc, self.keys, self.codes, self.sqr = desc, keys, codes, sqr
         self.upper, self._max, self.buckets, self.records = upper, max_bucket, buckets, records
+        self.table_records = None
         self.n = desc.shape[0]
+        return self
+
+    def pack_table_records(self, out=None, stream=None):
+        """Copies the records into each table's bucket-list order (rsfm_ranked_pack_table_records):
+        as a train image, a candidate then costs one load at its list position instead of a
+        bucket-entry load and a record load. out: optional int32 [8 * n, 8] device tensor to fill
+        (32-byte aligned)."""
+        lib = _lib.load()
+        if out is None:
+            out = torch.empty((8 * max(self.n, 1), 8), dtype=torch.int32, device=self.desc.device)
+        _lib.check(lib.rsfm_ranked_pack_table_records(_p(self.records), _p(self.buckets), self.n, _p(out),
+                                                      _stream_ptr(stream)), "rsfm_ranked_pack_table_records")
+        self.table_records = out
         return self
 
     def max_bucket_size(self):
@@ -72,7 +87,8 @@ class RankedImage:
     def as_ctype(self):
         return _lib.RankedImage(self.desc.data_ptr(), self.keys.data_ptr(), self.codes.data_ptr(),
                                 self.upper.data_ptr(), self.buckets.data_ptr(), self.sqr.data_ptr(), self.n,
-                                self.records.data_ptr())
+                                self.records.data_ptr(),
+                                self.table_records.data_ptr() if self.table_records is not None else None)
 
 
 def _ranked_hasher(hasher):
@@ -83,13 +99,14 @@ def _ranked_hasher(hasher):
     return _lib.RankedHasher(hasher.w.data_ptr(), hasher.bias.data_ptr(), 192, None)
 
 
-def register_ranked_images(hasher, descs, stream=None):
+def register_ranked_images(hasher, descs, stream=None, table_records=False):
     """Hashes and indexes many images at once (rsfm_ranked_register_flat): per image the 8 bucket
     keys, the 128-bit code, squared norms, bucket bounds and lists and the packed records. The
     descriptors are first copied back to back into one buffer; every per-descriptor step then runs
     once over all of them and every bucket-build step once for all images. hasher: a CasHash with
-    192 channels or a learned_hash.LearnedHash. Returns one RankedImage per input (views of shared
-    buffers, including the packed copy of its descriptors)."""
+    192 channels or a learned_hash.LearnedHash. table_records: also pack each image's records in
+    bucket-list order (RankedImage.pack_table_records, one launch per image). Returns one
+    RankedImage per input (views of shared buffers, including the packed copy of its descriptors)."""
     lib = _lib.load()
     for d in descs:
         _check_desc(d)
@@ -121,6 +138,11 @@ def register_ranked_images(hasher, descs, stream=None):
         o = int(offs[k])
         imgs.append(RankedImage.from_parts(flat[o:o + n], keys[o:o + n], codes[o:o + n], sqr[o:o + n], upper[k],
                                            maxb[k:k + 1], buckets[8 * o:8 * (o + n)].view(8, n), records[o:o + n]))
+    if table_records:
+        trec = torch.empty((8 * cap, 8), dtype=torch.int32, device=dev)
+        for k, img in enumerate(imgs):
+            o = int(offs[k])
+            img.pack_table_records(out=trec[8 * o:8 * (o + img.n)] if img.n else trec[:8], stream=stream)
     return imgs
 
 

@@ -30,6 +30,7 @@ struct Img {
     const uint32_t* buckets;  // [8][n]: bucket (s, b) at buckets[s*n + lower(s,b)]
     const uint32_t* sqr;
     const uint4* rec;      // optional packed records, 2 x uint4 per descriptor (see pack_kernel)
+    const uint4* trec;     // optional table records: [8][n] records in bucket-list order, index in word 7
     uint32_t n;
 };
 
@@ -47,10 +48,10 @@ __global__ void pack_kernel(const uint2* __restrict__ keys, const uint4* __restr
 // True when any of the first s key bytes of t equals q's (bytes 0-3 in .x, 4-7 in .y): the
 // candidate was already found in an earlier table. __vcmpeq4 sets 0xFF per equal byte.
 // Alignment the kernels' vector loads rely on: descriptors and packed records 32 bytes, codes
-// and bucket lists 16, keys 8.
+// and bucket lists 16, keys 8, table records 32.
 inline bool aligned(const Img& I) {
     auto a = [](const void* p, uintptr_t m) { return (reinterpret_cast<uintptr_t>(p) & (m - 1)) == 0; };
-    return a(I.desc, 32) && a(I.keys, 8) && a(I.codes, 16) && a(I.buckets, 16) && a(I.rec, 32);
+    return a(I.desc, 32) && a(I.keys, 8) && a(I.codes, 16) && a(I.buckets, 16) && a(I.rec, 32) && a(I.trec, 32);
 }
 
 __device__ __forceinline__ bool collides_before(uint2 t, uint2 q, uint32_t s) {
@@ -358,6 +359,11 @@ __device__ __forceinline__ void ldg_record(const uint4* p, uint4& a, uint4& b) {
 constexpr int kThreadBlock = 128;
 constexpr int kThreadMinBlocks = 7;  // 72 registers, 28 warps per SM (6: 80 registers, 2 % slower)
 
+// kTrec: the train image has table records (each table's records in its bucket-list order, the
+// index in word 7): a candidate is then one load at its list position instead of a bucket-entry
+// load followed by a record load, and a step takes the next four entries of the list, whatever
+// their alignment.
+template <bool kTrec>
 __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
                                                    uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
                                                    const Out& O) {
@@ -385,40 +391,59 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
         while (x == hi && s + 1 < nt) open_table(++s);
         if (x >= hi) break;
         const size_t e = size_t(s) * T.n + x;
-        uint32_t off = 0, cnt = 1;
-        uint4 w;
-        if ((e | 3u) < size_t(nt) * T.n) {
-            off = uint32_t(e) & 3u;
-            w = __ldg(reinterpret_cast<const uint4*>(T.buckets + (e - off)));
-            cnt = min(4u - off, hi - x);
-        } else {
-            w.x = __ldg(&T.buckets[e]);
-            w.y = w.z = w.w = 0xFFFFFFFFu;
-        }
-        x += cnt;
         uint32_t j[4], su[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const uint32_t pos = off + uint32_t(u);
-            const uint32_t v = pos == 0 ? w.x : pos == 1 ? w.y : pos == 2 ? w.z : w.w;
-            su[u] = s;
-            j[u] = uint32_t(u) < cnt ? v : 0xFFFFFFFFu;
-        }
         uint2 tk[4];
         uint4 tc[4];
+        if constexpr (kTrec) {
+            const uint32_t cnt = min(4u, hi - x);
+            x += cnt;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (j[u] == 0xFFFFFFFFu) {
+            for (int u = 0; u < 4; ++u) {
+                su[u] = s;
+                j[u] = 0xFFFFFFFFu;
                 tk[u] = make_uint2(0, 0);
                 tc[u] = make_uint4(0, 0, 0, 0);
-            } else if (T.rec) {
-                uint4 r0, r1;
-                ldg_record(&T.rec[2 * size_t(j[u])], r0, r1);
-                tk[u] = make_uint2(r0.x, r0.y);
-                tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
+                if (uint32_t(u) < cnt) {
+                    uint4 r0, r1;
+                    ldg_record(&T.trec[2 * (e + u)], r0, r1);
+                    j[u] = r1.w;
+                    tk[u] = make_uint2(r0.x, r0.y);
+                    tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
+                }
+            }
+        } else {
+            uint32_t off = 0, cnt = 1;
+            uint4 w;
+            if ((e | 3u) < size_t(nt) * T.n) {
+                off = uint32_t(e) & 3u;
+                w = __ldg(reinterpret_cast<const uint4*>(T.buckets + (e - off)));
+                cnt = min(4u - off, hi - x);
             } else {
-                tk[u] = __ldg(&T.keys[j[u]]);
-                tc[u] = __ldg(&T.codes[j[u]]);
+                w.x = __ldg(&T.buckets[e]);
+                w.y = w.z = w.w = 0xFFFFFFFFu;
+            }
+            x += cnt;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t pos = off + uint32_t(u);
+                const uint32_t v = pos == 0 ? w.x : pos == 1 ? w.y : pos == 2 ? w.z : w.w;
+                su[u] = s;
+                j[u] = uint32_t(u) < cnt ? v : 0xFFFFFFFFu;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (j[u] == 0xFFFFFFFFu) {
+                    tk[u] = make_uint2(0, 0);
+                    tc[u] = make_uint4(0, 0, 0, 0);
+                } else if (T.rec) {
+                    uint4 r0, r1;
+                    ldg_record(&T.rec[2 * size_t(j[u])], r0, r1);
+                    tk[u] = make_uint2(r0.x, r0.y);
+                    tc[u] = make_uint4(r0.z, r0.w, r1.x, r1.y);
+                } else {
+                    tk[u] = __ldg(&T.keys[j[u]]);
+                    tc[u] = __ldg(&T.codes[j[u]]);
+                }
             }
         }
 #pragma unroll
@@ -483,10 +508,12 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
     if (O.nbCand) O.nbCand[i] = total;
 }
 
+template <bool kTrec>
 __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
                                                                       uint32_t ratioNum, uint32_t ratioDen, Out O) {
     const uint32_t t = blockIdx.x * kThreadBlock + threadIdx.x;
-    if (t < Q.n) match_query_thread(Q, T, Q.buckets ? __ldg(&Q.buckets[t]) : t, tables, topK, ratioNum, ratioDen, O);
+    if (t < Q.n)
+        match_query_thread<kTrec>(Q, T, Q.buckets ? __ldg(&Q.buckets[t]) : t, tables, topK, ratioNum, ratioDen, O);
 }
 
 __device__ __forceinline__ uint32_t pair_of(const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t g) {
@@ -498,6 +525,23 @@ __device__ __forceinline__ uint32_t pair_of(const uint32_t* __restrict__ begin, 
     return lo;
 }
 
+// Table records: out[s n + pos] = records[buckets[s n + pos]] with word 7 = the index, for s < tables.
+__global__ void table_records_kernel(const uint4* __restrict__ rec, const uint32_t* __restrict__ buckets, uint32_t n,
+                                     uint32_t count, uint4* __restrict__ out) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const uint32_t j = buckets[e];
+        uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0xFFFFFFFFu);
+        if (j < n) {
+            a = rec[2 * size_t(j)];
+            b = rec[2 * size_t(j) + 1];
+            b.w = j;
+        }
+        out[2 * size_t(e)] = a;
+        out[2 * size_t(e) + 1] = b;
+    }
+}
+
+template <bool kTrec>
 __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_batch_kernel(
     const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
     uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
@@ -510,7 +554,7 @@ __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_
     // neighbouring threads then share their first table's candidate list, walk it in step and
     // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
     if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
-    match_query_thread(P.q, P.t, i, tables, topK, ratioNum, ratioDen, P.o);
+    match_query_thread<kTrec>(P.q, P.t, i, tables, topK, ratioNum, ratioDen, P.o);
 }
 
 // Kernel choice: one thread per query when topK fits the register list, unless
@@ -547,6 +591,7 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
         I.buckets = m->buckets;
         I.sqr = m->sqrNormDesc;
         I.rec = reinterpret_cast<const uint4*>(m->records);
+        I.trec = reinterpret_cast<const uint4*>(m->tableRecords);
         I.n = m->nbDesc;
         return I;
     };
@@ -560,7 +605,12 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     const chr::Out O{reinterpret_cast<unsigned long long*>(best), secondDist, flags, nbCandidates};
     if (chr::use_thread_kernel(topK)) {
         const uint32_t grid = (Q.n + chr::kThreadBlock - 1) / chr::kThreadBlock;
-        chr::ranked_thread_kernel<<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+        if (T.trec)
+            chr::ranked_thread_kernel<true>
+                <<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+        else
+            chr::ranked_thread_kernel<false>
+                <<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
     } else {
         const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
         chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
@@ -575,6 +625,7 @@ struct rsfm_ranked_batch {
     chr::PairDev* dPairs = nullptr;
     uint32_t* dBegin = nullptr;
     uint32_t nPairs = 0, total = 0, tables = 0, topK = 0, ratioNum = 0, ratioDen = 1;
+    bool tableRecords = false;  // every train image with work has table records
 };
 
 extern "C" int rsfm_ranked_batch_destroy(rsfm_ranked_batch* b) {
@@ -594,6 +645,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
     std::vector<chr::PairDev> host(nbPairs);
     std::vector<uint32_t> begin(nbPairs + 1, 0);
     uint64_t total = 0;
+    bool allTrec = true;
     auto mk = [](const rsfm_ranked_image* m) {
         chr::Img I;
         I.desc = static_cast<const uint8_t*>(m->desc);
@@ -603,6 +655,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
         I.buckets = m->buckets;
         I.sqr = m->sqrNormDesc;
         I.rec = reinterpret_cast<const uint4*>(m->records);
+        I.trec = reinterpret_cast<const uint4*>(m->tableRecords);
         I.n = m->nbDesc;
         return I;
     };
@@ -619,6 +672,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
             return RSFM_ERR_INVALID_ARG;
         host[p].q = mk(q);
         host[p].t = mk(t);
+        if (q->nbDesc && t->nbDesc && !t->tableRecords) allTrec = false;
         if (!chr::aligned(host[p].q) || !chr::aligned(host[p].t)) return RSFM_ERR_INVALID_ARG;
         host[p].o = chr::Out{reinterpret_cast<unsigned long long*>(in.best), in.secondDist, in.flags, in.nbCandidates};
         begin[p] = uint32_t(total);
@@ -641,6 +695,7 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
     b->topK = topK;
     b->ratioNum = ratioNum;
     b->ratioDen = ratioDen;
+    b->tableRecords = allTrec;
     *out = b;
     return RSFM_OK;
 }
@@ -653,8 +708,12 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
     const bool prof = profile_begin(stream, &tok);
     if (chr::use_thread_kernel(b->topK)) {
         const uint32_t grid = (b->total + chr::kThreadBlock - 1) / chr::kThreadBlock;
-        chr::ranked_thread_batch_kernel<<<grid, chr::kThreadBlock, 0, stream>>>(
-            b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
+        if (b->tableRecords)
+            chr::ranked_thread_batch_kernel<true><<<grid, chr::kThreadBlock, 0, stream>>>(
+                b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
+        else
+            chr::ranked_thread_batch_kernel<false><<<grid, chr::kThreadBlock, 0, stream>>>(
+                b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
     } else {
         const uint32_t grid = std::min<uint32_t>((b->total + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
         chr::ranked_batch_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total,
@@ -677,6 +736,22 @@ extern "C" int rsfm_ranked_pack_records(const uint8_t* keys, const uint32_t* cod
     chr::pack_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const uint2*>(keys),
                                                reinterpret_cast<const uint4*>(codes), sqrNormDesc, nbDesc,
                                                reinterpret_cast<uint4*>(records));
+    RSFM_CUDA_TRY(cudaGetLastError());
+    launch_count_add(1);
+    return RSFM_OK;
+}
+
+extern "C" int rsfm_ranked_pack_table_records(const uint32_t* records, const uint32_t* buckets, uint32_t nbDesc,
+                                              uint32_t* tableRecords, cudaStream_t stream) {
+    launch_count_reset();
+    if (nbDesc == 0) return RSFM_OK;
+    if (!records || !buckets || !tableRecords || nbDesc >= (1u << 24) || (reinterpret_cast<uintptr_t>(records) & 31u) ||
+        (reinterpret_cast<uintptr_t>(tableRecords) & 31u))
+        return RSFM_ERR_INVALID_ARG;
+    const uint32_t count = 8 * nbDesc;
+    const uint32_t grid = std::min<uint32_t>((count + 255) / 256, uint32_t(8 * sm_count()));
+    chr::table_records_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const uint4*>(records), buckets, nbDesc,
+                                                        count, reinterpret_cast<uint4*>(tableRecords));
     RSFM_CUDA_TRY(cudaGetLastError());
     launch_count_add(1);
     return RSFM_OK;

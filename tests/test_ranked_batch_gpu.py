@@ -14,7 +14,7 @@ def _dev(x):
     return torch.from_numpy(np.ascontiguousarray(x)).cuda()
 
 
-def _images(ch, sizes, seed):
+def _images(ch, sizes, seed, table=False):
     cas = ch.CasHash(ch.gaussian_weights(seed))
     rng = np.random.default_rng(seed)
     imgs = []
@@ -23,14 +23,18 @@ def _images(ch, sizes, seed):
         dq, dt = _dev(q), _dev(t)
         cas.fit(dq)
         cas.fit(dt)
-        imgs.append((cas.ranked_image(dq), cas.ranked_image(dt)))
+        qi, ti = cas.ranked_image(dq), cas.ranked_image(dt)
+        if table:
+            ti.pack_table_records()
+        imgs.append((qi, ti))
     return imgs
 
 
-@pytest.mark.parametrize("tables,topk", [(6, 10), (3, 4)])
-def test_batch_equals_per_pair(rsfm, tables, topk):
+@pytest.mark.parametrize("table", [False, True])
+@pytest.mark.parametrize("tables,topk", [(6, 10), (3, 4), (8, 32)])
+def test_batch_equals_per_pair(rsfm, tables, topk, table):
     from rapidsfm_b200 import cashash as ch
-    imgs = _images(ch, [(3000, 2000), (17, 5000), (4096, 4096), (1, 1), (700, 130)], 3)
+    imgs = _images(ch, [(3000, 2000), (17, 5000), (4096, 4096), (1, 1), (700, 130)], 3, table)
     batch = ch.RankedBatch(imgs, tables, topk, count_candidates=True)
     got = batch.launch()
     for (q, t), (b, s, f, c) in zip(imgs, got):
@@ -38,6 +42,41 @@ def test_batch_equals_per_pair(rsfm, tables, topk):
         torch.cuda.synchronize()
         assert torch.equal(b, eb) and torch.equal(s, es) and torch.equal(f, ef) and torch.equal(c, ec)
     batch.close()
+
+
+@pytest.mark.parametrize("tables,topk", [(6, 10), (2, 32)])
+def test_table_records_equal_plain_images(rsfm, tables, topk):
+    """Registration with table records (candidates read at their bucket-list positions) gives the
+    results of the same images without them, per pair and batched, with an empty train
+    image and a batch that mixes trains with and without table records."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(17))
+    rng = np.random.default_rng(17)
+    descs = [_dev(synth.make_pair(n, 1, 0.5, 8.0, seed=int(rng.integers(1 << 30)))[0]) for n in (2500, 1, 3333, 640)]
+    for d in descs:
+        cas.fit(d)
+    empty = torch.empty((0, 128), dtype=torch.uint8, device="cuda")
+    plain = ch.register_ranked_images(cas, descs + [empty])
+    packed = ch.register_ranked_images(cas, descs + [empty], table_records=True)
+    torch.cuda.synchronize()
+    for p in packed[:4]:
+        assert p.table_records is not None and p.table_records.shape == (8 * p.n, 8)
+    idx = [(0, 2), (2, 0), (3, 1), (1, 3), (0, 4), (4, 2), (3, 3)]
+    for a, b in idx:
+        e = ch.match_ranked(plain[a], plain[b], tables, topk, count_candidates=True)
+        g = ch.match_ranked(plain[a], packed[b], tables, topk, count_candidates=True)
+        torch.cuda.synchronize()
+        assert all(torch.equal(x, y) for x, y in zip(e, g)), (a, b)
+    for trains in (packed, [packed[0], plain[1], packed[2], plain[3], packed[4]]):
+        batch = ch.RankedBatch([(plain[a], trains[b]) for a, b in idx], tables, topk, count_candidates=True)
+        got = batch.launch()
+        torch.cuda.synchronize()
+        assert rsfm.device_error() == 0
+        for (a, b), g in zip(idx, got):
+            e = ch.match_ranked(plain[a], plain[b], tables, topk, count_candidates=True)
+            torch.cuda.synchronize()
+            assert all(torch.equal(x, y) for x, y in zip(e, g)), (a, b)
+        batch.close()
 
 
 def test_cascade_matcher_fallback_is_exact(rsfm, oracle):

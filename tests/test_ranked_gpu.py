@@ -27,29 +27,39 @@ def _prep(oracle, desc, w, bias):
             "sqr": oracle.sqr_norm(desc)}
 
 
-def _ranked_image(rsfm, img, keep, records=False):
+def _ranked_image(rsfm, img, keep, records=False, table=False):
     t = {k: _dev(v.view(np.int32) if v.dtype == np.uint32 else v) for k, v in img.items()}
     keep.append(t)
-    rec = 0
-    if records:
+    rec = trec = 0
+    if records or table:
         r = torch.empty((max(len(img["desc"]), 1), 8), dtype=torch.int32, device="cuda")
         keep.append(r)
         rsfm._lib.check(rsfm._lib.load().rsfm_ranked_pack_records(
             ctypes.c_void_p(t["keys"].data_ptr()), ctypes.c_void_p(t["codes"].data_ptr()),
             ctypes.c_void_p(t["sqr"].data_ptr()), len(img["desc"]), ctypes.c_void_p(r.data_ptr()), None), "pack")
         rec = r.data_ptr()
+    if table:  # each table's records in its bucket-list order: one warp per query over record runs
+        tr = torch.empty((8 * max(len(img["desc"]), 1), 8), dtype=torch.int32, device="cuda")
+        keep.append(tr)
+        rsfm._lib.check(rsfm._lib.load().rsfm_ranked_pack_table_records(
+            ctypes.c_void_p(rec), ctypes.c_void_p(t["buckets"].data_ptr()), len(img["desc"]),
+            ctypes.c_void_p(tr.data_ptr()), None), "pack table records")
+        trec = tr.data_ptr()
+        if not records:
+            rec = 0
     return rsfm._lib.RankedImage(t["desc"].data_ptr(), t["keys"].data_ptr(), t["codes"].data_ptr(),
                                  t["upper"].data_ptr(), t["buckets"].data_ptr(), t["sqr"].data_ptr(),
-                                 len(img["desc"]), rec)
+                                 len(img["desc"]), rec, trec)
 
 
-@pytest.mark.parametrize("records", [False, True])
+@pytest.mark.parametrize("layout", ["plain", "records", "table"])
 # topK <= 12 runs one thread per query, larger topK one warp per query: 12 and 13 sit either side.
+# With table records ("table") the thread kernel reads candidates at their list positions.
 # tables x n not a multiple of 4 (1001 x 3, 999 x 5): the last 16-byte block of the bucket lists
 # would pass their end and is read one entry at a time.
 @pytest.mark.parametrize("n,tables,topk", [(8192, 6, 10), (3000, 6, 10), (1000, 8, 32), (500, 1, 1),
                                            (2000, 4, 12), (2000, 4, 13), (1001, 3, 10), (999, 5, 12)])
-def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, records):
+def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, layout):
     q, t, _ = synth.make_pair(n, n, 0.4, 8.0, seed=n + tables)
     w = _gauss_weights(7)
     acc = oracle.cashash_accumulate(np.concatenate([q, t]))
@@ -57,7 +67,8 @@ def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, records):
     bias = oracle.cashash_bias(w, base, acc, 2 * n)
     Q, T = _prep(oracle, q, w, bias), _prep(oracle, t, w, bias)
     keep = []
-    qi, ti = _ranked_image(rsfm, Q, keep, records), _ranked_image(rsfm, T, keep, records)
+    records, table = layout == "records", layout == "table"
+    qi, ti = _ranked_image(rsfm, Q, keep, records, table), _ranked_image(rsfm, T, keep, records, table)
     best = torch.empty(n, dtype=torch.int64, device="cuda")
     sec = torch.empty(n, dtype=torch.int32, device="cuda")
     flg = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -76,8 +87,10 @@ def test_ranked_matches_oracle(rsfm, oracle, n, tables, topk, records):
     np.testing.assert_array_equal(flg.cpu().numpy().view(np.uint32), ef)
 
 
-def test_ranked_large_candidate_sets(rsfm, oracle):
-    # Few distinct keys: every query has thousands of candidates (buffer flushes + merges).
+@pytest.mark.parametrize("table", [False, True])
+def test_ranked_large_candidate_sets(rsfm, oracle, table):
+    # Few distinct keys: every query has thousands of candidates (buffer flushes + merges), read
+    # through the bucket lists or, with table records, at their list positions.
     n = 4000
     q, t, _ = synth.make_pair(n, n, 0.5, 6.0, seed=3)
     rng = np.random.default_rng(1)
@@ -88,7 +101,7 @@ def test_ranked_large_candidate_sets(rsfm, oracle):
     for img in (Q, T):
         _, _, img["upper"], _, img["buckets"] = oracle.cashash_buckets(img["keys"])
     keep = []
-    qi, ti = _ranked_image(rsfm, Q, keep), _ranked_image(rsfm, T, keep)
+    qi, ti = _ranked_image(rsfm, Q, keep, table=table), _ranked_image(rsfm, T, keep, table=table)
     best = torch.empty(n, dtype=torch.int64, device="cuda")
     sec = torch.empty(n, dtype=torch.int32, device="cuda")
     flg = torch.empty(n, dtype=torch.int32, device="cuda")
