@@ -359,6 +359,55 @@ __device__ __forceinline__ void ldg_record(const uint4* p, uint4& a, uint4& b) {
 constexpr int kThreadBlock = 128;
 constexpr int kThreadMinBlocks = 7;  // 72 registers, 28 warps per SM (6: 80 registers, 2 % slower)
 
+// Exact L2 of the topK best-ranked candidates (top: ascending keys, ~0u = none), then best match,
+// second-best distance, ratio-test flag and candidate count of query i.
+__device__ __forceinline__ void rerank_write(const Img& Q, const Img& T, uint32_t i, const uint32_t (&top)[kThreadTopK],
+                                             uint32_t total, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
+                                             const Out& O) {
+    const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
+    uint4 qr[8];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ldg_record(&qd[2 * k], qr[2 * k], qr[2 * k + 1]);
+    const uint32_t nq = __ldg(&Q.sqr[i]);
+    uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) {
+        if (uint32_t(r) >= topK || top[r] == 0xFFFFFFFFu) continue;
+        const uint32_t jr = top[r] & 0xFFFFFFu;
+        const uint4* td = reinterpret_cast<const uint4*>(T.desc + size_t(jr) * 128);
+        uint32_t dot = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint4 t0, t1;
+            ldg_record(&td[2 * k], t0, t1);  // 32 bytes of the row per load
+            const uint4 q0 = qr[2 * k], q1 = qr[2 * k + 1];
+            dot = __dp4a(q0.x, t0.x, dot);
+            dot = __dp4a(q0.y, t0.y, dot);
+            dot = __dp4a(q0.z, t0.z, dot);
+            dot = __dp4a(q0.w, t0.w, dot);
+            dot = __dp4a(q1.x, t1.x, dot);
+            dot = __dp4a(q1.y, t1.y, dot);
+            dot = __dp4a(q1.z, t1.z, dot);
+            dot = __dp4a(q1.w, t1.w, dot);
+        }
+        const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
+        const uint32_t d = nq + ns - 2u * dot;
+        if (d < bd || (d == bd && jr < bj)) {
+            sd = bd;
+            bd = d;
+            bj = jr;
+        } else if (d < sd) {
+            sd = d;
+        }
+    }
+    O.best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
+    O.second[i] = sd;
+    uint32_t f = 0;
+    if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+    O.flags[i] = f;
+    if (O.nbCand) O.nbCand[i] = total;
+}
+
 // kTrec: the train image has table records (each table's records in its bucket-list order, the
 // index in word 7): a candidate is then one load at its list position instead of a bucket-entry
 // load followed by a record load, and a step takes the next four entries of the list, whatever
@@ -463,49 +512,7 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
             }
         }
     }
-    // exact L2 of the topK best-ranked candidates
-    const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
-    uint4 qr[8];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) ldg_record(&qd[2 * k], qr[2 * k], qr[2 * k + 1]);
-    const uint32_t nq = __ldg(&Q.sqr[i]);
-    uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
-#pragma unroll
-    for (int r = 0; r < kThreadTopK; ++r) {
-        if (uint32_t(r) >= topK || top[r] == 0xFFFFFFFFu) continue;
-        const uint32_t jr = top[r] & 0xFFFFFFu;
-        const uint4* td = reinterpret_cast<const uint4*>(T.desc + size_t(jr) * 128);
-        uint32_t dot = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            uint4 t0, t1;
-            ldg_record(&td[2 * k], t0, t1);  // 32 bytes of the row per load
-            const uint4 q0 = qr[2 * k], q1 = qr[2 * k + 1];
-            dot = __dp4a(q0.x, t0.x, dot);
-            dot = __dp4a(q0.y, t0.y, dot);
-            dot = __dp4a(q0.z, t0.z, dot);
-            dot = __dp4a(q0.w, t0.w, dot);
-            dot = __dp4a(q1.x, t1.x, dot);
-            dot = __dp4a(q1.y, t1.y, dot);
-            dot = __dp4a(q1.z, t1.z, dot);
-            dot = __dp4a(q1.w, t1.w, dot);
-        }
-        const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
-        const uint32_t d = nq + ns - 2u * dot;
-        if (d < bd || (d == bd && jr < bj)) {
-            sd = bd;
-            bd = d;
-            bj = jr;
-        } else if (d < sd) {
-            sd = d;
-        }
-    }
-    O.best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
-    O.second[i] = sd;
-    uint32_t f = 0;
-    if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
-    O.flags[i] = f;
-    if (O.nbCand) O.nbCand[i] = total;
+    rerank_write(Q, T, i, top, total, topK, ratioNum, ratioDen, O);
 }
 
 template <bool kTrec>
@@ -555,6 +562,126 @@ __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_
     // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
     if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
     match_query_thread<kTrec>(P.q, P.t, i, tables, topK, ratioNum, ratioDen, P.o);
+}
+
+// ---------------------------------------------------------------- table by table (batch, table records)
+// The candidate walk split into one pass per table. Pass s gives the threads the queries in the order
+// of the query image's table-s bucket lists, so the threads of a warp mostly hold queries of one
+// bucket, whose table-s candidates are one and the same list: the lanes load the same table records
+// (one L1 wavefront for all of them instead of one per lane) and run the same number of steps.
+// Between passes each query's running top-12 and candidate count wait in a 64-byte slot; the pairs
+// are processed in chunks (whole pairs, at most kPassChunk queries unless one pair is larger) whose
+// slots stay in L2. The last pass re-ranks and writes the results. Same results as the kernels above:
+// the same candidates in the same tables, the same keys, the same top-K set.
+constexpr uint32_t kPassChunk = 1u << 20;
+constexpr int kPassBlock = 128;
+constexpr int kPassMinBlocks = 8;  // 64 registers; the last pass (re-rank) keeps the thread kernel's 72
+
+__device__ __forceinline__ void stg_record(uint4* p, const uint4& a, const uint4& b) {
+    asm volatile("st.global.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+                 "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                 : "memory");
+}
+
+// Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
+template <uint32_t S, bool kLast>
+__global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMinBlocks) ranked_pass_kernel(
+    const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, const uint32_t* __restrict__ blockPair,
+    uint32_t g0, uint32_t g1, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, uint4* __restrict__ state) {
+    const uint32_t g = g0 + blockIdx.x * kPassBlock + threadIdx.x;
+    if (g >= g1) return;
+    uint32_t top[kThreadTopK], total = 0;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
+    {
+        uint32_t lo = __ldg(&blockPair[blockIdx.x]);
+        uint32_t hi = __ldg(&blockPair[blockIdx.x + 1]);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&begin[mid]) <= g) lo = mid; else hi = mid - 1;
+        }
+        const PairDev& P = pairs[lo];
+        const uint32_t b0 = __ldg(&begin[lo]);
+        uint32_t i = g - b0;
+        if (P.q.buckets) i = __ldg(&P.q.buckets[size_t(S) * P.q.n + i]);
+        uint4* slot = state + 4 * size_t(b0 + i - g0);
+        if (S > 0) {
+            uint4 a, b, c, d;
+            ldg_record(slot, a, b);
+            ldg_record(slot + 2, c, d);
+            top[0] = a.x, top[1] = a.y, top[2] = a.z, top[3] = a.w;
+            top[4] = b.x, top[5] = b.y, top[6] = b.z, top[7] = b.w;
+            top[8] = c.x, top[9] = c.y, top[10] = c.z, top[11] = c.w;
+            total = d.x;
+        }
+        const Img& T = P.t;
+        if (T.n) {
+            uint2 qk;
+            uint4 qc;
+            if (P.q.rec) {  // the query's packed record: keys and code in one load
+                uint4 r0, r1;
+                ldg_record(&P.q.rec[2 * size_t(i)], r0, r1);
+                qk = make_uint2(r0.x, r0.y);
+                qc = make_uint4(r0.z, r0.w, r1.x, r1.y);
+            } else {
+                qk = __ldg(&P.q.keys[i]);
+                qc = __ldg(&P.q.codes[i]);
+            }
+            const uint32_t bk = ((S < 4 ? qk.x : qk.y) >> (8 * (S & 3u))) & 0xFFu;
+            uint32_t x = bk ? __ldg(&T.ends[S * 256 + bk - 1]) : 0u;
+            const uint32_t end = __ldg(&T.ends[S * 256 + bk]);
+            const uint4* rec = T.trec + 2 * size_t(S) * T.n;
+            for (; x < end; x += 4) {
+                const uint32_t cnt = min(4u, end - x);
+                uint4 r0[4], r1[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (uint32_t(u) < cnt) ldg_record(&rec[2 * size_t(x + u)], r0[u], r1[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (uint32_t(u) >= cnt) continue;
+                    if (S > 0 && collides_before(make_uint2(r0[u].x, r0[u].y), qk, S)) continue;
+                    ++total;
+                    const uint32_t h = __popc(r0[u].z ^ qc.x) + __popc(r0[u].w ^ qc.y) + __popc(r1[u].x ^ qc.z) +
+                                       __popc(r1[u].y ^ qc.w);
+                    uint32_t key = (h << 24) | r1[u].w;
+                    if (key < top[kThreadTopK - 1]) {
+#pragma unroll
+                        for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
+                            const uint32_t v = top[r];
+                            top[r] = min(v, key);
+                            key = max(v, key);
+                        }
+                    }
+                }
+            }
+        }
+        if (kLast) {
+            rerank_write(P.q, T, i, top, total, topK, ratioNum, ratioDen, P.o);
+        } else {
+            stg_record(slot, make_uint4(top[0], top[1], top[2], top[3]), make_uint4(top[4], top[5], top[6], top[7]));
+            stg_record(slot + 2, make_uint4(top[8], top[9], top[10], top[11]), make_uint4(total, 0u, 0u, 0u));
+        }
+    }
+}
+
+using PassKernel = void (*)(const PairDev*, const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint32_t, uint32_t,
+                            uint32_t, uint4*);
+template <uint32_t S>
+constexpr PassKernel pass_kernel(bool last) {
+    return last ? ranked_pass_kernel<S, true> : ranked_pass_kernel<S, false>;
+}
+inline PassKernel pass_kernel_for(uint32_t s, bool last) {
+    switch (s) {
+        case 0: return pass_kernel<0>(last);
+        case 1: return pass_kernel<1>(last);
+        case 2: return pass_kernel<2>(last);
+        case 3: return pass_kernel<3>(last);
+        case 4: return pass_kernel<4>(last);
+        case 5: return pass_kernel<5>(last);
+        case 6: return pass_kernel<6>(last);
+        default: return pass_kernel<7>(last);
+    }
 }
 
 // Kernel choice: one thread per query when topK fits the register list, unless
@@ -626,12 +753,20 @@ struct rsfm_ranked_batch {
     uint32_t* dBegin = nullptr;
     uint32_t nPairs = 0, total = 0, tables = 0, topK = 0, ratioNum = 0, ratioDen = 1;
     bool tableRecords = false;  // every train image with work has table records
+    uint4* dState = nullptr;    // per-table passes: 64-byte slot per query of the largest chunk
+    uint32_t* dBlockPair = nullptr;  // per chunk and pass block: first pair of the block, then a sentinel
+    struct Chunk {
+        uint32_t g0, g1, blockPair;  // query range of whole pairs, offset of its block-pair table
+    };
+    std::vector<Chunk> chunks;
 };
 
 extern "C" int rsfm_ranked_batch_destroy(rsfm_ranked_batch* b) {
     if (!b) return RSFM_OK;
     if (b->dPairs) cudaFree(b->dPairs);
     if (b->dBegin) cudaFree(b->dBegin);
+    if (b->dState) cudaFree(b->dState);
+    if (b->dBlockPair) cudaFree(b->dBlockPair);
     delete b;
     return RSFM_OK;
 }
@@ -696,6 +831,37 @@ extern "C" int rsfm_ranked_batch_create(const rsfm_ranked_pair* pairs, uint32_t 
     b->ratioNum = ratioNum;
     b->ratioDen = ratioDen;
     b->tableRecords = allTrec;
+    if (allTrec && chr::use_thread_kernel(topK) && total) {
+        // per-table passes over chunks of whole pairs; for every pass block the range of pairs its
+        // queries fall in (the pair of its first query, then the next block's)
+        std::vector<uint32_t> bp;
+        auto pair_of = [&](uint32_t g) {
+            return uint32_t(std::upper_bound(begin.begin(), begin.begin() + nbPairs, g) - begin.begin()) - 1u;
+        };
+        auto close = [&](uint32_t g0, uint32_t g1) {
+            const uint32_t off = uint32_t(bp.size());
+            for (uint32_t g = g0; g < g1; g += chr::kPassBlock) bp.push_back(pair_of(g));
+            bp.push_back(pair_of(g1 - 1));
+            b->chunks.push_back({g0, g1, off});
+        };
+        uint32_t g0 = 0, most = 0;
+        for (uint32_t p = 0; p < nbPairs; ++p) {
+            if (begin[p + 1] - g0 > chr::kPassChunk && begin[p] > g0) {
+                close(g0, begin[p]);
+                most = std::max(most, begin[p] - g0);
+                g0 = begin[p];
+            }
+        }
+        close(g0, begin[nbPairs]);
+        most = std::max(most, begin[nbPairs] - g0);
+        if (cudaMalloc(reinterpret_cast<void**>(&b->dState), size_t(most) * 64) != cudaSuccess ||
+            cudaMalloc(reinterpret_cast<void**>(&b->dBlockPair), sizeof(uint32_t) * bp.size()) != cudaSuccess ||
+            cudaMemcpy(b->dBlockPair, bp.data(), sizeof(uint32_t) * bp.size(), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+            rsfm_ranked_batch_destroy(b);
+            return RSFM_ERR_CUDA;
+        }
+    }
     *out = b;
     return RSFM_OK;
 }
@@ -706,7 +872,19 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
     if (b->total == 0) return RSFM_OK;
     void* tok = nullptr;
     const bool prof = profile_begin(stream, &tok);
-    if (chr::use_thread_kernel(b->topK)) {
+    uint32_t launches = 1;
+    if (b->dState) {
+        launches = 0;
+        for (const auto& c : b->chunks) {
+            const uint32_t grid = (c.g1 - c.g0 + chr::kPassBlock - 1) / chr::kPassBlock;
+            for (uint32_t s = 0; s < b->tables; ++s) {
+                chr::pass_kernel_for(s, s + 1 == b->tables)<<<grid, chr::kPassBlock, 0, stream>>>(
+                    b->dPairs, b->dBegin, b->dBlockPair + c.blockPair, c.g0, c.g1, b->topK, b->ratioNum, b->ratioDen,
+                    b->dState);
+                ++launches;
+            }
+        }
+    } else if (chr::use_thread_kernel(b->topK)) {
         const uint32_t grid = (b->total + chr::kThreadBlock - 1) / chr::kThreadBlock;
         if (b->tableRecords)
             chr::ranked_thread_batch_kernel<true><<<grid, chr::kThreadBlock, 0, stream>>>(
@@ -721,7 +899,7 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
     }
     RSFM_CUDA_TRY(cudaGetLastError());
     if (prof) profile_end(stream, tok);
-    launch_count_add(1);
+    launch_count_add(launches);
     return RSFM_OK;
 }
 

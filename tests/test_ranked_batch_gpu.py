@@ -1,6 +1,8 @@
 """Batched ranked matching (one launch over many pairs) gives the per-pair results, and the
 cascade matcher's brute-force fallback gives the exact matcher's results (no reference
 counterpart for either)."""
+import copy
+
 import numpy as np
 import pytest
 import torch
@@ -220,3 +222,75 @@ def test_find_best_match_batch_repeated_and_many_pairs(rsfm, oracle):
         np.testing.assert_array_equal(bq.cpu().numpy().view(np.uint32).reshape(-1, 2), eq)
         np.testing.assert_array_equal(bt.cpu().numpy().view(np.uint32).reshape(-1, 2), et)
     batch.close()
+
+
+def _host(x):
+    return x.cpu().numpy()
+
+
+@pytest.mark.parametrize("tables,topk", [(6, 10), (1, 3), (8, 12)])
+def test_batch_table_passes_match_oracle(rsfm, oracle, tables, topk):
+    """The batch over train images with table records (one pass per table, queries in the order of
+    their own bucket in that table, top lists carried between passes) against the oracle, pair by
+    pair; pairs with a one-descriptor query, an empty query and an empty train image."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(21))
+    rng = np.random.default_rng(21)
+    descs = []
+    for k, (na, nb) in enumerate([(3000, 2500), (800, 4096), (1, 700)]):
+        q, t, _ = synth.make_pair(na, nb, float(rng.uniform(0.2, 0.6)), 8.0, seed=2100 + k)
+        descs += [_dev(q), _dev(t)]
+    for d in descs:
+        cas.fit(d)
+    empty = torch.empty((0, 128), dtype=torch.uint8, device="cuda")
+    imgs = ch.register_ranked_images(cas, descs + [empty], table_records=True)
+    pairs = [(imgs[0], imgs[1]), (imgs[2], imgs[3]), (imgs[4], imgs[5]), (imgs[6], imgs[1]), (imgs[0], imgs[6])]
+    batch = ch.RankedBatch(pairs, tables, topk, count_candidates=True)
+    got = batch.launch()
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    for (qi, ti), (b, s, f, c) in zip(pairs, got):
+        if qi.n == 0:
+            continue
+        eb, es, ef, ec = oracle.cashash_match_ranked(_host(qi.desc), _host(qi.keys), _host(qi.codes).view(np.uint32),
+                                                     _host(ti.desc), _host(ti.keys), _host(ti.codes).view(np.uint32),
+                                                     tables=tables, top_k=topk)
+        np.testing.assert_array_equal(_host(c).view(np.uint32), ec)
+        np.testing.assert_array_equal(_host(b).view(np.uint32).reshape(-1, 2), eb)
+        np.testing.assert_array_equal(_host(s).view(np.uint32), es)
+        np.testing.assert_array_equal(_host(f).view(np.uint32), ef)
+    batch.close()
+
+
+def test_batch_table_passes_in_chunks(rsfm):
+    """More than 2^20 queries: the per-table passes run over chunks of whole pairs (one pair alone
+    above the chunk size), with results equal to the one-thread-per-query kernel's on the same
+    images without table records."""
+    from rapidsfm_b200 import cashash as ch
+    cas = ch.CasHash(ch.gaussian_weights(23))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(23)
+    sizes = [(1100000, 3000), (300000, 8192), (400000, 8192), (500000, 2000), (5000, 5000)]
+    descs = []
+    for na, nb in sizes:
+        q, t = synth.make_pair_torch(na, nb, 0.4, 8.0, g, "cuda")[:2]
+        descs += [q, t]
+    for d in descs[:2]:
+        cas.fit(d)
+    imgs = ch.register_ranked_images(cas, descs, table_records=True)
+    pairs = list(zip(imgs[0::2], imgs[1::2]))
+    bare = []
+    for q, t in pairs:
+        b = copy.copy(t)
+        b.table_records = None
+        bare.append((q, b))
+    for tables, topk in ((6, 10), (2, 12)):
+        got = ch.RankedBatch(pairs, tables, topk, count_candidates=True)
+        ref = ch.RankedBatch(bare, tables, topk, count_candidates=True)
+        a, e = got.launch(), ref.launch()
+        torch.cuda.synchronize()
+        assert rsfm.device_error() == 0
+        for x, y in zip(a, e):
+            assert all(torch.equal(u, v) for u, v in zip(x, y))
+        got.close()
+        ref.close()
