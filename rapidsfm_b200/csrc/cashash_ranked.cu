@@ -583,6 +583,69 @@ __device__ __forceinline__ void stg_record(uint4* p, const uint4& a, const uint4
                  : "memory");
 }
 
+// collides_before for a table index known at compile time: a byte of t ^ q is zero where the keys
+// agree; (v - 0x01..01) & ~v & 0x80..80 flags the lowest zero byte of v exactly (flags above it may
+// be spurious, but only above a real zero byte), so masking to the first S bytes is exact.
+__host__ __device__ constexpr uint32_t zero_byte_mask(uint32_t bytes) {
+    return bytes >= 4 ? 0x80808080u : (0x80808080u & ((1u << (8 * bytes)) - 1u));
+}
+template <uint32_t S>
+__device__ __forceinline__ bool collides_before_c(uint2 t, uint2 q) {
+    if (S == 0) return false;
+    const uint32_t vx = t.x ^ q.x;
+    uint32_t f = (vx - 0x01010101u) & ~vx & zero_byte_mask(S);
+    if (S > 4) {
+        const uint32_t vy = t.y ^ q.y;
+        f |= (vy - 0x01010101u) & ~vy & zero_byte_mask(S > 4 ? S - 4 : 0);
+    }
+    return f != 0u;
+}
+
+__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {  // a <- min, b <- max
+    const uint32_t x = min(a, b);
+    b = max(a, b);
+    a = x;
+}
+
+// top (ascending, kThreadTopK = 12) <- the 12 smallest of top and k[0..3]. k is sorted (5 compare-
+// exchanges), reversed behind top to form a bitonic sequence of 16, and merged keeping the lower 12:
+// the first half-cleaner only touches top[4..7] (top[i] <= top[i + 8] already), the lower 8 are
+// sorted by a bitonic merge, the upper 4 are the minima of the upper half's next half-cleaner,
+// sorted the same way. Same list as inserting the four keys one by one (keys are distinct).
+__device__ __forceinline__ void merge4(uint32_t (&top)[kThreadTopK], uint32_t (&k)[4]) {
+    cas(k[0], k[1]);
+    cas(k[2], k[3]);
+    cas(k[0], k[2]);
+    cas(k[1], k[3]);
+    cas(k[1], k[2]);
+    if (k[0] >= top[kThreadTopK - 1]) return;
+    // x[0..11] = top, x[12..15] = k[3], k[2], k[1], k[0]; half-cleaner at distance 8
+    uint32_t u[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        u[i] = top[i + 8];                // i < 4: top[i] <= top[i + 8]
+        const uint32_t a = top[i + 4], b = k[3 - i];
+        top[i + 4] = min(a, b);
+        u[i + 4] = max(a, b);
+    }
+    // lower 8 (bitonic): merge at distances 4, 2, 1
+#pragma unroll
+    for (int d = 4; d > 0; d >>= 1)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if ((i & d) == 0) cas(top[i], top[i + d]);
+    // upper 8 (bitonic): its 4 smallest are the minima at distance 4, then merge at distances 2, 1
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) w[i] = min(u[i], u[i + 4]);
+    cas(w[0], w[2]);
+    cas(w[1], w[3]);
+    cas(w[0], w[1]);
+    cas(w[2], w[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) top[8 + i] = w[i];
+}
+
 // Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
 template <uint32_t S, bool kLast>
 __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMinBlocks) ranked_pass_kernel(
@@ -637,23 +700,17 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     if (uint32_t(u) < cnt) ldg_record(&rec[2 * size_t(x + u)], r0[u], r1[u]);
+                uint32_t k[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    if (uint32_t(u) >= cnt) continue;
-                    if (S > 0 && collides_before(make_uint2(r0[u].x, r0[u].y), qk, S)) continue;
+                    k[u] = 0xFFFFFFFFu;
+                    if (uint32_t(u) >= cnt || collides_before_c<S>(make_uint2(r0[u].x, r0[u].y), qk)) continue;
                     ++total;
                     const uint32_t h = __popc(r0[u].z ^ qc.x) + __popc(r0[u].w ^ qc.y) + __popc(r1[u].x ^ qc.z) +
                                        __popc(r1[u].y ^ qc.w);
-                    uint32_t key = (h << 24) | r1[u].w;
-                    if (key < top[kThreadTopK - 1]) {
-#pragma unroll
-                        for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
-                            const uint32_t v = top[r];
-                            top[r] = min(v, key);
-                            key = max(v, key);
-                        }
-                    }
+                    k[u] = (h << 24) | r1[u].w;
                 }
+                merge4(top, k);
             }
         }
         if (kLast) {

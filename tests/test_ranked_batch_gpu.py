@@ -294,3 +294,32 @@ def test_batch_table_passes_in_chunks(rsfm):
             assert all(torch.equal(u, v) for u, v in zip(x, y))
         got.close()
         ref.close()
+
+
+@pytest.mark.parametrize("tables,topk", [(6, 10), (8, 12), (5, 1)])
+def test_batch_table_passes_many_collisions(rsfm, oracle, tables, topk):
+    """Key bytes drawn from {0, 1}: every query has thousands of candidates and most of them
+    collide with it in several tables (the duplicate test drops all but the first), through the
+    per-table passes, against the oracle."""
+    from rapidsfm_b200 import cashash as ch
+    rng = np.random.default_rng(31)
+    n = 3000
+    q, t, _ = synth.make_pair(n, n, 0.5, 6.0, seed=31)
+    imgs = []
+    for d in (q, t):
+        keys = rng.integers(0, 2, size=(n, 8)).astype(np.uint8)
+        codes = rng.integers(0, 2**32, size=(n, 4), dtype=np.uint64).astype(np.uint32)
+        imgs.append(ch.RankedImage(_dev(d), _dev(keys), _dev(codes.view(np.int32))))
+    imgs[1].pack_table_records()
+    batch = ch.RankedBatch([(imgs[0], imgs[1])], tables, topk, count_candidates=True)
+    (b, s, f, c), = batch.launch()
+    torch.cuda.synchronize()
+    assert rsfm.device_error() == 0
+    eb, es, ef, ec = oracle.cashash_match_ranked(q, _host(imgs[0].keys), _host(imgs[0].codes).view(np.uint32), t,
+                                                 _host(imgs[1].keys), _host(imgs[1].codes).view(np.uint32),
+                                                 tables=tables, top_k=topk)
+    np.testing.assert_array_equal(_host(c).view(np.uint32), ec)
+    np.testing.assert_array_equal(_host(b).view(np.uint32).reshape(-1, 2), eb)
+    np.testing.assert_array_equal(_host(s).view(np.uint32), es)
+    np.testing.assert_array_equal(_host(f).view(np.uint32), ef)
+    batch.close()
