@@ -342,9 +342,9 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
 // ---------------------------------------------------------------- one thread per query
 // The same matching with one query per thread (for topK <= kThreadTopK = 12): the candidate walk,
 // duplicate test and Hamming key are per-thread scalar work with no cross-lane traffic, the
-// running top-K is a sorted register list (one compare-exchange pass per insertion; keys past
-// the kThreadTopK-th are rejected by one compare), and the re-rank reads each ranked train
-// descriptor as eight 16-byte loads. Results are identical to the warp kernel: same keys, same
+// running top-K is a sorted register list (each step's four keys sorted and merged into it by a
+// compare-exchange network, skipped when none beats the kThreadTopK-th), and the re-rank reads
+// each ranked train descriptor as four 32-byte loads. Results are identical to the warp kernel: same keys, same
 // set of the topK smallest, same exact re-rank rule.
 constexpr int kThreadTopK = 12;
 
@@ -358,6 +358,51 @@ __device__ __forceinline__ void ldg_record(const uint4* p, uint4& a, uint4& b) {
 }
 constexpr int kThreadBlock = 128;
 constexpr int kThreadMinBlocks = 7;  // 72 registers, 28 warps per SM (6: 80 registers, 2 % slower)
+
+__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {  // a <- min, b <- max
+    const uint32_t x = min(a, b);
+    b = max(a, b);
+    a = x;
+}
+
+// top (ascending, kThreadTopK = 12) <- the 12 smallest of top and k[0..3]. k is sorted (5 compare-
+// exchanges), reversed behind top to form a bitonic sequence of 16, and merged keeping the lower 12:
+// the first half-cleaner only touches top[4..7] (top[i] <= top[i + 8] already), the lower 8 are
+// sorted by a bitonic merge, the upper 4 are the minima of the upper half's next half-cleaner,
+// sorted the same way. Same list as inserting the four keys one by one (keys are distinct).
+__device__ __forceinline__ void merge4(uint32_t (&top)[kThreadTopK], uint32_t (&k)[4]) {
+    cas(k[0], k[1]);
+    cas(k[2], k[3]);
+    cas(k[0], k[2]);
+    cas(k[1], k[3]);
+    cas(k[1], k[2]);
+    if (k[0] >= top[kThreadTopK - 1]) return;
+    // x[0..11] = top, x[12..15] = k[3], k[2], k[1], k[0]; half-cleaner at distance 8
+    uint32_t u[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        u[i] = top[i + 8];                // i < 4: top[i] <= top[i + 8]
+        const uint32_t a = top[i + 4], b = k[3 - i];
+        top[i + 4] = min(a, b);
+        u[i + 4] = max(a, b);
+    }
+    // lower 8 (bitonic): merge at distances 4, 2, 1
+#pragma unroll
+    for (int d = 4; d > 0; d >>= 1)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if ((i & d) == 0) cas(top[i], top[i + d]);
+    // upper 8 (bitonic): its 4 smallest are the minima at distance 4, then merge at distances 2, 1
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) w[i] = min(u[i], u[i + 4]);
+    cas(w[0], w[2]);
+    cas(w[1], w[3]);
+    cas(w[0], w[1]);
+    cas(w[2], w[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) top[8 + i] = w[i];
+}
 
 // Exact L2 of the topK best-ranked candidates (top: ascending keys, ~0u = none), then best match,
 // second-best distance, ratio-test flag and candidate count of query i.
@@ -495,22 +540,17 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
                 }
             }
         }
+        uint32_t k[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
+            k[u] = 0xFFFFFFFFu;
             if (j[u] == 0xFFFFFFFFu || collides_before(tk[u], qk, su[u])) continue;
             ++total;
             const uint32_t h = __popc(tc[u].x ^ qc.x) + __popc(tc[u].y ^ qc.y) + __popc(tc[u].z ^ qc.z) +
                                __popc(tc[u].w ^ qc.w);
-            uint32_t key = (h << 24) | j[u];
-            if (key < top[kThreadTopK - 1]) {
-#pragma unroll
-                for (int r = 0; r < kThreadTopK; ++r) {  // insert: keep the smaller, carry the larger
-                    const uint32_t a = top[r];
-                    top[r] = min(a, key);
-                    key = max(a, key);
-                }
-            }
+            k[u] = (h << 24) | j[u];
         }
+        merge4(top, k);
     }
     rerank_write(Q, T, i, top, total, topK, ratioNum, ratioDen, O);
 }
@@ -599,51 +639,6 @@ __device__ __forceinline__ bool collides_before_c(uint2 t, uint2 q) {
         f |= (vy - 0x01010101u) & ~vy & zero_byte_mask(S > 4 ? S - 4 : 0);
     }
     return f != 0u;
-}
-
-__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {  // a <- min, b <- max
-    const uint32_t x = min(a, b);
-    b = max(a, b);
-    a = x;
-}
-
-// top (ascending, kThreadTopK = 12) <- the 12 smallest of top and k[0..3]. k is sorted (5 compare-
-// exchanges), reversed behind top to form a bitonic sequence of 16, and merged keeping the lower 12:
-// the first half-cleaner only touches top[4..7] (top[i] <= top[i + 8] already), the lower 8 are
-// sorted by a bitonic merge, the upper 4 are the minima of the upper half's next half-cleaner,
-// sorted the same way. Same list as inserting the four keys one by one (keys are distinct).
-__device__ __forceinline__ void merge4(uint32_t (&top)[kThreadTopK], uint32_t (&k)[4]) {
-    cas(k[0], k[1]);
-    cas(k[2], k[3]);
-    cas(k[0], k[2]);
-    cas(k[1], k[3]);
-    cas(k[1], k[2]);
-    if (k[0] >= top[kThreadTopK - 1]) return;
-    // x[0..11] = top, x[12..15] = k[3], k[2], k[1], k[0]; half-cleaner at distance 8
-    uint32_t u[8];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        u[i] = top[i + 8];                // i < 4: top[i] <= top[i + 8]
-        const uint32_t a = top[i + 4], b = k[3 - i];
-        top[i + 4] = min(a, b);
-        u[i + 4] = max(a, b);
-    }
-    // lower 8 (bitonic): merge at distances 4, 2, 1
-#pragma unroll
-    for (int d = 4; d > 0; d >>= 1)
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-            if ((i & d) == 0) cas(top[i], top[i + d]);
-    // upper 8 (bitonic): its 4 smallest are the minima at distance 4, then merge at distances 2, 1
-    uint32_t w[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) w[i] = min(u[i], u[i + 4]);
-    cas(w[0], w[2]);
-    cas(w[1], w[3]);
-    cas(w[0], w[1]);
-    cas(w[2], w[3]);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) top[8 + i] = w[i];
 }
 
 // Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
