@@ -641,18 +641,88 @@ __device__ __forceinline__ bool collides_before_c(uint2 t, uint2 q) {
     return f != 0u;
 }
 
+// The exact re-rank of a warp's queries by groups of 4 lanes, each lane reading 32 bytes of the
+// same train row (a load touches one cache line per row instead of one per lane and 32-byte piece).
+// Group G takes the queries of lanes 4G .. 4G + 3 in turn; their indices come through shared
+// memory (rows of 17 words: the 8 groups' reads fall in different banks). The train norm comes from
+// the row itself: each lane accumulates sum(t^2) - 2 sum(q t) over its 32 bytes (mod 2^32, as the
+// norms and distances are), so d = |q|^2 + the group's sum — the value nq + ns - 2 dot of
+// rerank_write. Same best / second-best rule. All 32 lanes of the warp call it.
+constexpr int kRowWords = 17;
+__device__ __forceinline__ void rerank_group4(const PairDev* __restrict__ pairs, bool live, uint32_t pair, uint32_t i,
+                                              const uint32_t (&top)[kThreadTopK], uint32_t total, uint32_t topK,
+                                              uint32_t ratioNum, uint32_t ratioDen, uint32_t* rows) {
+    const uint32_t lane = threadIdx.x & 31u, grp = lane >> 2, part = lane & 3u;
+    uint32_t* mine = rows + lane * kRowWords;
+    mine[0] = live ? 1u : 0u;
+    mine[1] = pair;
+    mine[2] = i;
+    mine[3] = total;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) mine[4 + r] = top[r];
+    __syncwarp();
+    const uint32_t gmask = 0xFu << (4 * grp);
+#pragma unroll 1
+    for (uint32_t qq = 0; qq < 4; ++qq) {
+        const uint32_t* row = rows + (4 * grp + qq) * kRowWords;
+        if (row[0] == 0u) continue;  // the same for the 4 lanes of a group
+        const PairDev& P = pairs[row[1]];
+        const uint32_t iq = row[2];
+        uint4 q0, q1;
+        ldg_record(reinterpret_cast<const uint4*>(P.q.desc + size_t(iq) * 128) + 2 * part, q0, q1);
+        const uint32_t nq = __ldg(&P.q.sqr[iq]);
+        uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+#pragma unroll 1
+        for (uint32_t r = 0; r < topK; ++r) {
+            const uint32_t key = row[4 + r];
+            if (key == 0xFFFFFFFFu) break;
+            const uint32_t jr = key & 0xFFFFFFu;
+            uint4 t0, t1;
+            ldg_record(reinterpret_cast<const uint4*>(P.t.desc + size_t(jr) * 128) + 2 * part, t0, t1);
+            uint32_t tt = __dp4a(t0.x, t0.x, 0u), qt = __dp4a(q0.x, t0.x, 0u);
+            tt = __dp4a(t0.y, t0.y, tt), qt = __dp4a(q0.y, t0.y, qt);
+            tt = __dp4a(t0.z, t0.z, tt), qt = __dp4a(q0.z, t0.z, qt);
+            tt = __dp4a(t0.w, t0.w, tt), qt = __dp4a(q0.w, t0.w, qt);
+            tt = __dp4a(t1.x, t1.x, tt), qt = __dp4a(q1.x, t1.x, qt);
+            tt = __dp4a(t1.y, t1.y, tt), qt = __dp4a(q1.y, t1.y, qt);
+            tt = __dp4a(t1.z, t1.z, tt), qt = __dp4a(q1.z, t1.z, qt);
+            tt = __dp4a(t1.w, t1.w, tt), qt = __dp4a(q1.w, t1.w, qt);
+            uint32_t v = tt - 2u * qt;
+            v += __shfl_xor_sync(gmask, v, 1);
+            v += __shfl_xor_sync(gmask, v, 2);
+            const uint32_t d = nq + v;
+            if (d < bd || (d == bd && jr < bj)) {
+                sd = bd;
+                bd = d;
+                bj = jr;
+            } else if (d < sd) {
+                sd = d;
+            }
+        }
+        if (part == 0) {
+            P.o.best[iq] = (static_cast<unsigned long long>(bd) << 32) | bj;
+            P.o.second[iq] = sd;
+            uint32_t f = 0;
+            if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+            P.o.flags[iq] = f;
+            if (P.o.nbCand) P.o.nbCand[iq] = row[3];
+        }
+    }
+}
+
 // Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
 template <uint32_t S, bool kLast>
 __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMinBlocks) ranked_pass_kernel(
     const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, const uint32_t* __restrict__ blockPair,
     uint32_t g0, uint32_t g1, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, uint4* __restrict__ state) {
     const uint32_t g = g0 + blockIdx.x * kPassBlock + threadIdx.x;
-    if (g >= g1) return;
-    uint32_t top[kThreadTopK], total = 0;
+    const bool live = g < g1;
+    if (!kLast && !live) return;  // the last pass re-ranks by lane groups: every lane stays
+    uint32_t top[kThreadTopK], total = 0, lo = 0, i = 0;
 #pragma unroll
     for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
-    {
-        uint32_t lo = __ldg(&blockPair[blockIdx.x]);
+    if (live) {
+        lo = __ldg(&blockPair[blockIdx.x]);
         uint32_t hi = __ldg(&blockPair[blockIdx.x + 1]);
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
@@ -660,7 +730,7 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
         }
         const PairDev& P = pairs[lo];
         const uint32_t b0 = __ldg(&begin[lo]);
-        uint32_t i = g - b0;
+        i = g - b0;
         if (P.q.buckets) i = __ldg(&P.q.buckets[size_t(S) * P.q.n + i]);
         uint4* slot = state + 4 * size_t(b0 + i - g0);
         if (S > 0) {
@@ -708,12 +778,14 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
                 merge4(top, k);
             }
         }
-        if (kLast) {
-            rerank_write(P.q, T, i, top, total, topK, ratioNum, ratioDen, P.o);
-        } else {
+        if (!kLast) {
             stg_record(slot, make_uint4(top[0], top[1], top[2], top[3]), make_uint4(top[4], top[5], top[6], top[7]));
             stg_record(slot + 2, make_uint4(top[8], top[9], top[10], top[11]), make_uint4(total, 0u, 0u, 0u));
         }
+    }
+    if constexpr (kLast) {
+        __shared__ uint32_t rows[kPassBlock / 32][32 * kRowWords];
+        rerank_group4(pairs, live, lo, i, top, total, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
     }
 }
 
