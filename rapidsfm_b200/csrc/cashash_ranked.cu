@@ -343,9 +343,9 @@ __global__ void __launch_bounds__(32 * kWarps, 4) ranked_batch_kernel(const Pair
 // The same matching with one query per thread (for topK <= kThreadTopK = 12): the candidate walk,
 // duplicate test and Hamming key are per-thread scalar work with no cross-lane traffic, the
 // running top-K is a sorted register list (each step's four keys sorted and merged into it by a
-// compare-exchange network, skipped when none beats the kThreadTopK-th), and the re-rank reads
-// each ranked train descriptor as four 32-byte loads. Results are identical to the warp kernel: same keys, same
-// set of the topK smallest, same exact re-rank rule.
+// compare-exchange network, skipped when none beats the kThreadTopK-th), and the re-rank is done by
+// groups of four lanes per train row (rerank_group4). Results are identical to the warp kernel: same
+// keys, same set of the topK smallest, same exact re-rank rule.
 constexpr int kThreadTopK = 12;
 
 // 32 bytes in one load (256-bit, read-only path): each thread of a warp reads a different
@@ -404,53 +404,86 @@ __device__ __forceinline__ void merge4(uint32_t (&top)[kThreadTopK], uint32_t (&
     for (int i = 0; i < 4; ++i) top[8 + i] = w[i];
 }
 
-// Exact L2 of the topK best-ranked candidates (top: ascending keys, ~0u = none), then best match,
-// second-best distance, ratio-test flag and candidate count of query i.
-__device__ __forceinline__ void rerank_write(const Img& Q, const Img& T, uint32_t i, const uint32_t (&top)[kThreadTopK],
-                                             uint32_t total, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
-                                             const Out& O) {
-    const uint4* qd = reinterpret_cast<const uint4*>(Q.desc + size_t(i) * 128);
-    uint4 qr[8];
+struct PairList {
+    const PairDev* p;
+    __device__ const PairDev& operator[](uint32_t k) const { return p[k]; }
+};
+struct OnePair {
+    PairDev v;
+    __device__ const PairDev& operator[](uint32_t) const { return v; }
+};
+
+// The exact re-rank of a warp's queries by groups of 4 lanes, each lane reading 32 bytes of the
+// same train row (a load touches one cache line per row instead of one per lane and 32-byte piece).
+// Group G takes the queries of lanes 4G .. 4G + 3 in turn; their indices come through shared
+// memory (rows of 17 words: the 8 groups' reads fall in different banks). The train norm comes from
+// the row itself: each lane accumulates sum(t^2) - 2 sum(q t) over its 32 bytes (mod 2^32, as the
+// norms and distances are), so d = |q|^2 + the group's sum = |q|^2 + |t|^2 - 2 q.t exactly. best =
+// lexicographic minimum (d, index) of the topK ranked candidates, second = the smallest d among
+// the others; the ratio flag and candidate count as documented for the C entry points. All 32
+// lanes of the warp call it. pairs[k] gives the PairDev of pair k (PairList: a device array;
+// OnePair: the single pair of a kernel argument).
+constexpr int kRowWords = 17;
+template <class Pairs>
+__device__ __forceinline__ void rerank_group4(const Pairs& pairs, bool live, uint32_t pair, uint32_t i,
+                                              const uint32_t (&top)[kThreadTopK], uint32_t total, uint32_t topK,
+                                              uint32_t ratioNum, uint32_t ratioDen, uint32_t* rows) {
+    const uint32_t lane = threadIdx.x & 31u, grp = lane >> 2, part = lane & 3u;
+    uint32_t* mine = rows + lane * kRowWords;
+    mine[0] = live ? 1u : 0u;
+    mine[1] = pair;
+    mine[2] = i;
+    mine[3] = total;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ldg_record(&qd[2 * k], qr[2 * k], qr[2 * k + 1]);
-    const uint32_t nq = __ldg(&Q.sqr[i]);
-    uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
-#pragma unroll
-    for (int r = 0; r < kThreadTopK; ++r) {
-        if (uint32_t(r) >= topK || top[r] == 0xFFFFFFFFu) continue;
-        const uint32_t jr = top[r] & 0xFFFFFFu;
-        const uint4* td = reinterpret_cast<const uint4*>(T.desc + size_t(jr) * 128);
-        uint32_t dot = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
+    for (int r = 0; r < kThreadTopK; ++r) mine[4 + r] = top[r];
+    __syncwarp();
+    const uint32_t gmask = 0xFu << (4 * grp);
+#pragma unroll 1
+    for (uint32_t qq = 0; qq < 4; ++qq) {
+        const uint32_t* row = rows + (4 * grp + qq) * kRowWords;
+        if (row[0] == 0u) continue;  // the same for the 4 lanes of a group
+        const PairDev& P = pairs[row[1]];
+        const uint32_t iq = row[2];
+        uint4 q0, q1;
+        ldg_record(reinterpret_cast<const uint4*>(P.q.desc + size_t(iq) * 128) + 2 * part, q0, q1);
+        const uint32_t nq = __ldg(&P.q.sqr[iq]);
+        uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
+#pragma unroll 1
+        for (uint32_t r = 0; r < topK; ++r) {
+            const uint32_t key = row[4 + r];
+            if (key == 0xFFFFFFFFu) break;
+            const uint32_t jr = key & 0xFFFFFFu;
             uint4 t0, t1;
-            ldg_record(&td[2 * k], t0, t1);  // 32 bytes of the row per load
-            const uint4 q0 = qr[2 * k], q1 = qr[2 * k + 1];
-            dot = __dp4a(q0.x, t0.x, dot);
-            dot = __dp4a(q0.y, t0.y, dot);
-            dot = __dp4a(q0.z, t0.z, dot);
-            dot = __dp4a(q0.w, t0.w, dot);
-            dot = __dp4a(q1.x, t1.x, dot);
-            dot = __dp4a(q1.y, t1.y, dot);
-            dot = __dp4a(q1.z, t1.z, dot);
-            dot = __dp4a(q1.w, t1.w, dot);
+            ldg_record(reinterpret_cast<const uint4*>(P.t.desc + size_t(jr) * 128) + 2 * part, t0, t1);
+            uint32_t tt = __dp4a(t0.x, t0.x, 0u), qt = __dp4a(q0.x, t0.x, 0u);
+            tt = __dp4a(t0.y, t0.y, tt), qt = __dp4a(q0.y, t0.y, qt);
+            tt = __dp4a(t0.z, t0.z, tt), qt = __dp4a(q0.z, t0.z, qt);
+            tt = __dp4a(t0.w, t0.w, tt), qt = __dp4a(q0.w, t0.w, qt);
+            tt = __dp4a(t1.x, t1.x, tt), qt = __dp4a(q1.x, t1.x, qt);
+            tt = __dp4a(t1.y, t1.y, tt), qt = __dp4a(q1.y, t1.y, qt);
+            tt = __dp4a(t1.z, t1.z, tt), qt = __dp4a(q1.z, t1.z, qt);
+            tt = __dp4a(t1.w, t1.w, tt), qt = __dp4a(q1.w, t1.w, qt);
+            uint32_t v = tt - 2u * qt;
+            v += __shfl_xor_sync(gmask, v, 1);
+            v += __shfl_xor_sync(gmask, v, 2);
+            const uint32_t d = nq + v;
+            if (d < bd || (d == bd && jr < bj)) {
+                sd = bd;
+                bd = d;
+                bj = jr;
+            } else if (d < sd) {
+                sd = d;
+            }
         }
-        const uint32_t ns = T.rec ? __ldg(&T.rec[2 * size_t(jr) + 1].z) : __ldg(&T.sqr[jr]);
-        const uint32_t d = nq + ns - 2u * dot;
-        if (d < bd || (d == bd && jr < bj)) {
-            sd = bd;
-            bd = d;
-            bj = jr;
-        } else if (d < sd) {
-            sd = d;
+        if (part == 0) {
+            P.o.best[iq] = (static_cast<unsigned long long>(bd) << 32) | bj;
+            P.o.second[iq] = sd;
+            uint32_t f = 0;
+            if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
+            P.o.flags[iq] = f;
+            if (P.o.nbCand) P.o.nbCand[iq] = row[3];
         }
     }
-    O.best[i] = (static_cast<unsigned long long>(bd) << 32) | bj;
-    O.second[i] = sd;
-    uint32_t f = 0;
-    if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
-    O.flags[i] = f;
-    if (O.nbCand) O.nbCand[i] = total;
 }
 
 // kTrec: the train image has table records (each table's records in its bucket-list order, the
@@ -458,15 +491,10 @@ __device__ __forceinline__ void rerank_write(const Img& Q, const Img& T, uint32_
 // load followed by a record load, and a step takes the next four entries of the list, whatever
 // their alignment.
 template <bool kTrec>
-__device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
-                                                   uint32_t topK, uint32_t ratioNum, uint32_t ratioDen,
-                                                   const Out& O) {
+__device__ __forceinline__ void walk_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
+                                                  uint32_t (&top)[kThreadTopK], uint32_t& total) {
     const uint2 qk = __ldg(&Q.keys[i]);
     const uint4 qc = __ldg(&Q.codes[i]);
-    uint32_t top[kThreadTopK];
-#pragma unroll
-    for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
-    uint32_t total = 0;
     // One walk over the concatenated bucket lists of all tables (a cursor that moves to the next
     // table when a list ends), four candidates per step, so the threads of a warp stay together
     // across table boundaries. An empty train image has no tables.
@@ -552,15 +580,23 @@ __device__ __forceinline__ void match_query_thread(const Img& Q, const Img& T, u
         }
         merge4(top, k);
     }
-    rerank_write(Q, T, i, top, total, topK, ratioNum, ratioDen, O);
 }
 
 template <bool kTrec>
-__global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_kernel(Img Q, Img T, uint32_t tables, uint32_t topK,
-                                                                      uint32_t ratioNum, uint32_t ratioDen, Out O) {
+__global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_kernel(OnePair P, uint32_t tables,
+                                                                                      uint32_t topK, uint32_t ratioNum,
+                                                                                      uint32_t ratioDen) {
+    __shared__ uint32_t rows[kThreadBlock / 32][32 * kRowWords];
     const uint32_t t = blockIdx.x * kThreadBlock + threadIdx.x;
-    if (t < Q.n)
-        match_query_thread<kTrec>(Q, T, Q.buckets ? __ldg(&Q.buckets[t]) : t, tables, topK, ratioNum, ratioDen, O);
+    const bool live = t < P.v.q.n;
+    uint32_t top[kThreadTopK], total = 0, i = 0;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
+    if (live) {
+        i = P.v.q.buckets ? __ldg(&P.v.q.buckets[t]) : t;
+        walk_query_thread<kTrec>(P.v.q, P.v.t, i, tables, top, total);
+    }
+    rerank_group4(P, live, 0u, i, top, total, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
 }
 
 __device__ __forceinline__ uint32_t pair_of(const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t g) {
@@ -592,16 +628,23 @@ template <bool kTrec>
 __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_batch_kernel(
     const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
     uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
+    __shared__ uint32_t rows[kThreadBlock / 32][32 * kRowWords];
     const uint32_t g = blockIdx.x * kThreadBlock + threadIdx.x;
-    if (g >= total) return;
-    const uint32_t p = pair_of(begin, nPairs, g);
-    const PairDev& P = pairs[p];
-    uint32_t i = g - __ldg(&begin[p]);
-    // Queries in the order of the query image's first-table bucket lists (when it has them):
-    // neighbouring threads then share their first table's candidate list, walk it in step and
-    // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
-    if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
-    match_query_thread<kTrec>(P.q, P.t, i, tables, topK, ratioNum, ratioDen, P.o);
+    const bool live = g < total;
+    uint32_t top[kThreadTopK], cand = 0, i = 0, p = 0;
+#pragma unroll
+    for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
+    if (live) {
+        p = pair_of(begin, nPairs, g);
+        const PairDev& P = pairs[p];
+        i = g - __ldg(&begin[p]);
+        // Queries in the order of the query image's first-table bucket lists (when it has them):
+        // neighbouring threads then share their first table's candidate list, walk it in step and
+        // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
+        if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
+        walk_query_thread<kTrec>(P.q, P.t, i, tables, top, cand);
+    }
+    rerank_group4(PairList{pairs}, live, p, i, top, cand, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------- table by table (batch, table records)
@@ -639,75 +682,6 @@ __device__ __forceinline__ bool collides_before_c(uint2 t, uint2 q) {
         f |= (vy - 0x01010101u) & ~vy & zero_byte_mask(S > 4 ? S - 4 : 0);
     }
     return f != 0u;
-}
-
-// The exact re-rank of a warp's queries by groups of 4 lanes, each lane reading 32 bytes of the
-// same train row (a load touches one cache line per row instead of one per lane and 32-byte piece).
-// Group G takes the queries of lanes 4G .. 4G + 3 in turn; their indices come through shared
-// memory (rows of 17 words: the 8 groups' reads fall in different banks). The train norm comes from
-// the row itself: each lane accumulates sum(t^2) - 2 sum(q t) over its 32 bytes (mod 2^32, as the
-// norms and distances are), so d = |q|^2 + the group's sum — the value nq + ns - 2 dot of
-// rerank_write. Same best / second-best rule. All 32 lanes of the warp call it.
-constexpr int kRowWords = 17;
-__device__ __forceinline__ void rerank_group4(const PairDev* __restrict__ pairs, bool live, uint32_t pair, uint32_t i,
-                                              const uint32_t (&top)[kThreadTopK], uint32_t total, uint32_t topK,
-                                              uint32_t ratioNum, uint32_t ratioDen, uint32_t* rows) {
-    const uint32_t lane = threadIdx.x & 31u, grp = lane >> 2, part = lane & 3u;
-    uint32_t* mine = rows + lane * kRowWords;
-    mine[0] = live ? 1u : 0u;
-    mine[1] = pair;
-    mine[2] = i;
-    mine[3] = total;
-#pragma unroll
-    for (int r = 0; r < kThreadTopK; ++r) mine[4 + r] = top[r];
-    __syncwarp();
-    const uint32_t gmask = 0xFu << (4 * grp);
-#pragma unroll 1
-    for (uint32_t qq = 0; qq < 4; ++qq) {
-        const uint32_t* row = rows + (4 * grp + qq) * kRowWords;
-        if (row[0] == 0u) continue;  // the same for the 4 lanes of a group
-        const PairDev& P = pairs[row[1]];
-        const uint32_t iq = row[2];
-        uint4 q0, q1;
-        ldg_record(reinterpret_cast<const uint4*>(P.q.desc + size_t(iq) * 128) + 2 * part, q0, q1);
-        const uint32_t nq = __ldg(&P.q.sqr[iq]);
-        uint32_t bd = 0xFFFFFFFFu, bj = 0xFFFFFFFFu, sd = 0xFFFFFFFFu;
-#pragma unroll 1
-        for (uint32_t r = 0; r < topK; ++r) {
-            const uint32_t key = row[4 + r];
-            if (key == 0xFFFFFFFFu) break;
-            const uint32_t jr = key & 0xFFFFFFu;
-            uint4 t0, t1;
-            ldg_record(reinterpret_cast<const uint4*>(P.t.desc + size_t(jr) * 128) + 2 * part, t0, t1);
-            uint32_t tt = __dp4a(t0.x, t0.x, 0u), qt = __dp4a(q0.x, t0.x, 0u);
-            tt = __dp4a(t0.y, t0.y, tt), qt = __dp4a(q0.y, t0.y, qt);
-            tt = __dp4a(t0.z, t0.z, tt), qt = __dp4a(q0.z, t0.z, qt);
-            tt = __dp4a(t0.w, t0.w, tt), qt = __dp4a(q0.w, t0.w, qt);
-            tt = __dp4a(t1.x, t1.x, tt), qt = __dp4a(q1.x, t1.x, qt);
-            tt = __dp4a(t1.y, t1.y, tt), qt = __dp4a(q1.y, t1.y, qt);
-            tt = __dp4a(t1.z, t1.z, tt), qt = __dp4a(q1.z, t1.z, qt);
-            tt = __dp4a(t1.w, t1.w, tt), qt = __dp4a(q1.w, t1.w, qt);
-            uint32_t v = tt - 2u * qt;
-            v += __shfl_xor_sync(gmask, v, 1);
-            v += __shfl_xor_sync(gmask, v, 2);
-            const uint32_t d = nq + v;
-            if (d < bd || (d == bd && jr < bj)) {
-                sd = bd;
-                bd = d;
-                bj = jr;
-            } else if (d < sd) {
-                sd = d;
-            }
-        }
-        if (part == 0) {
-            P.o.best[iq] = (static_cast<unsigned long long>(bd) << 32) | bj;
-            P.o.second[iq] = sd;
-            uint32_t f = 0;
-            if (bj != 0xFFFFFFFFu && uint64_t(ratioDen) * bd < uint64_t(ratioNum) * sd) f |= 1u;
-            P.o.flags[iq] = f;
-            if (P.o.nbCand) P.o.nbCand[iq] = row[3];
-        }
-    }
 }
 
 // Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
@@ -785,7 +759,7 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
     }
     if constexpr (kLast) {
         __shared__ uint32_t rows[kPassBlock / 32][32 * kRowWords];
-        rerank_group4(pairs, live, lo, i, top, total, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
+        rerank_group4(PairList{pairs}, live, lo, i, top, total, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
     }
 }
 
@@ -856,12 +830,13 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     const chr::Out O{reinterpret_cast<unsigned long long*>(best), secondDist, flags, nbCandidates};
     if (chr::use_thread_kernel(topK)) {
         const uint32_t grid = (Q.n + chr::kThreadBlock - 1) / chr::kThreadBlock;
+        const chr::OnePair P{chr::PairDev{Q, T, O}};
         if (T.trec)
             chr::ranked_thread_kernel<true>
-                <<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+                <<<grid, chr::kThreadBlock, 0, stream>>>(P, nbTables, topK, ratioNum, ratioDen);
         else
             chr::ranked_thread_kernel<false>
-                <<<grid, chr::kThreadBlock, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
+                <<<grid, chr::kThreadBlock, 0, stream>>>(P, nbTables, topK, ratioNum, ratioDen);
     } else {
         const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
         chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
