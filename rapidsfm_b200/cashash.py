@@ -303,12 +303,15 @@ class CascadeMatcher:
     ranked pipeline: `hasher` (CasHash, or a learned_hash.LearnedHash) gives each image its 8 key
     bytes and 128-bit code at registration; match() runs all pairs in one ranked launch. A pair
     whose train image has a bucket larger than `bucket_limit` in one of the tables used falls back
-    to the exact brute-force matcher."""
+    to the exact brute-force matcher. table_records: also pack each image's records in bucket-list
+    order at registration (8 x 32 bytes more per descriptor), so that batches whose train images all
+    have them run one pass per table (same results, faster)."""
 
     def __init__(self, hasher, tables=6, top_k=10, bucket_limit=512, ratio_num=RATIO_NUM_08,
-                 ratio_den=RATIO_DEN_08):
+                 ratio_den=RATIO_DEN_08, table_records=True):
         self.hasher = hasher
         self.tables, self.top_k, self.bucket_limit = tables, top_k, bucket_limit
+        self.table_records = table_records
         self.ratio = (ratio_num, ratio_den)
         self.images = {}
         self.fallback_pairs = []
@@ -319,7 +322,10 @@ class CascadeMatcher:
             keys, codes = self.hasher.hash(desc, stream=stream)
         else:
             keys, codes, _ = self.hasher.hash(desc, stream=stream)
-        self.images[handle] = RankedImage(desc, keys, codes, stream=stream)
+        img = RankedImage(desc, keys, codes, stream=stream)
+        if self.table_records:
+            img.pack_table_records(stream=stream)
+        self.images[handle] = img
 
     def _bucket_overflow(self, img):
         # largest bucket over the tables in use (bucket sizes from the inclusive upper bounds)

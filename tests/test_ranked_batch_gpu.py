@@ -323,3 +323,21 @@ def test_batch_table_passes_many_collisions(rsfm, oracle, tables, topk):
     np.testing.assert_array_equal(_host(s).view(np.uint32), es)
     np.testing.assert_array_equal(_host(f).view(np.uint32), ef)
     batch.close()
+
+
+def test_cascade_matcher_table_records_same_results(rsfm):
+    """CascadeMatcher with table records (the default: per-table passes) and without them (the
+    one-thread-per-query kernel) give the same results for every pair."""
+    from rapidsfm_b200 import cashash as ch
+    rng = np.random.default_rng(41)
+    descs = [_dev(synth.make_pair(int(n), 1, 0.5, 8.0, seed=int(rng.integers(1 << 30)))[0]) for n in (2000, 1500, 2600)]
+    got = []
+    for tr in (True, False):
+        cm = ch.CascadeMatcher(ch.CasHash(ch.gaussian_weights(41)), table_records=tr)
+        for k, d in enumerate(descs):
+            cm.register_image(k, d)
+        assert all((img.table_records is not None) == tr for img in cm.images.values())
+        got.append(cm.match([(0, 1), (1, 2), (2, 0), (0, 2)], count_candidates=True))
+    torch.cuda.synchronize()
+    for a, b in zip(*got):
+        assert all(torch.equal(x, y) for x, y in zip(a, b))
