@@ -97,8 +97,9 @@ def test_new_entry_points_validate_without_gpu(rsfm):
 
 
 def test_ranked_alignment_checked_without_gpu(rsfm):
-    """The ranked matcher's vector loads need aligned arrays (descriptors and records 32 bytes,
-    codes and bucket lists 16, keys 8); a misaligned array is rejected before any CUDA call."""
+    """The ranked matcher's vector loads need aligned arrays (descriptors, records and table
+    records 32 bytes, codes and bucket lists 16, keys 8); a misaligned array is rejected before
+    any CUDA call."""
     lib = rsfm._lib.load()
     R = rsfm._lib.RankedImage
 
@@ -109,7 +110,7 @@ def test_ranked_alignment_checked_without_gpu(rsfm):
         return R(**f)
 
     for bad in (dict(buckets=0x50004), dict(records=0x70010), dict(codes=0x30008), dict(keys=0x20004),
-                dict(desc=0x10010)):
+                dict(desc=0x10010), dict(tableRecords=0x78010)):
         q, t = img(), img(**bad)
         assert lib.rsfm_cashash_match_ranked(ctypes.byref(q), ctypes.byref(t), 6, 10, 4, 5,
                                              0x80000, 0x90000, 0xA0000, None, None) == 1
@@ -117,3 +118,17 @@ def test_ranked_alignment_checked_without_gpu(rsfm):
         h = ctypes.c_void_p(0)
         assert lib.rsfm_ranked_batch_create(ctypes.byref(pair), 1, 6, 10, 4, 5, ctypes.byref(h)) == 1
         assert not h.value
+
+
+def test_pack_table_records_arguments_checked_without_gpu(rsfm):
+    """rsfm_ranked_pack_table_records: nothing to do for an empty image; missing or misaligned
+    (records and table records 32 bytes) arrays and images of 2^24 descriptors or more are
+    rejected before any CUDA call."""
+    lib = rsfm._lib.load()
+    pack = lib.rsfm_ranked_pack_table_records
+    assert pack(None, None, 0, None, None) == 0
+    assert pack(0x10000, 0x20000, 100, 0x30000 + 16, None) == 1
+    assert pack(0x10000 + 16, 0x20000, 100, 0x30000, None) == 1
+    assert pack(None, 0x20000, 100, 0x30000, None) == 1
+    assert pack(0x10000, None, 100, 0x30000, None) == 1
+    assert pack(0x10000, 0x20000, 1 << 24, 0x30000, None) == 1
