@@ -105,7 +105,8 @@ def register_ranked_images(hasher, descs, stream=None, table_records=False):
     descriptors are first copied back to back into one buffer; every per-descriptor step then runs
     once over all of them and every bucket-build step once for all images. hasher: a CasHash with
     192 channels or a learned_hash.LearnedHash. table_records: also pack each image's records in
-    bucket-list order (RankedImage.pack_table_records, one launch per image). Returns one
+    bucket-list order (RankedImage.pack_table_records, one launch per image; only train images use
+    them, and only images of fewer than 2^24 descriptors can have them). Returns one
     RankedImage per input (views of shared buffers, including the packed copy of its descriptors)."""
     lib = _lib.load()
     for d in descs:

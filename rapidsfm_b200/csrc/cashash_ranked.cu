@@ -653,10 +653,12 @@ __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_
 // bucket, whose table-s candidates are one and the same list: the lanes load the same table records
 // (one L1 wavefront for all of them instead of one per lane) and run the same number of steps.
 // Between passes each query's running top-12 and candidate count wait in a 64-byte slot; the pairs
-// are processed in chunks (whole pairs, at most kPassChunk queries unless one pair is larger) whose
-// slots stay in L2. The last pass re-ranks and writes the results. Same results as the kernels above:
+// are processed in chunks of whole pairs (at most kPassChunk queries unless one pair is larger),
+// which bounds the slots' memory (64 bytes per query, 1 GiB at kPassChunk); within that bound a
+// larger chunk is faster (measured at 2^18 .. 2^23 queries: fewer partial waves per launch outweigh
+// keeping the slots in L2). The last pass re-ranks and writes the results. Same results as the kernels above:
 // the same candidates in the same tables, the same keys, the same top-K set.
-constexpr uint32_t kPassChunk = 1u << 20;
+constexpr uint32_t kPassChunk = 1u << 24;
 constexpr int kPassBlock = 128;
 constexpr int kPassMinBlocks = 8;  // 64 registers; the last pass (re-rank) keeps the thread kernel's 72
 
