@@ -737,6 +737,13 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
             const uint4* rec = T.trec + 2 * size_t(S) * T.n;
             for (; x < end; x += 4) {
                 const uint32_t cnt = min(4u, end - x);
+                // The records two steps ahead into L2 (their one or two 128-byte lines), in every pass
+                // but the last: measured 4-5 % faster at 6 / 8 tables; in the last pass, whose re-rank
+                // loads compete, it cost time.
+                if (!kLast && x + 8u < end) {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(&rec[2 * size_t(x + 8u)]));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(&rec[2 * size_t(min(x + 11u, end - 1u))]));
+                }
                 uint4 r0[4], r1[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
