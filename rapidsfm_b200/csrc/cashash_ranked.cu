@@ -4,11 +4,17 @@
 // by lower index), the best `topK` are re-ranked by exact L2, and the query gets the best match,
 // the second-best distance and the ratio-test flag.
 //
-// One warp per query. Duplicate candidates (a train descriptor colliding in several tables) are
-// dropped without a set: a candidate found in table s is kept only if it collides with the query
-// in no table before s. Candidate keys (hamming << 24 | index) go to a per-warp shared buffer; the
-// top-K are extracted by K rounds of a warp minimum (keys are distinct), merging buffer flushes
-// with the running top-K when a query has more candidates than the buffer holds.
+// Duplicate candidates (a train descriptor colliding in several tables) are dropped without a set:
+// a candidate found in table s is kept only if it collides with the query in no table before s.
+// Candidate keys are hamming << 24 | index (distinct). Three kernels compute the same results:
+// - one warp per query (any topK up to 32): keys go to a per-warp shared buffer, the top-K are
+//   extracted by a histogram threshold and a bitonic sort (K rounds of a warp minimum otherwise);
+// - one thread per query (topK <= 12; the single-pair entry and batches without table records):
+//   one cursor over the concatenated bucket lists, a sorted register top list;
+// - one pass per table (batches whose train images have table records, topK <= 12): queries in
+//   each table's bucket order so a warp's lanes walk the same list, top lists carried between
+//   passes in 64-byte slots, the last pass re-ranks.
+// The thread and pass kernels re-rank by groups of four lanes per train row.
 #include "common.h"
 #include <algorithm>
 #include <cstdlib>
