@@ -410,6 +410,36 @@ __device__ __forceinline__ void merge4(uint32_t (&top)[kThreadTopK], uint32_t (&
     for (int i = 0; i < 4; ++i) top[8 + i] = w[i];
 }
 
+// The same for a list of 10 (top[10], top[11] stay ~0u; topK <= 10): x = top[0..9], ~0u, ~0u,
+// k[3..0] is bitonic; after the first half-cleaner the lower 8 are sorted as above and the upper
+// half's two smallest are min(top[8], max(top[4], k[3])), min(top[9], max(top[5], k[2])),
+// max(top[6], k[1]), max(top[7], k[0]) taken pairwise at distance 2, then ordered: 48 min/max
+// instead of 54.
+__device__ __forceinline__ void merge4_10(uint32_t (&top)[kThreadTopK], uint32_t (&k)[4]) {
+    cas(k[0], k[1]);
+    cas(k[2], k[3]);
+    cas(k[0], k[2]);
+    cas(k[1], k[3]);
+    cas(k[1], k[2]);
+    if (k[0] >= top[9]) return;
+    uint32_t u[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t a = top[i + 4], b = k[3 - i];
+        top[i + 4] = min(a, b);
+        u[i] = max(a, b);
+    }
+#pragma unroll
+    for (int d = 4; d > 0; d >>= 1)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if ((i & d) == 0) cas(top[i], top[i + d]);
+    uint32_t z0 = min(min(top[8], u[0]), u[2]), z1 = min(min(top[9], u[1]), u[3]);
+    cas(z0, z1);
+    top[8] = z0;
+    top[9] = z1;
+}
+
 struct PairList {
     const PairDev* p;
     __device__ const PairDev& operator[](uint32_t k) const { return p[k]; }
@@ -693,7 +723,8 @@ __device__ __forceinline__ bool collides_before_c(uint2 t, uint2 q) {
 }
 
 // Pass over table S. blockPair[k] .. blockPair[k + 1]: the pairs that block k's queries can belong to.
-template <uint32_t S, bool kLast>
+// kShort (topK <= 10): a top list of 10 (merge4_10); slots 10 and 11 of the list and state hold ~0u.
+template <uint32_t S, bool kLast, bool kShort>
 __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMinBlocks) ranked_pass_kernel(
     const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, const uint32_t* __restrict__ blockPair,
     uint32_t g0, uint32_t g1, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen, uint4* __restrict__ state) {
@@ -723,6 +754,7 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
             top[4] = b.x, top[5] = b.y, top[6] = b.z, top[7] = b.w;
             top[8] = c.x, top[9] = c.y, top[10] = c.z, top[11] = c.w;
             total = d.x;
+            if (kShort) top[10] = top[11] = 0xFFFFFFFFu;
         }
         const Img& T = P.t;
         if (T.n) {
@@ -764,7 +796,10 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
                                        __popc(r1[u].y ^ qc.w);
                     k[u] = (h << 24) | r1[u].w;
                 }
-                merge4(top, k);
+                if (kShort)
+                    merge4_10(top, k);
+                else
+                    merge4(top, k);
             }
         }
         if (!kLast) {
@@ -781,19 +816,20 @@ __global__ void __launch_bounds__(kPassBlock, kLast ? kThreadMinBlocks : kPassMi
 using PassKernel = void (*)(const PairDev*, const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint32_t, uint32_t,
                             uint32_t, uint4*);
 template <uint32_t S>
-constexpr PassKernel pass_kernel(bool last) {
-    return last ? ranked_pass_kernel<S, true> : ranked_pass_kernel<S, false>;
+constexpr PassKernel pass_kernel(bool last, bool shrt) {
+    return last ? (shrt ? ranked_pass_kernel<S, true, true> : ranked_pass_kernel<S, true, false>)
+                : (shrt ? ranked_pass_kernel<S, false, true> : ranked_pass_kernel<S, false, false>);
 }
-inline PassKernel pass_kernel_for(uint32_t s, bool last) {
+inline PassKernel pass_kernel_for(uint32_t s, bool last, bool shrt) {
     switch (s) {
-        case 0: return pass_kernel<0>(last);
-        case 1: return pass_kernel<1>(last);
-        case 2: return pass_kernel<2>(last);
-        case 3: return pass_kernel<3>(last);
-        case 4: return pass_kernel<4>(last);
-        case 5: return pass_kernel<5>(last);
-        case 6: return pass_kernel<6>(last);
-        default: return pass_kernel<7>(last);
+        case 0: return pass_kernel<0>(last, shrt);
+        case 1: return pass_kernel<1>(last, shrt);
+        case 2: return pass_kernel<2>(last, shrt);
+        case 3: return pass_kernel<3>(last, shrt);
+        case 4: return pass_kernel<4>(last, shrt);
+        case 5: return pass_kernel<5>(last, shrt);
+        case 6: return pass_kernel<6>(last, shrt);
+        default: return pass_kernel<7>(last, shrt);
     }
 }
 
@@ -992,7 +1028,7 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
         for (const auto& c : b->chunks) {
             const uint32_t grid = (c.g1 - c.g0 + chr::kPassBlock - 1) / chr::kPassBlock;
             for (uint32_t s = 0; s < b->tables; ++s) {
-                chr::pass_kernel_for(s, s + 1 == b->tables)<<<grid, chr::kPassBlock, 0, stream>>>(
+                chr::pass_kernel_for(s, s + 1 == b->tables, b->topK <= 10)<<<grid, chr::kPassBlock, 0, stream>>>(
                     b->dPairs, b->dBegin, b->dBlockPair + c.blockPair, c.g0, c.g1, b->topK, b->ratioNum, b->ratioDen,
                     b->dState);
                 ++launches;
