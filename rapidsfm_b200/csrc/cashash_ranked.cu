@@ -525,8 +525,8 @@ __device__ __forceinline__ void rerank_group4(const Pairs& pairs, bool live, uin
 // kTrec: the train image has table records (each table's records in its bucket-list order, the
 // index in word 7): a candidate is then one load at its list position instead of a bucket-entry
 // load followed by a record load, and a step takes the next four entries of the list, whatever
-// their alignment.
-template <bool kTrec>
+// their alignment. kShort (topK <= 10): a top list of 10 (merge4_10; top[10], top[11] stay ~0u).
+template <bool kTrec, bool kShort>
 __device__ __forceinline__ void walk_query_thread(const Img& Q, const Img& T, uint32_t i, uint32_t tables,
                                                   uint32_t (&top)[kThreadTopK], uint32_t& total) {
     const uint2 qk = __ldg(&Q.keys[i]);
@@ -614,11 +614,14 @@ __device__ __forceinline__ void walk_query_thread(const Img& Q, const Img& T, ui
                                __popc(tc[u].w ^ qc.w);
             k[u] = (h << 24) | j[u];
         }
-        merge4(top, k);
+        if (kShort)
+            merge4_10(top, k);
+        else
+            merge4(top, k);
     }
 }
 
-template <bool kTrec>
+template <bool kTrec, bool kShort>
 __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_kernel(OnePair P, uint32_t tables,
                                                                                       uint32_t topK, uint32_t ratioNum,
                                                                                       uint32_t ratioDen) {
@@ -630,7 +633,7 @@ __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_
     for (int r = 0; r < kThreadTopK; ++r) top[r] = 0xFFFFFFFFu;
     if (live) {
         i = P.v.q.buckets ? __ldg(&P.v.q.buckets[t]) : t;
-        walk_query_thread<kTrec>(P.v.q, P.v.t, i, tables, top, total);
+        walk_query_thread<kTrec, kShort>(P.v.q, P.v.t, i, tables, top, total);
     }
     rerank_group4(P, live, 0u, i, top, total, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
 }
@@ -660,7 +663,7 @@ __global__ void table_records_kernel(const uint4* __restrict__ rec, const uint32
     }
 }
 
-template <bool kTrec>
+template <bool kTrec, bool kShort>
 __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_batch_kernel(
     const PairDev* __restrict__ pairs, const uint32_t* __restrict__ begin, uint32_t nPairs, uint32_t total,
     uint32_t tables, uint32_t topK, uint32_t ratioNum, uint32_t ratioDen) {
@@ -678,7 +681,7 @@ __global__ void __launch_bounds__(kThreadBlock, kThreadMinBlocks) ranked_thread_
         // neighbouring threads then share their first table's candidate list, walk it in step and
         // read the same records. (Measured against natural order and a candidate-count sort: fastest.)
         if (P.q.buckets) i = __ldg(&P.q.buckets[i]);
-        walk_query_thread<kTrec>(P.q, P.t, i, tables, top, cand);
+        walk_query_thread<kTrec, kShort>(P.q, P.t, i, tables, top, cand);
     }
     rerank_group4(PairList{pairs}, live, p, i, top, cand, topK, ratioNum, ratioDen, rows[threadIdx.x >> 5]);
 }
@@ -882,12 +885,10 @@ extern "C" int rsfm_cashash_match_ranked(const rsfm_ranked_image* query, const r
     if (chr::use_thread_kernel(topK)) {
         const uint32_t grid = (Q.n + chr::kThreadBlock - 1) / chr::kThreadBlock;
         const chr::OnePair P{chr::PairDev{Q, T, O}};
-        if (T.trec)
-            chr::ranked_thread_kernel<true>
-                <<<grid, chr::kThreadBlock, 0, stream>>>(P, nbTables, topK, ratioNum, ratioDen);
-        else
-            chr::ranked_thread_kernel<false>
-                <<<grid, chr::kThreadBlock, 0, stream>>>(P, nbTables, topK, ratioNum, ratioDen);
+        const bool shrt = topK <= 10;
+        auto k = T.trec ? (shrt ? chr::ranked_thread_kernel<true, true> : chr::ranked_thread_kernel<true, false>)
+                        : (shrt ? chr::ranked_thread_kernel<false, true> : chr::ranked_thread_kernel<false, false>);
+        k<<<grid, chr::kThreadBlock, 0, stream>>>(P, nbTables, topK, ratioNum, ratioDen);
     } else {
         const uint32_t grid = std::min<uint32_t>((Q.n + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
         chr::ranked_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(Q, T, nbTables, topK, ratioNum, ratioDen, O);
@@ -1036,12 +1037,12 @@ extern "C" int rsfm_ranked_batch_launch(rsfm_ranked_batch* b, cudaStream_t strea
         }
     } else if (chr::use_thread_kernel(b->topK)) {
         const uint32_t grid = (b->total + chr::kThreadBlock - 1) / chr::kThreadBlock;
-        if (b->tableRecords)
-            chr::ranked_thread_batch_kernel<true><<<grid, chr::kThreadBlock, 0, stream>>>(
-                b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
-        else
-            chr::ranked_thread_batch_kernel<false><<<grid, chr::kThreadBlock, 0, stream>>>(
-                b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK, b->ratioNum, b->ratioDen);
+        const bool shrt = b->topK <= 10;
+        auto k = b->tableRecords
+                     ? (shrt ? chr::ranked_thread_batch_kernel<true, true> : chr::ranked_thread_batch_kernel<true, false>)
+                     : (shrt ? chr::ranked_thread_batch_kernel<false, true> : chr::ranked_thread_batch_kernel<false, false>);
+        k<<<grid, chr::kThreadBlock, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total, b->tables, b->topK,
+                                                  b->ratioNum, b->ratioDen);
     } else {
         const uint32_t grid = std::min<uint32_t>((b->total + chr::kWarps - 1) / chr::kWarps, uint32_t(8 * sm_count()));
         chr::ranked_batch_kernel<<<grid, 32 * chr::kWarps, 0, stream>>>(b->dPairs, b->dBegin, b->nPairs, b->total,
